@@ -1,0 +1,204 @@
+"""CPU checkers for the lattice-Boltzmann hot path -- TEST INFRASTRUCTURE.
+
+Two implementations behind one Python interface (:class:`CpuSolver`):
+
+* ``backend="oracle"``: ``liboracle.so``, the plain-C restatement of the
+  reference algorithm in ``lbm_oracle_body.h`` (double or float arithmetic,
+  optional binary16 / bfloat16 storage rounding).
+* ``backend="ref"``: ``_ref/libm3lb_ref_{f64,f32}.so``, the reference's own
+  ``FluidSolver`` headers compiled unmodified against a host stand-in for the
+  Kokkos API (``ref/``).  Present only where the reference sources were
+  available at build time, or where the built libraries were carried along.
+
+Only the tests, the smoke check and the CPU-baseline leg of ``bench.py`` use
+this package, as the checker.  The product never imports it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ORACLE_LIB = HERE / "liboracle.so"
+REF_LIBS = {"f64": HERE / "_ref" / "libm3lb_ref_f64.so", "f32": HERE / "_ref" / "libm3lb_ref_f32.so"}
+
+OPS = {"none": 0, "bgk": 1, "trt": 2, "mrt": 3, "cm": 4}
+QUANT = {None: 0, "none": 0, "f16": 1, "bf16": 2}
+
+_dp = C.POINTER(C.c_double)
+_u8p = C.POINTER(C.c_uint8)
+_vp = C.c_void_p
+
+
+def _bind(lib, prefix):
+    sig = {
+        "create": (_vp, [C.c_int] * 6 + [C.c_int] * 6 + [C.c_double] * 5),
+        "destroy": (None, [_vp]),
+        "set_geometry": (None, [_vp, _u8p]),
+        "initialize": (None, [_vp] + [C.c_double] * 4),
+        "initialize_field": (None, [_vp] + [_dp] * 4),
+        "step": (None, [_vp, C.c_int, C.c_int]),
+        "macro": (None, [_vp] + [_dp] * 4),
+        "stored_macro": (None, [_vp] + [_dp] * 4),
+        "total_mass": (C.c_double, [_vp]),
+        "total_momentum": (C.c_double, [_vp, C.c_int]),
+        "gather": (None, [_vp, _dp]),
+        "seed": (None, [_vp, _dp]),
+        "slot_sum": (C.c_double, [_vp]),
+        "n_padded": (C.c_longlong, [_vp]),
+        "timestep": (C.c_longlong, [_vp]),
+    }
+    fns = {}
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, prefix + name)
+        fn.restype = res
+        fn.argtypes = args
+        fns[name] = fn
+    return fns
+
+
+_cache: dict = {}
+
+
+def _lib(backend: str, precision: str):
+    key = (backend, precision)
+    if key in _cache:
+        return _cache[key]
+    if backend == "oracle":
+        if not ORACLE_LIB.exists():
+            raise FileNotFoundError(f"{ORACLE_LIB} not built (make -C oracle oracle)")
+        lib = C.CDLL(str(ORACLE_LIB))
+        fns = _bind(lib, "lbmo_f64_" if precision == "f64" else "lbmo_f32_")
+    elif backend == "ref":
+        path = REF_LIBS[precision]
+        if not path.exists():
+            raise FileNotFoundError(f"{path} not built (make -C oracle ref)")
+        lib = C.CDLL(str(path))
+        fns = _bind(lib, "ref_")
+        lib.ref_set_threads.argtypes = [C.c_int]
+        lib.ref_get_threads.restype = C.c_int
+        fns["_lib"] = lib
+    else:
+        raise ValueError(backend)
+    _cache[key] = fns
+    return fns
+
+
+def ref_available(precision: str = "f64") -> bool:
+    return REF_LIBS[precision].exists()
+
+
+def set_ref_threads(n: int, precision: str = "f64") -> None:
+    """OpenMP threads the reference build uses (1 gives a deterministic order)."""
+    _lib("ref", precision)["_lib"].ref_set_threads(int(n))
+
+
+def _ptr(a):
+    return a.ctypes.data_as(_dp)
+
+
+class CpuSolver:
+    """One lattice on the CPU, reference-shaped API (FluidSolver.hpp:34-637).
+
+    Arrays exchanged with the caller are interior-only, shaped (nz, ny, nx),
+    x fastest; populations (``gather``/``seed``) are (n_padded, Q), node-major.
+    """
+
+    def __init__(self, backend="oracle", lattice=27, op="bgk", eq=0, shifted=True,
+                 forcing=False, nx=8, ny=8, nz=8, px=True, py=True, pz=True,
+                 omega=1.0, omega2=-1.0, fx=0.0, fy=0.0, fz=0.0, precision="f64",
+                 quant=None, streaming=0):
+        self.backend, self.precision = backend, precision
+        self.lattice, self.Q = lattice, lattice
+        self.nx, self.ny, self.nz = nx, ny, nz
+        self.shape = (nz, ny, nx)
+        self._f = _lib(backend, precision)
+        opc = OPS[op] if isinstance(op, str) else int(op)
+        if backend == "oracle":
+            if streaming:
+                raise ValueError("the C oracle implements Esoteric Pull only")
+            h = self._f["create"](lattice, opc, int(eq), int(shifted), int(forcing),
+                                  QUANT[quant], nx, ny, nz, int(px), int(py), int(pz),
+                                  omega, omega2, fx, fy, fz)
+        else:
+            if quant not in (None, "none"):
+                raise ValueError("the reference build has no narrow storage")
+            h = self._f["create"](lattice, int(streaming), opc, int(eq), int(shifted),
+                                  int(forcing), nx, ny, nz, int(px), int(py), int(pz),
+                                  omega, omega2, fx, fy, fz)
+        if not h:
+            raise ValueError("unsupported configuration")
+        self._h = h
+        self.n_padded = int(self._f["n_padded"](h))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._f["destroy"](self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- reference API ----
+    def set_geometry(self, flags):
+        fl = np.ascontiguousarray(flags, dtype=np.uint8).reshape(self.shape)
+        self._f["set_geometry"](self._h, fl.ctypes.data_as(_u8p))
+
+    def initialize(self, rho0=1.0, ux=0.0, uy=0.0, uz=0.0):
+        self._f["initialize"](self._h, rho0, ux, uy, uz)
+
+    def initialize_field(self, rho, ux, uy, uz):
+        arrs = [np.ascontiguousarray(np.broadcast_to(a, self.shape), dtype=np.float64)
+                for a in (rho, ux, uy, uz)]
+        self._f["initialize_field"](self._h, *[_ptr(a) for a in arrs])
+
+    def step(self, n=1, store_macro=False):
+        self._f["step"](self._h, int(n), int(store_macro))
+
+    def _four(self, fn):
+        out = [np.empty(self.shape, np.float64) for _ in range(4)]
+        fn(self._h, *[_ptr(a) for a in out])
+        return tuple(out)
+
+    def macro(self):
+        return self._four(self._f["macro"])
+
+    def stored_macro(self):
+        return self._four(self._f["stored_macro"])
+
+    def total_mass(self):
+        return float(self._f["total_mass"](self._h))
+
+    def total_momentum(self, a):
+        return float(self._f["total_momentum"](self._h, int(a)))
+
+    def gather(self):
+        out = np.empty((self.n_padded, self.Q), np.float64)
+        self._f["gather"](self._h, _ptr(out))
+        return out
+
+    def seed(self, pops):
+        arr = np.ascontiguousarray(pops, dtype=np.float64).reshape(self.n_padded, self.Q)
+        self._f["seed"](self._h, _ptr(arr))
+
+    def slot_sum(self):
+        return float(self._f["slot_sum"](self._h))
+
+    @property
+    def timestep(self):
+        return int(self._f["timestep"](self._h))
+
+
+def build(ref: bool = True, jobs: int | None = None) -> None:
+    """Build the C oracle and, when the reference sources exist, the reference."""
+    import subprocess
+    jobs = jobs or os.cpu_count() or 4
+    target = "all" if ref else "oracle"
+    subprocess.run(["make", "-C", str(HERE), f"-j{jobs}", target], check=True,
+                   stdout=subprocess.DEVNULL)

@@ -1,0 +1,60 @@
+/*
+ * CPU oracle for the M3LB lattice-Boltzmann time step -- TEST INFRASTRUCTURE
+ * (see lbm_oracle.h).  Build: `make -C oracle oracle` (gcc, -ffp-contract=off).
+ */
+#include "lbm_oracle.h"
+
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+/* Velocity sets in the Esoteric-Pull ordering: rest first, then opposite
+ * pairs at adjacent indices (src/lattice/Lattices.hpp:75-159).  The order is
+ * part of the storage contract, so it is the reference's order exactly. */
+static const int D2Q9_CX[9] = {0, 1, -1, 0, 0, 1, -1, 1, -1};
+static const int D2Q9_CY[9] = {0, 0, 0, 1, -1, 1, -1, -1, 1};
+static const int D2Q9_W[9] = {16, 4, 4, 4, 4, 1, 1, 1, 1}; /* / 36 */
+static const int D3Q27_CX[27] = {0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1,
+                                 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, -1, 1};
+static const int D3Q27_CY[27] = {0, 0, 0, 1, -1, 0, 0, 1, -1, -1, 1, 0, 0, 0, 0,
+                                 1, -1, 1, -1, 1, -1, 1, -1, -1, 1, 1, -1};
+static const int D3Q27_CZ[27] = {0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, -1, -1, 1,
+                                 1, -1, -1, 1, 1, -1, -1, 1, 1, -1, 1, -1};
+static const int D3Q27_W[27] = {64, 16, 16, 16, 16, 16, 16, 4, 4, 4, 4, 4, 4, 4,
+                                4,  4,  4,  4,  4,  1,  1,  1, 1, 1, 1, 1, 1}; /* / 216 */
+
+/* Direction index for component indices (velocity + 1), the product-basis
+ * table pi() of src/collision/ProductBasis.hpp:118-131. */
+static int D2Q9_DIR[3][3];
+static int D3Q27_DIR[3][3][3];
+static void build_dir_tables(void) {
+  for (int i = 0; i < 9; ++i) D2Q9_DIR[D2Q9_CX[i] + 1][D2Q9_CY[i] + 1] = i;
+  for (int i = 0; i < 27; ++i) D3Q27_DIR[D3Q27_CX[i] + 1][D3Q27_CY[i] + 1][D3Q27_CZ[i] + 1] = i;
+}
+__attribute__((constructor)) static void lbmo_init(void) { build_dir_tables(); }
+
+/* float -> bfloat16 -> float, round to nearest even (NaN kept quiet). */
+static inline float lbmo_bf16_round(float v) {
+  uint32_t u;
+  memcpy(&u, &v, 4);
+  if ((u & 0x7f800000u) == 0x7f800000u && (u & 0x007fffffu)) {
+    u |= 0x00400000u;
+  } else {
+    u += 0x7fffu + ((u >> 16) & 1u);
+  }
+  u &= 0xffff0000u;
+  memcpy(&v, &u, 4);
+  return v;
+}
+
+#define R double
+#define P lbmo_f64_
+#include "lbm_oracle_body.h"
+#undef R
+#undef P
+
+#define R float
+#define P lbmo_f32_
+#include "lbm_oracle_body.h"
+#undef R
+#undef P

@@ -1,0 +1,51 @@
+/*
+ * CPU oracle for the M3LB lattice-Boltzmann time step -- TEST INFRASTRUCTURE.
+ *
+ * A plain-C restatement of the reference's hot path (src/ of M3LB): Esoteric
+ * Pull in-place streaming on one population array, BGK / TRT / raw MRT /
+ * central-moment collision, Guo forcing, halfway bounce-back by skipping
+ * solid cells.  Only the tests, the smoke check and the CPU-baseline leg of
+ * the benchmark use it, as the checker; the product never calls it.
+ *
+ * Two builds of one body (lbm_oracle_body.h): lbmo_f64_* computes in double,
+ * lbmo_f32_* in float.  `quant` emulates narrow population storage with the
+ * same arithmetic: every value written into the population array is rounded
+ * to IEEE binary16 (1) or bfloat16 (2), round-to-nearest-even, exactly as a
+ * GPU store of a 16-bit population does.  0 stores at full precision.
+ *
+ * The entry points and their argument meanings are those of
+ * oracle/ref/ref_driver.cpp, so a test can run the reference build and this
+ * restatement side by side on one input.
+ *
+ * Codes: lattice 9 (D2Q9) / 27 (D3Q27); op 0 none (pure streaming), 1 BGK,
+ * 2 TRT, 3 MRT, 4 central moments; eq 0 second order, 1 product form (BGK and
+ * TRT only); flags per interior node: 0 fluid, 1 solid, 2 excluded.
+ */
+#ifndef LBM_ORACLE_H
+#define LBM_ORACLE_H
+#include <stdint.h>
+
+#define LBMO_DECLARE(P)                                                              \
+  void* P##create(int lattice, int op, int eq, int shifted, int forcing, int quant,  \
+                  int nx, int ny, int nz, int px, int py, int pz, double omega,      \
+                  double omega2, double fx, double fy, double fz);                   \
+  void P##destroy(void* h);                                                          \
+  void P##set_geometry(void* h, const uint8_t* flags);                               \
+  void P##initialize(void* h, double rho, double ux, double uy, double uz);          \
+  void P##initialize_field(void* h, const double* rho, const double* ux,             \
+                           const double* uy, const double* uz);                      \
+  void P##step(void* h, int n, int store_macro);                                     \
+  void P##macro(void* h, double* rho, double* ux, double* uy, double* uz);           \
+  void P##stored_macro(void* h, double* rho, double* ux, double* uy, double* uz);    \
+  double P##total_mass(void* h);                                                     \
+  double P##total_momentum(void* h, int axis);                                       \
+  void P##gather(void* h, double* out);                                              \
+  void P##seed(void* h, const double* in);                                           \
+  double P##slot_sum(void* h);                                                       \
+  long long P##n_padded(void* h);                                                    \
+  long long P##timestep(void* h);
+
+LBMO_DECLARE(lbmo_f64_)
+LBMO_DECLARE(lbmo_f32_)
+
+#endif
