@@ -1,0 +1,437 @@
+#!/usr/bin/env python
+"""Benchmark of the M3LB lattice-Boltzmann step on B200.
+
+Workload (one "step" = one fused stream-collide time step over the whole
+lattice): D3Q27 central-moment Taylor-Green vortex on a periodic 256^3
+lattice (u0 = 0.05, Re = 1600 on L = N / 2 pi, tau = 0.5 + 3 u0 N / (2 pi Re)),
+populations stored shifted in FP16 with FP32 arithmetic.  The same workload
+with FP32 storage is timed alongside for the FP16/FP32 ratio.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl m3lb|reference]
+
+One process per GPU; under torchrun each rank advances its own replica
+lattice (no data exchange: "replicas only"), time is the max over ranks.
+Prints one JSON line on rank 0.  --impl reference times the reference's own
+CPU implementation of the step (its src/ headers built against a host stand-in
+for Kokkos, oracle/_ref) on this machine's host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import csv
+import io
+import json
+import math
+import os
+import subprocess
+import sys
+import time
+from datetime import timedelta
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+import numpy as np  # noqa: E402
+
+N_DEFAULT = 256
+U0 = 0.05
+RE = 1600.0
+Q = 27
+L2_BYTES = 126 * 2 ** 20
+METRIC = "D3Q27 CM MLUPS & HBM GB/s (FP16 vs FP32 store) at 256^3; p99 request latency"
+WORKLOAD = ("D3Q27 central-moment Taylor-Green vortex, periodic 256^3, "
+            "shifted populations stored FP16, FP32 arithmetic")
+
+
+def tgv_params(n):
+    L = n / (2 * math.pi)
+    nu = U0 * L / RE
+    tau = 3 * nu + 0.5
+    return nu, tau, 1.0 / tau
+
+
+def tgv_fields(n, xp=np):
+    """Taylor-Green benchmark initial field (validation/tgv3d_bench.cpp IC):
+    u = u0 sin x cos y cos z, v = -u0 cos x sin y cos z, w = 0, analytic
+    pressure in the density."""
+    k = 2 * math.pi / n
+    i = xp.arange(n, dtype=xp.float64) * k
+    z, y, x = xp.meshgrid(i, i, i, indexing="ij")
+    dr = 3.0 * U0 * U0 / 16.0
+    rho = 1 + dr * (xp.cos(2 * x) + xp.cos(2 * y)) * (xp.cos(2 * z) + 2)
+    ux = U0 * xp.sin(x) * xp.cos(y) * xp.cos(z)
+    uy = -U0 * xp.cos(x) * xp.sin(y) * xp.cos(z)
+    uz = xp.zeros_like(ux)
+    return rho, ux, uy, uz
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def traffic_record(key):
+    p = ROOT / "profiles" / "traffic.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return d.get(key)
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled in the background."""
+
+    FIELDS = ("timestamp,index,pci.bus_id,clocks.sm,clocks.max.sm,power.draw,"
+              "clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, interval_ms=50):
+        self.proc = None
+        self.t0 = self.t1 = None
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 f"-lms={interval_ms}"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL,
+                text=True)
+        except Exception:
+            self.proc = None
+
+    def mark_start(self):
+        self.t0 = time.time()
+
+    def mark_end(self):
+        self.t1 = time.time()
+
+    def stop(self, bus_id=None):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.15)
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except Exception:
+            self.proc.kill()
+            out = ""
+        rows = []
+        for r in csv.reader(io.StringIO(out)):
+            if len(r) < 11:
+                continue
+            r = [c.strip() for c in r]
+            if bus_id and bus_id.lower() not in r[2].lower():
+                continue
+            try:
+                ts = time.mktime(time.strptime(r[0].split(".")[0], "%Y/%m/%d %H:%M:%S"))
+                ts += float("0." + r[0].split(".")[1]) if "." in r[0] else 0.0
+            except Exception:
+                ts = None
+            rows.append((ts, float(r[3]), float(r[4]), r[7:11]))
+        inside = [x for x in rows if x[0] is not None and self.t0 and
+                  self.t0 - 0.06 <= x[0] <= (self.t1 or 1e30) + 0.06]
+        use = inside or rows
+        if not use:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for x in use for k, v in enumerate(x[3]) if v == "Active"})
+        return {"sm_mhz": float(np.median([x[1] for x in use])),
+                "sm_max_mhz": float(max(x[2] for x in use)),
+                "reasons": reasons, "samples": len(use),
+                "window": "timed region" if inside else "whole run (timed region shorter than the sampling interval)"}
+
+
+# ------------------------------------------------------------------ GPU arm
+def gpu_arm(args, rank, world, dist):
+    import torch
+    from m3lb_b200 import capi
+    from m3lb_b200 import solver as S
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    props = torch.cuda.get_device_properties(dev)
+    bus = None
+    try:
+        bus = "%08x:%02x:%02x" % (props.pci_domain_id, props.pci_bus_id, props.pci_device_id)
+    except Exception:
+        bus = None
+    n = args.size
+    nodes = n ** 3
+    nu, tau, omega = tgv_params(n)
+    stream = torch.cuda.current_stream(dev)
+
+    def make(storage):
+        dom = S.Domain(n, n, n, True, True, True)
+        coll = S.CentralMoments(S.D3Q27, S.NoForcing(), S.ShiftedPopulations, omega=omega)
+        s = S.FluidSolver(dom, coll, storage=storage)
+        s.set_stream(stream)
+        rho, ux, uy, uz = [t.to(torch.float32).contiguous()
+                           for t in tgv_fields(n, _TorchNp(dev))]
+        s.initialize_field_device(rho, ux, uy, uz)
+        del rho, ux, uy, uz
+        return s
+
+    def timed(s, K, W):
+        for _ in range(W):
+            s.step()
+        torch.cuda.synchronize(dev)
+        if dist:
+            dist.barrier()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(K + 1)]
+        c0 = s.launch_count()
+        sampler.mark_start()
+        ev[0].record(stream)
+        for k in range(K):
+            s.step()
+            ev[k + 1].record(stream)
+        torch.cuda.synchronize(dev)
+        sampler.mark_end()
+        launches = s.launch_count() - c0
+        if dist:
+            dist.barrier()
+        total = ev[0].elapsed_time(ev[K]) / 1e3
+        per = [ev[k].elapsed_time(ev[k + 1]) / 1e3 for k in range(K)]
+        t = torch.tensor([total], dtype=torch.float64, device=dev)
+        if dist:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item()), float(np.mean(per)), launches
+
+    sampler = ClockSampler()
+    s16 = make(args.storage)
+    t16, per16, launches = timed(s16, args.steps, args.warmup)
+    red = s16.reduce()
+    finite = bool(np.isfinite(red).all())
+    mass_drift = None
+    s16.close()
+    clocks = sampler.stop(bus)
+
+    # FP32 storage on the same workload, for the FP16/FP32 ratio
+    s32 = make("f32")
+    t32, per32, _ = timed(s32, args.steps, args.warmup)
+    s32.close()
+
+    eb = 2 if args.storage in ("f16", "bf16") else (8 if args.storage == "f64" else 4)
+    bytes_per_launch = nodes * 2 * Q * eb
+    achieved = bytes_per_launch / per16 / 1e9
+    peak, peak_kind = measured_peaks()
+    value = world * nodes * args.steps / t16 / 1e6
+    value32 = world * nodes * args.steps / t32 / 1e6
+
+    out = {
+        "metric": METRIC, "value": round(value, 1), "unit": "MLUPS", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(t16 / args.steps * 1e3, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "storage": args.storage,
+        "data": "synthetic (analytic Taylor-Green initial field, generated on the device)",
+        "config": {"workload": WORKLOAD, "lattice": "D3Q27", "operator": "central moments",
+                   "nx": n, "ny": n, "nz": n, "nodes_per_gpu": nodes, "tau": round(tau, 6),
+                   "u0": U0, "Re": RE, "parallelism": f"replicas x{world}",
+                   "l2": f"inputs larger than L2 ({nodes * Q * eb / 1e6:.0f} MB of populations "
+                         f"per step vs {L2_BYTES / 1e6:.0f} MB L2)"},
+        "hbm_gbs": round(achieved, 1),
+        "fp32_storage": {"value": round(value32, 1), "unit": "MLUPS",
+                         "ms_per_step": round(t32 / args.steps * 1e3, 4),
+                         "hbm_gbs": round(nodes * 2 * Q * 4 / per32 / 1e9, 1)},
+        "fp16_over_fp32": round(value / value32, 3),
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
+                     "unit": "GB/s", "frac": round(achieved / peak, 4),
+                     "peak_kind": f"{peak_kind} (copy bandwidth)",
+                     "kernel": "step_pairs<D3Q27, F16, CM>",
+                     "algorithmic_bytes_per_launch": bytes_per_launch,
+                     "traffic": traffic_record(f"D3Q27_CM_{args.storage}_{n}")},
+        "gpu_launches": launches,
+        "clocks": clocks,
+        "state_finite": finite,
+    }
+    if mass_drift is not None:
+        out["mass_drift"] = mass_drift
+
+    if rank == 0 and not args.no_e2e:
+        out["e2e"] = e2e_arm(args, dev, stream, omega)
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(args)
+    return out
+
+
+class _TorchNp:
+    """The few numpy names tgv_fields uses, on a torch device."""
+
+    def __init__(self, dev):
+        import torch
+        self.t, self.dev = torch, dev
+        self.float64 = torch.float64
+
+    def arange(self, n, dtype=None):
+        return self.t.arange(n, dtype=dtype, device=self.dev)
+
+    def meshgrid(self, *a, indexing="ij"):
+        return self.t.meshgrid(*a, indexing=indexing)
+
+    def cos(self, x):
+        return self.t.cos(x)
+
+    def sin(self, x):
+        return self.t.sin(x)
+
+    def zeros_like(self, x):
+        return self.t.zeros_like(x)
+
+
+def e2e_arm(args, dev, stream, omega):
+    """Same metric through the public API with host buffers: each e2e step
+    copies the initial field from pinned host memory, advances
+    args.e2e_lbm_steps time steps and reads rho, u back to pinned memory."""
+    import torch
+    from m3lb_b200 import solver as S
+
+    n = args.size
+    nodes = n ** 3
+    dom = S.Domain(n, n, n, True, True, True)
+    coll = S.CentralMoments(S.D3Q27, S.NoForcing(), S.ShiftedPopulations, omega=omega)
+    s = S.FluidSolver(dom, coll, storage=args.storage)
+    s.set_stream(stream)
+    host_in = [torch.from_numpy(a.astype(np.float32)).pin_memory() for a in tgv_fields(n)]
+    host_out = [torch.empty((n, n, n), dtype=torch.float32).pin_memory() for _ in range(4)]
+    S_lbm = args.e2e_lbm_steps
+
+    def one():
+        s.initialize_field_f32(*host_in)
+        s.steps(S_lbm)
+        s.compute_macroscopic_f32(*host_out)
+
+    one()
+    torch.cuda.synchronize(dev)
+    reps = args.e2e_reps
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        one()
+    torch.cuda.synchronize(dev)
+    dt = time.perf_counter() - t0
+    ok = bool(torch.isfinite(host_out[1]).all())
+    s.close()
+    return {"value": round(nodes * S_lbm * reps / dt / 1e6, 1), "unit": "MLUPS",
+            "h2d_bytes_per_step": 4 * nodes * 4, "d2h_bytes_per_step": 4 * nodes * 4,
+            "lbm_steps_per_e2e_step": S_lbm, "e2e_steps": reps,
+            "ms_per_e2e_step": round(dt / reps * 1e3, 3), "finite": ok,
+            "api": "m3lb_b200.FluidSolver (C ABI: m3lb_init_field_f32, m3lb_step, m3lb_macro_f32)"}
+
+
+# ------------------------------------------------------------------ CPU legs
+def _host_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def _ref_rate(n, steps, threads, warm=1):
+    """MLUPS of the reference's own CPU path (oracle/_ref, FP32) on an n^3
+    periodic central-moment lattice."""
+    import oracle as O
+    O.set_ref_threads(threads, "f32")
+    _, _, omega = tgv_params(N_DEFAULT)
+    s = O.CpuSolver("ref", lattice=27, op="cm", shifted=True, nx=n, ny=n, nz=n,
+                    omega=omega, precision="f32")
+    s.initialize(1.0, U0, 0.0, 0.0)
+    s.step(warm)
+    t0 = time.perf_counter()
+    s.step(steps)
+    dt = time.perf_counter() - t0
+    s.close()
+    return n ** 3 * steps / dt / 1e6, dt
+
+
+def cpu_baseline(args):
+    import oracle as O
+    if not O.ref_available("f32"):
+        return {"value": None, "unit": "MLUPS", "cores": 0, "kind": "reference",
+                "sample": "reference build (oracle/_ref) not present"}
+    th = _host_threads()
+    # calibrate on a small lattice, then a bounded sample of ~10-20 s
+    rate, _ = _ref_rate(64, 2, th)
+    n = args.cpu_size
+    steps = max(1, int(min(12.0 * rate * 1e6 / n ** 3, 50)))
+    rate, dt = _ref_rate(n, steps, th)
+    return {"value": round(rate, 2), "unit": "MLUPS", "cores": th, "kind": "reference",
+            "sample": f"{steps} time steps of the reference src/ FluidSolver (FP32, "
+                      f"EsotericPull, CentralMoments, shifted) on a periodic {n}^3 lattice, "
+                      f"{dt:.1f} s, OpenMP {th} threads"}
+
+
+def reference_arm(args):
+    import oracle as O
+    th = _host_threads()
+    base = {"metric": METRIC, "unit": "MLUPS", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "impl": "reference",
+            "data": "synthetic (uniform flow initial state)"}
+    if not O.ref_available("f32"):
+        base.update({"unavailable": "reference build oracle/_ref not present"})
+        return base
+    # each step: one time step of a bounded sample lattice; the whole run
+    # (warm-up + steps) is sized to about two minutes of host time
+    rate, _ = _ref_rate(64, 2, th)
+    per_step_budget = 100.0 / max(args.steps + args.warmup, 1)
+    n = int(min(N_DEFAULT, max(32, (per_step_budget * rate * 1e6) ** (1 / 3))))
+    n -= n % 2
+    r, dt = _ref_rate(n, args.steps, th, warm=args.warmup)
+    base.update({
+        "value": round(r, 2), "ms_per_step": round(dt / args.steps * 1e3, 3),
+        "config": {"workload": f"D3Q27 central moments, FP32, periodic {n}^3 sample of the "
+                               f"256^3 workload", "nodes_per_step": n ** 3,
+                   "parallelism": f"{th} OpenMP threads"},
+        "cpu_baseline": {"value": round(r, 2), "unit": "MLUPS", "cores": th,
+                         "kind": "reference",
+                         "sample": f"{args.steps} time steps on a periodic {n}^3 lattice"},
+        "e2e": {"value": round(r, 2), "unit": "MLUPS", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    })
+    return base
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="m3lb", choices=["m3lb", "reference"])
+    ap.add_argument("--storage", default="f16", choices=["f16", "bf16", "f32"])
+    ap.add_argument("--size", type=int, default=N_DEFAULT)
+    ap.add_argument("--cpu-size", type=int, default=128)
+    ap.add_argument("--e2e-lbm-steps", type=int, default=100)
+    ap.add_argument("--e2e-reps", type=int, default=3)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(reference_arm(args)), flush=True)
+        return 0
+
+    dist = None
+    if world > 1:
+        import torch
+        import torch.distributed as tdist
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        tdist.init_process_group("nccl", timeout=timedelta(seconds=120))
+        dist = tdist
+    out = gpu_arm(args, rank, world, dist)
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,154 @@
+/*
+ * m3lb.h -- C ABI of the B200 lattice-Boltzmann step (libm3lb.so).
+ *
+ * One handle = one lattice resident in HBM: the Esoteric-Pull population array
+ * (one array, updated in place), the cell flags and the macroscopic fields.
+ * Every call returns M3LB_OK (0) or a negative status; m3lb_last_error()
+ * gives the message of the calling thread's last failure.  Nothing aborts.
+ * A handle is used by one host thread at a time; work is queued on the
+ * handle's CUDA stream (m3lb_set_stream), and calls that hand results to the
+ * host synchronise that stream.
+ *
+ * Each entry point replaces one member of the reference's C++ solver API
+ * (paths relative to the M3LB tree, src/solver/FluidSolver.hpp unless noted);
+ * the C++ headers under m3lb_b200/facade/ put those members back on top of
+ * this ABI.
+ *
+ * Codes
+ *   lattice : 9 (D2Q9), 27 (D3Q27)                 src/lattice/Lattices.hpp:75-159
+ *   op      : M3LB_OP_*                              src/collision/{BGK,TRT,MomentCollision}.hpp
+ *   eq      : M3LB_EQ_* (BGK and TRT only)           src/equilibrium/Equilibrium.hpp:131-136
+ *   storage : M3LB_STORE_* population element type; arithmetic is FP32 for
+ *             F32/F16/BF16 and FP64 for F64.  16-bit storage requires shifted
+ *             (except for M3LB_OP_NONE, which never reads the convention).
+ *   shifted : 1 stores g = f - w (ShiftedPopulations), 0 stores f (Raw)
+ *                                                    src/memory/Storage.hpp:27-35
+ *   flags   : per interior node, x fastest: 0 Fluid, 1 Solid, 2 Excluded
+ *                                                    src/boundary/Flags.hpp:20-33
+ */
+#ifndef M3LB_H
+#define M3LB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define M3LB_OK 0
+#define M3LB_ERR_INVALID -1     /* bad argument */
+#define M3LB_ERR_UNSUPPORTED -2 /* valid in the reference, not offered here */
+#define M3LB_ERR_CUDA -3        /* CUDA runtime failure */
+#define M3LB_ERR_MEMORY -4      /* device or host allocation failed */
+
+#define M3LB_OP_NONE 0 /* pure streaming: the NullCollision mock, tests/test_streaming.cpp:28-38 */
+#define M3LB_OP_BGK 1  /* src/collision/BGK.hpp:33-102 */
+#define M3LB_OP_TRT 2  /* src/collision/TRT.hpp:35-136 */
+#define M3LB_OP_MRT 3  /* MomentCollision<.., Central=false>, MomentCollision.hpp:380-381 */
+#define M3LB_OP_CM 4   /* MomentCollision<.., Central=true>,  MomentCollision.hpp:378-379 */
+
+#define M3LB_EQ_SECOND_ORDER 0 /* SecondOrderEquilibrium, Equilibrium.hpp:49-60 */
+#define M3LB_EQ_PRODUCT_FORM 1 /* ProductFormEquilibrium, Equilibrium.hpp:71-124 */
+
+#define M3LB_STORE_F32 0
+#define M3LB_STORE_F16 1
+#define M3LB_STORE_BF16 2
+#define M3LB_STORE_F64 3
+
+#define M3LB_OPT_NODE_KERNEL 1 /* value 1: always use the one-node step kernel */
+
+typedef struct m3lb_solver m3lb_solver;
+
+/* Message of the calling thread's last failed call ("" if none). */
+const char* m3lb_last_error(void);
+
+/* Bytes of HBM a lattice of this shape needs (populations, flags, macroscopic
+ * fields, reduction scratch): what an admission policy budgets. */
+int m3lb_footprint(int lattice, int nx, int ny, int nz, int px, int py, int pz, int storage,
+                   size_t* bytes);
+
+/* FluidSolver(const Domain&, const Collision&) (:42) with
+ * Domain(nx, ny, nz, px, py, pz) (src/grid/Domain.hpp:47-56) and
+ * EsotericPull<L>(Domain) (src/memory/EsotericPull.hpp:58).  Every interior
+ * node starts Fluid, halo nodes Excluded (:57-63); populations start at 0.
+ * Allocates on the current CUDA device. */
+int m3lb_create(int lattice, int nx, int ny, int nz, int px, int py, int pz, int op, int eq,
+                int storage, int shifted, int forcing, m3lb_solver** out);
+int m3lb_destroy(m3lb_solver* h);
+
+/* Public members of the collision policy: BGK::omega (BGK.hpp:43),
+ * TRT::omega_p / omega_m (TRT.hpp:46-47), MomentCollision::omega /
+ * omega_bulk (MomentCollision.hpp:89-90, omega2 < 0 follows omega), and
+ * Guo{fx, fy, fz} (src/forcing/Forcing.hpp:58-62, used when forcing != 0). */
+int m3lb_set_params(m3lb_solver* h, double omega, double omega2, double fx, double fy,
+                    double fz);
+
+/* set_geometry(fn(x, y, z) -> CellType) (:74-82), the result of fn given as
+ * an array over interior nodes.  RegWall / SpecWall / SpecNode cells are not
+ * offered (M3LB_ERR_UNSUPPORTED). */
+int m3lb_set_flags(m3lb_solver* h, const uint8_t* flags);
+
+/* initialize(rho0, ux, uy, uz) (:553-561): equilibrium on fluid nodes, rest
+ * equilibrium at rho0 elsewhere; resets the time step to 0. */
+int m3lb_init_eq(m3lb_solver* h, double rho0, double ux, double uy, double uz);
+
+/* initialize_field(fn(n) -> FlowState) (:568-579), the field given as four
+ * host arrays over interior nodes (x fastest); non-fluid nodes at rest, rho 1. */
+int m3lb_init_field_f32(m3lb_solver* h, const float* rho, const float* ux, const float* uy,
+                        const float* uz);
+int m3lb_init_field_f64(m3lb_solver* h, const double* rho, const double* ux, const double* uy,
+                        const double* uz);
+/* Same, from device arrays of the arithmetic type (float, or double for F64). */
+int m3lb_init_field_device(m3lb_solver* h, const void* rho, const void* ux, const void* uy,
+                           const void* uz);
+
+/* step(store_macroscopic) (:582-591), nsteps times: one fused stream-collide
+ * kernel per step.  store_macro != 0 writes rho, u of fluid nodes (the last
+ * step's values remain).  Asynchronous. */
+int m3lb_step(m3lb_solver* h, int nsteps, int store_macro);
+
+/* compute_macroscopic() + rho()/ux()/uy()/uz() (:597-599, :611-614): fields of
+ * every interior node at the current time (non-fluid nodes 0), to host. */
+int m3lb_macro_f32(m3lb_solver* h, float* rho, float* ux, float* uy, float* uz);
+int m3lb_macro_f64(m3lb_solver* h, double* rho, double* ux, double* uy, double* uz);
+/* The fields as last written (by step(store_macro) or a macro call), without
+ * recomputing: the reference's rho()/ux()/uy()/uz() views (:611-614). */
+int m3lb_stored_macro_f64(m3lb_solver* h, double* rho, double* ux, double* uy, double* uz);
+/* compute_macroscopic() into device memory; *rho.. receive device pointers to
+ * arrays of the arithmetic type owned by the handle.  Asynchronous. */
+int m3lb_macro_device(m3lb_solver* h, void** rho, void** ux, void** uy, void** uz);
+
+/* total_mass() / total_momentum(a) (:601-606) summed in FP64 on the device:
+ * out[0] mass, out[1..3] momentum, out[4] kinetic energy sum(rho |u|^2 / 2)
+ * over fluid nodes, out[5] sum of every stored population slot
+ * (EsotericPull::storage(), src/memory/EsotericPull.hpp:119-123). */
+int m3lb_reduce(m3lb_solver* h, double out[6]);
+
+/* gather_populations() (:620-624): logical populations, n_padded x Q,
+ * node-major, as double, or as raw storage elements. */
+int m3lb_gather(m3lb_solver* h, double* out);
+int m3lb_gather_raw(m3lb_solver* h, void* out);
+/* seed_populations(fn(n, i)) (:634-637), exact inverse of gather. */
+int m3lb_scatter(m3lb_solver* h, const double* in);
+int m3lb_scatter_raw(m3lb_solver* h, const void* in);
+
+/* timestep() (:617), domain() extents (:608): dims receives
+ * {nx, ny, nz, hx, hy, hz, sx, sy, sz, pitch, Q, storage}. */
+int m3lb_timestep(const m3lb_solver* h, long long* t);
+int m3lb_dims(const m3lb_solver* h, int dims[12]);
+/* populations() (:609): device pointer and byte size of the population array
+ * (row-blocked layout: element (x,y,z,q) at ((z*sy+y)*Q+q)*pitch + x). */
+int m3lb_populations(const m3lb_solver* h, void** ptr, size_t* bytes);
+
+/* Queue the handle's work on `stream` (a cudaStream_t; NULL = legacy default). */
+int m3lb_set_stream(m3lb_solver* h, void* stream);
+int m3lb_sync(m3lb_solver* h);
+int m3lb_set_option(m3lb_solver* h, int option, int value);
+/* Kernel launches queued by this handle since creation. */
+int m3lb_launch_count(const m3lb_solver* h, long long* n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* M3LB_H */

@@ -1,0 +1,103 @@
+"""ctypes binding of ``libm3lb.so`` (declarations in ``include/m3lb.h``).
+
+The library is built in-tree (``python -m m3lb_b200.build``).  Loading fails
+loudly when it is missing: there is no fallback implementation.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "libm3lb.so"
+HEADER = Path(__file__).resolve().parent.parent / "include" / "m3lb.h"
+
+OK = 0
+ERR_INVALID = -1
+ERR_UNSUPPORTED = -2
+ERR_CUDA = -3
+ERR_MEMORY = -4
+
+OP_NONE, OP_BGK, OP_TRT, OP_MRT, OP_CM = 0, 1, 2, 3, 4
+EQ_SECOND_ORDER, EQ_PRODUCT_FORM = 0, 1
+STORE_F32, STORE_F16, STORE_BF16, STORE_F64 = 0, 1, 2, 3
+OPT_NODE_KERNEL = 1
+
+STORAGE_NAMES = {"f32": STORE_F32, "f16": STORE_F16, "bf16": STORE_BF16, "f64": STORE_F64}
+STORAGE_BYTES = {STORE_F32: 4, STORE_F16: 2, STORE_BF16: 2, STORE_F64: 8}
+
+
+class M3lbError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"m3lb error {code}: {msg}")
+        self.code = code
+
+
+_vp = C.c_void_p
+_i = C.c_int
+_d = C.c_double
+_pp = C.POINTER(C.c_void_p)
+
+# name -> (restype, argtypes); every entry point of include/m3lb.h
+SIGNATURES = {
+    "m3lb_last_error": (C.c_char_p, []),
+    "m3lb_footprint": (_i, [_i] * 8 + [C.POINTER(C.c_size_t)]),
+    "m3lb_create": (_i, [_i] * 12 + [_pp]),
+    "m3lb_destroy": (_i, [_vp]),
+    "m3lb_set_params": (_i, [_vp] + [_d] * 5),
+    "m3lb_set_flags": (_i, [_vp, _vp]),
+    "m3lb_init_eq": (_i, [_vp] + [_d] * 4),
+    "m3lb_init_field_f32": (_i, [_vp] + [_vp] * 4),
+    "m3lb_init_field_f64": (_i, [_vp] + [_vp] * 4),
+    "m3lb_init_field_device": (_i, [_vp] + [_vp] * 4),
+    "m3lb_step": (_i, [_vp, _i, _i]),
+    "m3lb_macro_f32": (_i, [_vp] + [_vp] * 4),
+    "m3lb_macro_f64": (_i, [_vp] + [_vp] * 4),
+    "m3lb_stored_macro_f64": (_i, [_vp] + [_vp] * 4),
+    "m3lb_macro_device": (_i, [_vp] + [_pp] * 4),
+    "m3lb_reduce": (_i, [_vp, _vp]),
+    "m3lb_gather": (_i, [_vp, _vp]),
+    "m3lb_gather_raw": (_i, [_vp, _vp]),
+    "m3lb_scatter": (_i, [_vp, _vp]),
+    "m3lb_scatter_raw": (_i, [_vp, _vp]),
+    "m3lb_timestep": (_i, [_vp, C.POINTER(C.c_longlong)]),
+    "m3lb_dims": (_i, [_vp, C.POINTER(C.c_int)]),
+    "m3lb_populations": (_i, [_vp, _pp, C.POINTER(C.c_size_t)]),
+    "m3lb_set_stream": (_i, [_vp, _vp]),
+    "m3lb_sync": (_i, [_vp]),
+    "m3lb_set_option": (_i, [_vp, _i, _i]),
+    "m3lb_launch_count": (_i, [_vp, C.POINTER(C.c_longlong)]),
+}
+
+_lib = None
+
+
+def lib():
+    """Load libm3lb.so once; raise if it is not built."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise FileNotFoundError(
+                f"{LIB_PATH} is not built; run `python -m m3lb_b200.build` (nvcc, sm_100a)")
+        L = C.CDLL(str(LIB_PATH))
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def last_error() -> str:
+    return lib().m3lb_last_error().decode()
+
+
+def check(rc: int) -> None:
+    if rc != OK:
+        raise M3lbError(rc, last_error())
+
+
+def footprint(lattice, nx, ny, nz, px=True, py=True, pz=True, storage=STORE_F32) -> int:
+    out = C.c_size_t(0)
+    check(lib().m3lb_footprint(lattice, nx, ny, nz, int(px), int(py), int(pz), storage,
+                               C.byref(out)))
+    return int(out.value)

@@ -1,0 +1,228 @@
+// Lattice descriptors, storage formats and the arithmetic vocabulary shared by
+// every kernel of the M3LB lattice-Boltzmann step on sm_100a.
+//
+// Velocity sets keep the reference's Esoteric-Pull ordering
+// (src/lattice/Lattices.hpp:75-159): rest first, then opposite directions at
+// adjacent indices, opp(i) = i+1 for odd i.  The order is part of the storage
+// contract (it decides which slot a population sits in), so it is the
+// reference's order exactly.
+#pragma once
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace m3lb {
+
+// ---------------------------------------------------------------- lattices
+struct D2Q9 {
+  static constexpr int Q = 9, D = 2, WDEN = 36;
+  static constexpr int cx[9] = {0, 1, -1, 0, 0, 1, -1, 1, -1};
+  static constexpr int cy[9] = {0, 0, 0, 1, -1, 1, -1, -1, 1};
+  static constexpr int cz[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  static constexpr int wn[9] = {16, 4, 4, 4, 4, 1, 1, 1, 1};
+};
+struct D3Q27 {
+  static constexpr int Q = 27, D = 3, WDEN = 216;
+  static constexpr int cx[27] = {0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1,
+                                 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, -1, 1};
+  static constexpr int cy[27] = {0, 0, 0, 1, -1, 0, 0, 1, -1, -1, 1, 0, 0, 0, 0,
+                                 1, -1, 1, -1, 1, -1, 1, -1, -1, 1, 1, -1};
+  static constexpr int cz[27] = {0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, -1, -1, 1,
+                                 1, -1, -1, 1, 1, -1, -1, 1, 1, -1, 1, -1};
+  static constexpr int wn[27] = {64, 16, 16, 16, 16, 16, 16, 4, 4, 4, 4, 4, 4, 4,
+                                 4,  4,  4,  4,  4,  1,  1,  1, 1, 1, 1, 1, 1};
+};
+
+template <class L>
+__host__ __device__ constexpr int cvel(int i, int a) {
+  return a == 0 ? L::cx[i] : (a == 1 ? L::cy[i] : L::cz[i]);
+}
+// Direction with the given velocity components (each in -1..1), or -1.
+template <class L>
+__host__ __device__ constexpr int dir_of(int x, int y, int z) {
+  for (int i = 0; i < L::Q; ++i)
+    if (L::cx[i] == x && L::cy[i] == y && L::cz[i] == z) return i;
+  return -1;
+}
+
+// ---------------------------------------------------------- storage formats
+// Population storage: the element type in HBM.  Arithmetic is FP32 for the
+// 32- and 16-bit formats and FP64 for the 64-bit one.
+enum Store : int { kF32 = 0, kF16 = 1, kBF16 = 2, kF64 = 3 };
+
+template <int S> struct StoreT;
+template <> struct StoreT<kF32> {
+  using elem = float;  using word = float2;  using real = float;  using half_word = float;
+};
+template <> struct StoreT<kF64> {
+  using elem = double; using word = double2; using real = double; using half_word = double;
+};
+template <> struct StoreT<kF16> {
+  using elem = __half; using word = uint32_t; using real = float; using half_word = uint16_t;
+};
+template <> struct StoreT<kBF16> {
+  using elem = __nv_bfloat16; using word = uint32_t; using real = float; using half_word = uint16_t;
+};
+
+// ------------------------------------------------------ packed arithmetic
+// Two adjacent nodes are updated together with sm_100's paired FP32 ops
+// (add/mul/fma .f32x2), one instruction for both lanes.  Every operation is
+// an explicitly rounded IEEE op (no contraction left to the compiler), so the
+// paired path and the one-node path give bitwise identical results.
+struct f2 { float2 v; };
+
+__device__ __forceinline__ f2 mk(float a, float b) { return f2{make_float2(a, b)}; }
+__device__ __forceinline__ f2 splat2(float a) { return f2{make_float2(a, a)}; }
+__device__ __forceinline__ f2 add(f2 a, f2 b) { return f2{__fadd2_rn(a.v, b.v)}; }
+__device__ __forceinline__ f2 mul(f2 a, f2 b) { return f2{__fmul2_rn(a.v, b.v)}; }
+__device__ __forceinline__ f2 fma(f2 a, f2 b, f2 c) { return f2{__ffma2_rn(a.v, b.v, c.v)}; }
+// a - b as a + (-1)*b in one fused op: exactly the IEEE difference.
+__device__ __forceinline__ f2 sub(f2 a, f2 b) { return f2{__ffma2_rn(b.v, make_float2(-1.f, -1.f), a.v)}; }
+__device__ __forceinline__ f2 neg(f2 a) { return f2{make_float2(-a.v.x, -a.v.y)}; }
+__device__ __forceinline__ f2 rcp(f2 a) { return f2{make_float2(__frcp_rn(a.v.x), __frcp_rn(a.v.y))}; }
+
+__device__ __forceinline__ float add(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float fma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ float sub(float a, float b) { return __fmaf_rn(b, -1.f, a); }
+__device__ __forceinline__ float neg(float a) { return -a; }
+__device__ __forceinline__ float rcp(float a) { return __frcp_rn(a); }
+
+__device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double fma(double a, double b, double c) { return __fma_rn(a, b, c); }
+__device__ __forceinline__ double sub(double a, double b) { return __fma_rn(b, -1.0, a); }
+__device__ __forceinline__ double neg(double a) { return -a; }
+__device__ __forceinline__ double rcp(double a) { return __drcp_rn(a); }
+
+template <class V> struct Lanes;
+template <> struct Lanes<f2> { using S = float; static constexpr int N = 2; };
+template <> struct Lanes<float> { using S = float; static constexpr int N = 1; };
+template <> struct Lanes<double> { using S = double; static constexpr int N = 1; };
+
+template <class V> __device__ __forceinline__ V bc(typename Lanes<V>::S a);
+template <> __device__ __forceinline__ f2 bc<f2>(float a) { return splat2(a); }
+template <> __device__ __forceinline__ float bc<float>(float a) { return a; }
+template <> __device__ __forceinline__ double bc<double>(double a) { return a; }
+
+// Lane access for the paired type (lane 0 = lower x).
+__device__ __forceinline__ float lane_of(f2 a, int k) { return k ? a.v.y : a.v.x; }
+__device__ __forceinline__ float lane_of(float a, int) { return a; }
+__device__ __forceinline__ double lane_of(double a, int) { return a; }
+
+// -------------------------------------------- word <-> paired conversion
+// A "word" is the storage of two x-adjacent nodes of one direction.
+__device__ __forceinline__ f2 unpack(float2 w) { return f2{w}; }
+__device__ __forceinline__ float2 pack_f32(f2 v) { return v.v; }
+
+__device__ __forceinline__ f2 unpack_f16(uint32_t w) {
+  __half2 h = *reinterpret_cast<__half2*>(&w);
+  return f2{__half22float2(h)};
+}
+__device__ __forceinline__ uint32_t pack_f16(f2 v) {
+  __half2 h = __float22half2_rn(v.v);
+  return *reinterpret_cast<uint32_t*>(&h);
+}
+__device__ __forceinline__ f2 unpack_bf16(uint32_t w) {
+  return f2{make_float2(__uint_as_float(w << 16), __uint_as_float(w & 0xffff0000u))};
+}
+__device__ __forceinline__ uint32_t pack_bf16(f2 v) {
+  __nv_bfloat162 h = __float22bfloat162_rn(v.v);
+  return *reinterpret_cast<uint32_t*>(&h);
+}
+
+// Scalar element <-> arithmetic type.
+__device__ __forceinline__ float to_real(float e) { return e; }
+__device__ __forceinline__ double to_real(double e) { return e; }
+__device__ __forceinline__ float to_real(__half e) { return __half2float(e); }
+__device__ __forceinline__ float to_real(__nv_bfloat16 e) { return __bfloat162float(e); }
+template <class E> __device__ __forceinline__ E from_real(float v);
+template <class E> __device__ __forceinline__ E from_real(double v);
+template <> __device__ __forceinline__ float from_real<float>(float v) { return v; }
+template <> __device__ __forceinline__ double from_real<double>(double v) { return v; }
+template <> __device__ __forceinline__ __half from_real<__half>(float v) { return __float2half_rn(v); }
+template <> __device__ __forceinline__ __nv_bfloat16 from_real<__nv_bfloat16>(float v) {
+  return __float2bfloat16_rn(v);
+}
+template <> __device__ __forceinline__ double from_real<double>(float v) { return (double)v; }
+template <> __device__ __forceinline__ float from_real<float>(double v) { return (float)v; }
+template <> __device__ __forceinline__ __half from_real<__half>(double v) { return __double2half(v); }
+template <> __device__ __forceinline__ __nv_bfloat16 from_real<__nv_bfloat16>(double v) {
+  return __double2bfloat16(v);
+}
+
+// ------------------------------------------------------------ geometry
+// Padded block, x fastest, with a halo only along non-periodic axes
+// (src/grid/Domain.hpp:37-56).  Populations are stored in x-chunks of
+// kChunk = 64 nodes: every padded row (y, z) is cut into nch chunks, and a
+// chunk holds its Q direction segments one after the other:
+//   element (x, y, z, q) at (((z*sy + y)*nch + x/64)*Q + q)*64 + x%64.
+// One warp updates one chunk (32 lanes x 2 nodes), so each of its loads and
+// stores is one contiguous segment, and every direction sits at a
+// compile-time offset from the chunk start.
+constexpr int kChunk = 64;
+
+struct Geo {
+  int nx, ny, nz;     // interior extents
+  int hx, hy, hz;     // halo widths
+  int sx, sy, sz;     // padded extents
+  int px, py, pz;     // periodic flags
+  int nch;            // chunks per padded row, ceil(sx / 64)
+  long long n_padded; // sx*sy*sz
+};
+
+// Neighbour coordinate along one axis: periodic axes wrap inside [h, h+n),
+// others clamp into the padded range (Domain.hpp:113-123).
+__host__ __device__ __forceinline__ int shift_coord(int v, int h, int n, int s, int per) {
+  if (per) {
+    if (v < h) return v + n;
+    if (v >= h + n) return v - n;
+    return v;
+  }
+  if (v < 0) return 0;
+  if (v >= s) return s - 1;
+  return v;
+}
+
+// Parameters of one step launch, passed by value.
+struct StepArgs {
+  Geo g;
+  void* f;                 // populations
+  const uint8_t* flags;    // per padded node (0 fluid); nullptr: all interior fluid
+  void* rho;               // macroscopic outputs, per padded node, or nullptr
+  void* ux;
+  void* uy;
+  void* uz;
+  int parity;              // t % 2
+  double omega, omega2;    // BGK/TRT/MRT/CM rates (TRT: omega_p, omega_m; moments: omega, bulk)
+  double fx, fy, fz;       // uniform Guo body force
+};
+
+// Scatter (Access::scatter, EsotericPull.hpp:104-111): write, for node n and
+// direction i, the slot that load(n, i) reads.  mode 0: equilibrium at
+// (rho0, u0) on fluid nodes and at rest elsewhere (initialize,
+// FluidSolver.hpp:553-561); mode 1: per-node interior field arrays, rest at
+// rho = 1 elsewhere (initialize_field :568-579); mode 2: explicit logical
+// populations per padded node (seed_populations :634-637), as double or raw.
+struct SeedArgs {
+  Geo g;
+  void* f;
+  const uint8_t* flags;   // per padded node, never null here
+  int parity;
+  int mode;
+  double rho0, ux0, uy0, uz0;
+  const void* rho;        // mode 1: interior arrays of the arithmetic type
+  const void* ux;
+  const void* uy;
+  const void* uz;
+  const double* pops;     // mode 2 (double)
+  const void* raw;        // mode 2 (storage elements), used when pops == nullptr
+};
+
+// Global reductions: threads per block and values per block partial (mass,
+// momentum x/y/z, kinetic energy, sum of every stored slot).
+constexpr int kReduceThreads = 256;
+constexpr int kReduceVals = 6;
+
+}  // namespace m3lb

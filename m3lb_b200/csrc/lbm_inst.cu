@@ -1,0 +1,134 @@
+// Kernel instantiations and launchers for one (lattice, storage format),
+// selected at compile time:
+//   -DM3LB_LAT=D2Q9|D3Q27 -DM3LB_ST=kF32|kF16|kBF16|kF64 -DM3LB_NAME=launchers_<...>
+#include "lbm_kernels.cuh"
+#include "lbm_launch.h"
+
+#ifndef M3LB_LAT
+#error "M3LB_LAT not defined"
+#endif
+
+namespace m3lb {
+namespace {
+
+using L = M3LB_LAT;
+constexpr int ST = M3LB_ST;
+// 16-bit storage exists only as shifted populations.
+constexpr bool kRawOK = (ST == kF32 || ST == kF64);
+
+inline unsigned blocks_for(long long n, int threads) {
+  return (unsigned)((n + threads - 1) / threads);
+}
+
+template <int OP, int EQ, bool SH, bool FORCE>
+cudaError_t step_t(const StepArgs& a, bool pairs, cudaStream_t s) {
+  const Geo& g = a.g;
+  if (pairs) {
+    // one warp per 64-node chunk of every interior row
+    const long long nthreads = (long long)g.ny * g.nz * g.nch * 32;
+    step_pairs<L, ST, OP, EQ, SH, FORCE><<<blocks_for(nthreads, kPairThreads), kPairThreads, 0, s>>>(a);
+  } else {
+    const long long nn = (long long)g.nx * g.ny * g.nz;
+    step_nodes<L, ST, OP, EQ, SH, FORCE><<<blocks_for(nn, kNodeThreads), kNodeThreads, 0, s>>>(a);
+  }
+  return cudaGetLastError();
+}
+
+template <int OP, int EQ, bool SH>
+cudaError_t step_f(const StepArgs& a, bool force, bool pairs, cudaStream_t s) {
+  return force ? step_t<OP, EQ, SH, true>(a, pairs, s) : step_t<OP, EQ, SH, false>(a, pairs, s);
+}
+template <int OP, int EQ>
+cudaError_t step_s(const StepArgs& a, bool sh, bool force, bool pairs, cudaStream_t s) {
+  if (sh) return step_f<OP, EQ, true>(a, force, pairs, s);
+  if constexpr (kRawOK) return step_f<OP, EQ, false>(a, force, pairs, s);
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t step(const StepArgs& a, int op, int eq, bool sh, bool force, bool pairs,
+                 cudaStream_t s, int* launches) {
+  if (launches) *launches += 1;
+  switch (op) {
+    case 0: return step_t<0, 0, true, false>(a, pairs, s);
+    case 1: return eq ? step_s<1, 1>(a, sh, force, pairs, s) : step_s<1, 0>(a, sh, force, pairs, s);
+    case 2: return eq ? step_s<2, 1>(a, sh, force, pairs, s) : step_s<2, 0>(a, sh, force, pairs, s);
+    case 3: return step_s<3, 0>(a, sh, force, pairs, s);
+    case 4: return step_s<4, 0>(a, sh, force, pairs, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+template <int OP, int EQ, bool SH>
+cudaError_t seed_t(const SeedArgs& a, cudaStream_t s) {
+  seed_kernel<L, ST, OP, EQ, SH><<<blocks_for(a.g.n_padded, 128), 128, 0, s>>>(a);
+  return cudaGetLastError();
+}
+template <int OP, int EQ>
+cudaError_t seed_s(const SeedArgs& a, bool sh, cudaStream_t s) {
+  if (sh) return seed_t<OP, EQ, true>(a, s);
+  if constexpr (kRawOK) return seed_t<OP, EQ, false>(a, s);
+  return cudaErrorInvalidValue;
+}
+cudaError_t seed(const SeedArgs& a, int op, int eq, bool sh, cudaStream_t s) {
+  switch (op) {
+    case 0: return seed_t<0, 0, true>(a, s);
+    case 1:
+    case 2: return eq ? seed_s<1, 1>(a, sh, s) : seed_s<1, 0>(a, sh, s);
+    case 3:
+    case 4: return seed_s<3, 0>(a, sh, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t gather(const Geo& g, const void* f, int parity, double* out, void* raw,
+                   cudaStream_t s) {
+  gather_kernel<L, ST><<<blocks_for(g.n_padded, 128), 128, 0, s>>>(g, f, parity, out, raw);
+  return cudaGetLastError();
+}
+
+// Macroscopic readout depends on the operator only through "none" vs the
+// rest: every collision shares BGK's moment sums (BGK.hpp:63-78).
+template <bool SH, bool FORCE>
+cudaError_t macro_t(const StepArgs& a, int op, cudaStream_t s) {
+  const long long nn = (long long)a.g.nx * a.g.ny * a.g.nz;
+  if (op == 0)
+    macro_kernel<L, ST, 0, true, false><<<blocks_for(nn, 128), 128, 0, s>>>(a);
+  else
+    macro_kernel<L, ST, 1, SH, FORCE><<<blocks_for(nn, 128), 128, 0, s>>>(a);
+  return cudaGetLastError();
+}
+cudaError_t macro(const StepArgs& a, int op, bool sh, bool force, cudaStream_t s) {
+  if (sh) return force ? macro_t<true, true>(a, op, s) : macro_t<true, false>(a, op, s);
+  if constexpr (kRawOK) return force ? macro_t<false, true>(a, op, s) : macro_t<false, false>(a, op, s);
+  return cudaErrorInvalidValue;
+}
+
+template <bool SH, bool FORCE>
+cudaError_t reduce_t(const StepArgs& a, int op, double* partials, int nb, double* out,
+                     cudaStream_t s) {
+  if (op == 0)
+    reduce_kernel<L, ST, 0, true, false><<<nb, kReduceThreads, 0, s>>>(a, partials);
+  else
+    reduce_kernel<L, ST, 1, SH, FORCE><<<nb, kReduceThreads, 0, s>>>(a, partials);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  reduce_finish<<<1, 32, 0, s>>>(partials, nb, out);
+  return cudaGetLastError();
+}
+cudaError_t reduce(const StepArgs& a, int op, bool sh, bool force, double* partials, int nb,
+                   double* out, cudaStream_t s) {
+  if (sh) return force ? reduce_t<true, true>(a, op, partials, nb, out, s)
+                       : reduce_t<true, false>(a, op, partials, nb, out, s);
+  if constexpr (kRawOK)
+    return force ? reduce_t<false, true>(a, op, partials, nb, out, s)
+                 : reduce_t<false, false>(a, op, partials, nb, out, s);
+  return cudaErrorInvalidValue;
+}
+
+const Launchers kTable = {step, seed, gather, macro, reduce};
+
+}  // namespace
+
+const Launchers* M3LB_NAME() { return &kTable; }
+
+}  // namespace m3lb

@@ -1,0 +1,648 @@
+// Kernels of the M3LB lattice-Boltzmann step on sm_100a.
+//
+// Streaming is Esoteric Pull on one population array (src/memory/
+// EsotericPull.hpp:1-111): for every opposite pair (i, i+1), i odd, node n
+// reads and writes exactly two slots, its own slot of direction i+P and the
+// slot of direction i+1-P at node n + c_i (P = t % 2):
+//     f_i     <- own,      f_{i+1} <- remote      (load_pair  :88-91)
+//     remote  <- f_i',     own     <- f_{i+1}'    (store_pair :92-96)
+// Every slot has one reader and one writer, the same node, so the update is in
+// place and race free.  The parity only decides which of the two direction
+// rows is "own": it is folded into two base offsets, so one kernel serves
+// both parities with no per-node cost.
+//
+// Solid and excluded cells do nothing (implicit halfway bounce-back,
+// EsotericPull.hpp:27-33): the paired kernel writes their slots back
+// unchanged, the one-node kernel skips them.
+#pragma once
+#include "lbm_collide.cuh"
+
+namespace m3lb {
+
+constexpr int kPairThreads = 128;
+constexpr int kNodeThreads = 128;
+
+// ------------------------------------------------------- FP64 node pairs
+struct d2 { double x, y; };
+__device__ __forceinline__ d2 add(d2 a, d2 b) { return {__dadd_rn(a.x, b.x), __dadd_rn(a.y, b.y)}; }
+__device__ __forceinline__ d2 mul(d2 a, d2 b) { return {__dmul_rn(a.x, b.x), __dmul_rn(a.y, b.y)}; }
+__device__ __forceinline__ d2 fma(d2 a, d2 b, d2 c) { return {__fma_rn(a.x, b.x, c.x), __fma_rn(a.y, b.y, c.y)}; }
+__device__ __forceinline__ d2 sub(d2 a, d2 b) { return {__fma_rn(b.x, -1.0, a.x), __fma_rn(b.y, -1.0, a.y)}; }
+__device__ __forceinline__ d2 neg(d2 a) { return {-a.x, -a.y}; }
+__device__ __forceinline__ d2 rcp(d2 a) { return {__drcp_rn(a.x), __drcp_rn(a.y)}; }
+template <> struct Lanes<d2> { using S = double; static constexpr int N = 2; };
+template <> __device__ __forceinline__ d2 bc<d2>(double a) { return {a, a}; }
+__device__ __forceinline__ double lane_of(d2 a, int k) { return k ? a.y : a.x; }
+
+// ------------------------------------------------------------ word traits
+// A word holds one direction of two x-adjacent nodes (lo = even x).
+template <int ST> struct WordOps;
+template <> struct WordOps<kF32> {
+  using W = float2; using H = float; using V = f2; using E = float;
+  static __device__ __forceinline__ V unpack(W w) { return f2{w}; }
+  static __device__ __forceinline__ W pack(V v) { return v.v; }
+  static __device__ __forceinline__ H lo(W w) { return w.x; }
+  static __device__ __forceinline__ H hi(W w) { return w.y; }
+  static __device__ __forceinline__ W make(H l, H h) { return make_float2(l, h); }
+};
+template <> struct WordOps<kF64> {
+  using W = double2; using H = double; using V = d2; using E = double;
+  static __device__ __forceinline__ V unpack(W w) { return {w.x, w.y}; }
+  static __device__ __forceinline__ W pack(V v) { return make_double2(v.x, v.y); }
+  static __device__ __forceinline__ H lo(W w) { return w.x; }
+  static __device__ __forceinline__ H hi(W w) { return w.y; }
+  static __device__ __forceinline__ W make(H l, H h) { return make_double2(l, h); }
+};
+template <> struct WordOps<kF16> {
+  using W = uint32_t; using H = uint16_t; using V = f2; using E = __half;
+  static __device__ __forceinline__ V unpack(W w) { return unpack_f16(w); }
+  static __device__ __forceinline__ W pack(V v) { return pack_f16(v); }
+  static __device__ __forceinline__ H lo(W w) { return (H)(w & 0xffffu); }
+  static __device__ __forceinline__ H hi(W w) { return (H)(w >> 16); }
+  static __device__ __forceinline__ W make(H l, H h) { return (W)l | ((W)h << 16); }
+};
+template <> struct WordOps<kBF16> {
+  using W = uint32_t; using H = uint16_t; using V = f2; using E = __nv_bfloat16;
+  static __device__ __forceinline__ V unpack(W w) { return unpack_bf16(w); }
+  static __device__ __forceinline__ W pack(V v) { return pack_bf16(v); }
+  static __device__ __forceinline__ H lo(W w) { return (H)(w & 0xffffu); }
+  static __device__ __forceinline__ H hi(W w) { return (H)(w >> 16); }
+  static __device__ __forceinline__ W make(H l, H h) { return (W)l | ((W)h << 16); }
+};
+
+template <class H>
+__device__ __forceinline__ H shfl_h(H v, int src) { return __shfl_sync(0xffffffffu, v, src); }
+template <>
+__device__ __forceinline__ uint16_t shfl_h<uint16_t>(uint16_t v, int src) {
+  return (uint16_t)__shfl_sync(0xffffffffu, (unsigned)v, src);
+}
+
+// Element offset of slot (x, y, z, q) in the chunked layout.
+template <int Q>
+__device__ __forceinline__ size_t slot(const Geo& g, int x, int y, int z, int q) {
+  return ((((size_t)((long long)z * g.sy + y) * g.nch + (x >> 6)) * Q + q) << 6) + (size_t)(x & 63);
+}
+
+// ---------------------------------------------------- paired step kernel
+// Requires a periodic x axis (no x halo) and even nx.  Warp w owns chunk
+// (row, k) of the interior rows; lane l the node pair x0 = 64k + 2l,
+// x0 + 1.  A direction with c_x = +-1 needs an element of the neighbouring
+// pair: it comes from the adjacent lane by a shuffle, or, across a chunk
+// edge, from one extra element load; the shifted stores are recombined the
+// same way, so every bulk access is an aligned word of a 64-node segment.
+template <class L, int ST>
+struct PairCtx {
+  using WO = WordOps<ST>;
+  using W = typename WO::W;
+  using H = typename WO::H;
+  using E = typename WO::E;
+  static constexpr int Q = L::Q;
+  E* own;           // &A[row, chunk, dir 0 + P, x0 % 64]
+  E* rem[3][3];     // [dz+1][dy+1]: &A[row + (dy,dz), chunk, dir 1 - P, x0 % 64]
+  int nxt_off;      // element offset from this lane's word to x0 + 2 (wrapped), same direction
+  int prv_off;      // element offset from this lane's word to x0 - 1 (wrapped)
+  int nxt_src, prv_src;
+  bool nxt_in, prv_in, active;
+
+  template <int I>
+  __device__ __forceinline__ void load_pair(W& o, W& r) const {
+    constexpr int cx = L::cx[I], cy = L::cy[I], cz = L::cz[I];
+    o = active ? *reinterpret_cast<const W*>(own + I * kChunk) : W{};
+    const E* rp = rem[cz + 1][cy + 1] + I * kChunk;
+    const W w = active ? *reinterpret_cast<const W*>(rp) : W{};
+    if constexpr (cx == 0) {
+      r = w;
+    } else if constexpr (cx > 0) {
+      // elements (x0+1, x0+2): own hi and the next pair's lo
+      H nlo = shfl_h(WO::lo(w), nxt_src);
+      if (active && !nxt_in) nlo = *reinterpret_cast<const H*>(rp + nxt_off);
+      r = WO::make(WO::hi(w), nlo);
+    } else {
+      // elements (x0-1, x0): the previous pair's hi and own lo
+      H phi = shfl_h(WO::hi(w), prv_src);
+      if (active && !prv_in) phi = *reinterpret_cast<const H*>(rp + prv_off);
+      r = WO::make(phi, WO::lo(w));
+    }
+  }
+
+  // f_i' to the remote slot, f_{i+1}' to the own slot.
+  template <int I>
+  __device__ __forceinline__ void store_pair(W out_i, W out_j) const {
+    constexpr int cx = L::cx[I], cy = L::cy[I], cz = L::cz[I];
+    if (active) *reinterpret_cast<W*>(own + I * kChunk) = out_j;
+    E* rp = rem[cz + 1][cy + 1] + I * kChunk;
+    if constexpr (cx == 0) {
+      if (active) *reinterpret_cast<W*>(rp) = out_i;
+    } else if constexpr (cx > 0) {
+      // outputs of (x0, x0+1) land on (x0+1, x0+2)
+      const H phi = shfl_h(WO::hi(out_i), prv_src);
+      if (active) {
+        if (prv_in) *reinterpret_cast<W*>(rp) = WO::make(phi, WO::lo(out_i));
+        else *reinterpret_cast<H*>(rp + 1) = WO::lo(out_i);
+        if (!nxt_in) *reinterpret_cast<H*>(rp + nxt_off) = WO::hi(out_i);
+      }
+    } else {
+      // outputs of (x0, x0+1) land on (x0-1, x0)
+      const H nlo = shfl_h(WO::lo(out_i), nxt_src);
+      if (active) {
+        if (nxt_in) *reinterpret_cast<W*>(rp) = WO::make(WO::hi(out_i), nlo);
+        else *reinterpret_cast<H*>(rp) = WO::hi(out_i);
+        if (!prv_in) *reinterpret_cast<H*>(rp + prv_off) = WO::lo(out_i);
+      }
+    }
+  }
+};
+
+// Element offset, within one direction, from chunk-local position xa of chunk
+// ca to position xb of chunk cb.
+__device__ __forceinline__ int chunk_delta(int Q, int xa, int xb) {
+  return ((xb >> 6) - (xa >> 6)) * Q * kChunk + ((xb & 63) - (xa & 63));
+}
+
+// Resident 128-thread blocks per SM the register allocation must allow:
+// four (<= 128 registers) for the moment operators, three for BGK/TRT, whose
+// per-pair equilibria keep more values live, and for 32-bit pure streaming,
+// two for FP64 pairs, which need twice the registers per value.
+template <int OP, int ST>
+constexpr int pair_min_blocks() {
+  return ST == kF64 ? 2 : ((OP == 1 || OP == 2 || (OP == 0 && ST == kF32)) ? 3 : 4);
+}
+
+template <class L, int ST, int OP, int EQ, bool SH, bool FORCE>
+__global__ void __launch_bounds__(kPairThreads, pair_min_blocks<OP, ST>())
+step_pairs(StepArgs a) {
+  using WO = WordOps<ST>;
+  using W = typename WO::W;
+  using E = typename WO::E;
+  using V = typename WO::V;
+  using S = typename Lanes<V>::S;
+  constexpr int Q = L::Q;
+  const Geo& g = a.g;
+
+  const int lane = threadIdx.x & 31;
+  const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const long long nrows = (long long)g.ny * g.nz;
+  const bool warp_ok = warp < nrows * g.nch;
+  const long long wsafe = warp_ok ? warp : 0;
+  const int row = (int)(wsafe / g.nch);
+  const int k = (int)(wsafe - (long long)row * g.nch);
+  const int x0 = k * kChunk + 2 * lane;
+  const int yi = row % g.ny, zi = row / g.ny;
+  const int py = yi + g.hy, pz = zi + g.hz;
+
+  PairCtx<L, ST> c;
+  c.active = warp_ok && x0 < g.nx;
+  {
+    int nx_ = x0 + 2; if (nx_ >= g.nx) nx_ -= g.nx;
+    int px_ = x0 - 2; if (px_ < 0) px_ += g.nx;
+    c.nxt_in = (nx_ >> 6) == k;
+    c.prv_in = (px_ >> 6) == k;
+    c.nxt_src = c.nxt_in ? ((nx_ & 63) >> 1) : lane;
+    c.prv_src = c.prv_in ? ((px_ & 63) >> 1) : lane;
+    int xn = x0 + 2; if (xn >= g.nx) xn -= g.nx;
+    int xp = x0 - 1; if (xp < 0) xp += g.nx;
+    c.nxt_off = chunk_delta(Q, x0, xn);
+    c.prv_off = chunk_delta(Q, x0, xp);
+    E* A = reinterpret_cast<E*>(a.f);
+    const int P = a.parity;
+    int yy[3], zz[3];
+#pragma unroll
+    for (int d = -1; d <= 1; ++d) {
+      yy[d + 1] = shift_coord(py + d, g.hy, g.ny, g.sy, g.py);
+      zz[d + 1] = (L::D == 3) ? shift_coord(pz + d, g.hz, g.nz, g.sz, g.pz) : pz;
+    }
+    const int xl = x0 & 63;
+#pragma unroll
+    for (int dz = 0; dz < 3; ++dz)
+#pragma unroll
+      for (int dy = 0; dy < 3; ++dy)
+        c.rem[dz][dy] = A + slot<Q>(g, k * kChunk, yy[dy], zz[dz], 1 - P) + xl;
+    c.own = A + slot<Q>(g, k * kChunk, py, pz, P) + xl;
+  }
+  E* rest = c.own - a.parity * kChunk;
+
+  // ---- load
+  W w[Q];
+  w[0] = c.active ? *reinterpret_cast<const W*>(rest) : W{};
+  static_for<1, Q, 2>([&](auto I) {
+    constexpr int i = decltype(I)::value;
+    c.template load_pair<i>(w[i], w[i + 1]);
+  });
+
+  bool solid0 = false, solid1 = false;
+  Macro<V> m;
+  if constexpr (OP != 0) {
+    V f[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) f[q] = WO::unpack(w[q]);
+
+    // ---- collide
+    const CollideParams<S> prm{(S)a.omega, (S)a.omega2, (S)a.fx, (S)a.fy, (S)a.fz};
+    m = collide<L, OP, EQ, SH, FORCE>(f, prm);
+#pragma unroll
+    for (int q = 0; q < Q; ++q) w[q] = WO::pack(f[q]);
+  }
+
+  // ---- solid / excluded nodes write back what they read (the identity)
+  if (a.flags) {
+    const uint16_t fl = c.active ? *reinterpret_cast<const uint16_t*>(
+        a.flags + ((long long)pz * g.sy + py) * g.sx + x0) : 0;
+    solid0 = (fl & 0xffu) != 0;
+    solid1 = (fl >> 8) != 0;
+    if (__any_sync(0xffffffffu, solid0 || solid1)) {
+      auto pick = [&](W vin, W vout) -> W {
+        return WO::make(solid0 ? WO::lo(vin) : WO::lo(vout), solid1 ? WO::hi(vin) : WO::hi(vout));
+      };
+      w[0] = pick(c.active ? *reinterpret_cast<const W*>(rest) : W{}, w[0]);
+      static_for<1, Q, 2>([&](auto I) {
+        constexpr int i = decltype(I)::value;
+        W wo, wr;
+        c.template load_pair<i>(wo, wr);
+        // bounce-back: f_i' = f_{i+1}, f_{i+1}' = f_i, so the stores land in place
+        w[i] = pick(wr, w[i]);
+        w[i + 1] = pick(wo, w[i + 1]);
+      });
+    }
+  }
+
+  // ---- store
+  if (c.active) *reinterpret_cast<W*>(rest) = w[0];
+  static_for<1, Q, 2>([&](auto I) {
+    constexpr int i = decltype(I)::value;
+    c.template store_pair<i>(w[i], w[i + 1]);
+  });
+
+  if constexpr (OP != 0) {
+    if (a.rho && c.active) {
+      using R = S;
+      const size_t kk = ((size_t)zi * g.ny + yi) * g.nx + x0;
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        if (e == 0 ? solid0 : solid1) continue;
+        reinterpret_cast<R*>(a.rho)[kk + e] = (R)lane_of(m.rho, e);
+        reinterpret_cast<R*>(a.ux)[kk + e] = (R)lane_of(m.ux, e);
+        reinterpret_cast<R*>(a.uy)[kk + e] = (R)lane_of(m.uy, e);
+        reinterpret_cast<R*>(a.uz)[kk + e] = (R)lane_of(m.uz, e);
+      }
+    }
+  }
+}
+
+// -------------------------------------------------- one-node step kernel
+// Any geometry: full neighbour arithmetic of Domain::fill_neighbours
+// (Domain.hpp:82-101) per node.  Used where the paired kernel does not apply
+// (non-periodic x, odd nx).
+template <class L>
+struct NodeNb {
+  int x, y, z;
+  int nb[L::Q][3];  // neighbour coordinates for odd i
+};
+template <class L>
+__device__ __forceinline__ void node_neighbours(const Geo& g, int x, int y, int z, NodeNb<L>& nb) {
+  nb.x = x; nb.y = y; nb.z = z;
+  static_for<1, L::Q, 2>([&](auto I) {
+    constexpr int i = decltype(I)::value;
+    constexpr int cx = L::cx[i], cy = L::cy[i], cz = L::cz[i];
+    nb.nb[i][0] = shift_coord(x + cx, g.hx, g.nx, g.sx, g.px);
+    nb.nb[i][1] = shift_coord(y + cy, g.hy, g.ny, g.sy, g.py);
+    nb.nb[i][2] = shift_coord(z + cz, g.hz, g.nz, g.sz, g.pz);
+  });
+}
+// Access::load(nb, i) (EsotericPull.hpp:69-77): slot holding the population of
+// direction i about to arrive at the node.
+template <class L>
+__device__ __forceinline__ size_t load_slot(const Geo& g, const NodeNb<L>& nb, int par, int i) {
+  if (i == 0) return slot<L::Q>(g, nb.x, nb.y, nb.z, 0);
+  if (i & 1) return slot<L::Q>(g, nb.x, nb.y, nb.z, par == 0 ? i : i + 1);
+  const int* m = nb.nb[i - 1];
+  return slot<L::Q>(g, m[0], m[1], m[2], par == 0 ? i : i - 1);
+}
+
+template <class L, int ST, int OP, int EQ, bool SH, bool FORCE>
+__global__ void __launch_bounds__(kNodeThreads)
+step_nodes(StepArgs a) {
+  using E = typename StoreT<ST>::elem;
+  using R = typename StoreT<ST>::real;
+  constexpr int Q = L::Q;
+  const Geo& g = a.g;
+  const long long nint = (long long)g.nx * g.ny * g.nz;
+  const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nint) return;
+  const int xi = (int)(k % g.nx), yi = (int)((k / g.nx) % g.ny), zi = (int)(k / ((long long)g.nx * g.ny));
+  const int x = xi + g.hx, y = yi + g.hy, z = zi + g.hz;
+  if (a.flags && a.flags[((long long)z * g.sy + y) * g.sx + x] != 0) return;
+  NodeNb<L> nb;
+  node_neighbours<L>(g, x, y, z, nb);
+  E* A = reinterpret_cast<E*>(a.f);
+  const int P = a.parity;
+  R f[Q];
+  f[0] = to_real(A[slot<Q>(g, x, y, z, 0)]);
+#pragma unroll
+  for (int i = 1; i < Q; i += 2) {
+    const int* m = nb.nb[i];
+    f[i] = to_real(A[slot<Q>(g, x, y, z, i + P)]);
+    f[i + 1] = to_real(A[slot<Q>(g, m[0], m[1], m[2], i + 1 - P)]);
+  }
+  const CollideParams<R> prm{(R)a.omega, (R)a.omega2, (R)a.fx, (R)a.fy, (R)a.fz};
+  const Macro<R> mc = collide<L, OP, EQ, SH, FORCE>(f, prm);
+  A[slot<Q>(g, x, y, z, 0)] = from_real<E>(f[0]);
+#pragma unroll
+  for (int i = 1; i < Q; i += 2) {
+    const int* m = nb.nb[i];
+    A[slot<Q>(g, m[0], m[1], m[2], i + 1 - P)] = from_real<E>(f[i]);
+    A[slot<Q>(g, x, y, z, i + P)] = from_real<E>(f[i + 1]);
+  }
+  if (a.rho) {
+    reinterpret_cast<R*>(a.rho)[k] = mc.rho;
+    reinterpret_cast<R*>(a.ux)[k] = mc.ux;
+    reinterpret_cast<R*>(a.uy)[k] = mc.uy;
+    reinterpret_cast<R*>(a.uz)[k] = mc.uz;
+  }
+}
+
+// ------------------------------------------------------- initialisation
+// seed_value (BGK.hpp:95-99, TRT.hpp:129-133, MomentCollision.hpp:320-330)
+// evaluated in the reference's operation order, one rounding per operation.
+template <class L, int OP, int EQ, bool SH, class R>
+__device__ __forceinline__ void seed_all(R rho, R ux, R uy, R uz, R* out) {
+  if constexpr (OP == 0) {
+#pragma unroll
+    for (int i = 0; i < L::Q; ++i) out[i] = rho;
+  } else if constexpr (OP == 1 || OP == 2) {
+    static_for<0, L::Q>([&](auto I) {
+      constexpr int i = decltype(I)::value;
+      constexpr int icx = L::cx[i], icy = L::cy[i], icz = L::cz[i], iwn = L::wn[i];
+      const R cx = (R)icx, cy = (R)icy, cz = (R)icz;
+      R phi;
+      if constexpr (EQ == 0) {
+        const R ics2 = R(3);
+        const R cu = add(add(mul(cx, ux), mul(cy, uy)), mul(cz, uz));
+        const R uu = add(add(mul(ux, ux), mul(uy, uy)), mul(uz, uz));
+        phi = sub(add(mul(ics2, cu), mul(mul(R(4.5), cu), cu)), mul(R(1.5), uu));
+      } else if constexpr (L::D == 2) {
+        const R cs2v = R(1) / R(3);
+        const R ax = sub(mul(cx, cx), cs2v), ay = sub(mul(cy, cy), cs2v);
+        const R o1 = add(mul(cx, ux), mul(cy, uy)) / cs2v;
+        const R o2 = add(add(mul(mul(ax, ux), ux), mul(mul(ay, uy), uy)),
+                         mul(mul(mul(mul(R(2), cx), cy), ux), uy)) /
+                     mul(mul(R(2), cs2v), cs2v);
+        const R o3 = add(mul(mul(mul(mul(ax, cy), ux), ux), uy),
+                         mul(mul(mul(mul(ay, cx), ux), uy), uy)) /
+                     mul(mul(mul(R(2), cs2v), cs2v), cs2v);
+        const R o4 = mul(mul(mul(mul(mul(ax, ay), ux), ux), uy), uy) /
+                     mul(mul(mul(mul(R(4), cs2v), cs2v), cs2v), cs2v);
+        phi = add(add(add(o1, o2), o3), o4);
+      } else {
+        constexpr int c3[3] = {icx, icy, icz};
+        const R u3[3] = {ux, uy, uz};
+        R ch[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+          ch[a] = c3[a] == 0 ? sub(R(1), mul(mul(R(1.5), u3[a]), u3[a]))
+                             : add(R(1), mul(mul(R(3), u3[a]), add((R)c3[a], u3[a])));
+        phi = sub(mul(mul(ch[0], ch[1]), ch[2]), R(1));
+      }
+      const R w = (R)iwn / (R)L::WDEN;
+      if constexpr (SH) {
+        const R drho = sub(rho, R(1));
+        out[i] = mul(w, add(drho, mul(add(R(1), drho), phi)));
+      } else {
+        out[i] = mul(mul(w, rho), add(R(1), phi));
+      }
+    });
+  } else {
+    // inverse transform of the equilibrium moments at u_b = 0
+    constexpr int D = L::D;
+    constexpr int NM = D == 3 ? 27 : 9;
+    const R du[3] = {ux, uy, uz};
+    R k[27];
+#pragma unroll
+    for (int n = 0; n < NM; ++n) {
+      const int p = D == 3 ? n / 9 : n / 3, q = D == 3 ? (n / 3) % 3 : n % 3, r = D == 3 ? n % 3 : 0;
+      const R Qx = p == 0 ? R(1) : (p == 1 ? du[0] : mul(du[0], du[0]));
+      const R Qy = q == 0 ? R(1) : (q == 1 ? du[1] : mul(du[1], du[1]));
+      const R Qz = r == 0 ? R(1) : (r == 1 ? du[2] : mul(du[2], du[2]));
+      R e = mul(mul(rho, Qx), Qy);
+      if (D == 3) e = mul(e, Qz);
+      const R wv = (n == 0) ? R(1) : R(0);
+      k[n] = SH ? sub(e, wv) : e;
+    }
+    const R cs2v = R(1) / R(3);
+    auto inv0 = [&](R& a0, R& b0, R& c0) {
+      const R m0 = a0, m1 = b0, m2 = c0;
+      const R s1 = m1;
+      const R s2 = sub(m2, mul(sub(R(0), cs2v), m0));
+      a0 = mul(R(0.5), sub(s2, s1));
+      b0 = sub(m0, s2);
+      c0 = mul(R(0.5), add(s2, s1));
+    };
+    if constexpr (D == 3) {
+#pragma unroll
+      for (int qr = 0; qr < 9; ++qr) inv0(k[qr], k[9 + qr], k[18 + qr]);
+#pragma unroll
+      for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int r = 0; r < 3; ++r) inv0(k[a * 9 + r], k[a * 9 + 3 + r], k[a * 9 + 6 + r]);
+#pragma unroll
+      for (int ab = 0; ab < 9; ++ab) inv0(k[ab * 3], k[ab * 3 + 1], k[ab * 3 + 2]);
+      static_for<0, 27>([&](auto NN) {
+        constexpr int n = decltype(NN)::value;
+        out[dir_of<L>(n / 9 - 1, (n / 3) % 3 - 1, n % 3 - 1)] = k[n];
+      });
+    } else {
+#pragma unroll
+      for (int q = 0; q < 3; ++q) inv0(k[q], k[3 + q], k[6 + q]);
+#pragma unroll
+      for (int a = 0; a < 3; ++a) inv0(k[a * 3], k[a * 3 + 1], k[a * 3 + 2]);
+      static_for<0, 9>([&](auto NN) {
+        constexpr int n = decltype(NN)::value;
+        out[dir_of<L>(n / 3 - 1, n % 3 - 1, 0)] = k[n];
+      });
+    }
+  }
+}
+
+// Does node coordinate v own slot target t = shift(v + c) when several nodes
+// map onto t?  Only the clamped (non-periodic) axes can collide; the
+// reference's sequential scatter leaves the value of the highest node index,
+// i.e. the largest preimage on every axis.
+__device__ __forceinline__ bool axis_winner(int v, int c, int t, int per, int s) {
+  if (per || c == 0) return true;
+  if (c > 0) return v == ((t == s - 1) ? s - 1 : t - 1);
+  return v == ((t == 0) ? min(1, s - 1) : t + 1);
+}
+
+
+template <class L, int ST, int OP, int EQ, bool SH>
+__global__ void seed_kernel(SeedArgs a) {
+  using E = typename StoreT<ST>::elem;
+  using R = typename StoreT<ST>::real;
+  constexpr int Q = L::Q;
+  const Geo& g = a.g;
+  const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= g.n_padded) return;
+  const int x = (int)(n % g.sx), y = (int)((n / g.sx) % g.sy), z = (int)(n / ((long long)g.sx * g.sy));
+  const bool fluid = a.flags[n] == 0;
+  R rho = (R)a.rho0, ux = 0, uy = 0, uz = 0;
+  if (a.mode == 0) {
+    if (fluid) { ux = (R)a.ux0; uy = (R)a.uy0; uz = (R)a.uz0; }
+  } else if (a.mode == 1) {
+    rho = R(1);
+    if (fluid) {
+      const size_t k = ((size_t)(z - g.hz) * g.ny + (y - g.hy)) * g.nx + (x - g.hx);
+      rho = reinterpret_cast<const R*>(a.rho)[k];
+      ux = reinterpret_cast<const R*>(a.ux)[k];
+      uy = reinterpret_cast<const R*>(a.uy)[k];
+      uz = reinterpret_cast<const R*>(a.uz)[k];
+    }
+  }
+  NodeNb<L> nb;
+  node_neighbours<L>(g, x, y, z, nb);
+  E* A = reinterpret_cast<E*>(a.f);
+  const int P = a.parity;
+  R sv[Q];
+  if (a.mode != 2) seed_all<L, OP, EQ, SH, R>(rho, ux, uy, uz, sv);
+  static_for<0, Q>([&](auto I) {
+    constexpr int i = decltype(I)::value;
+    if constexpr (i > 0 && (i & 1) == 0) {
+      constexpr int cx = L::cx[i - 1], cy = L::cy[i - 1], cz = L::cz[i - 1];
+      const int* m = nb.nb[i - 1];
+      if (!axis_winner(x, cx, m[0], g.px, g.sx) || !axis_winner(y, cy, m[1], g.py, g.sy) ||
+          !axis_winner(z, cz, m[2], g.pz, g.sz))
+        return;
+    }
+    const size_t s = load_slot<L>(g, nb, P, i);
+    if (a.mode == 2) {
+      if (a.pops) A[s] = from_real<E>(a.pops[n * Q + i]);
+      else A[s] = reinterpret_cast<const E*>(a.raw)[n * Q + i];
+    } else {
+      A[s] = from_real<E>(sv[i]);
+    }
+  });
+}
+
+// gather_populations (FluidSolver.hpp:620-624, 1243-1253): logical
+// populations of every padded node, as double or as raw storage elements.
+template <class L, int ST>
+__global__ void gather_kernel(Geo g, const void* f, int parity, double* out, void* raw) {
+  using E = typename StoreT<ST>::elem;
+  constexpr int Q = L::Q;
+  const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= g.n_padded) return;
+  const int x = (int)(n % g.sx), y = (int)((n / g.sx) % g.sy), z = (int)(n / ((long long)g.sx * g.sy));
+  NodeNb<L> nb;
+  node_neighbours<L>(g, x, y, z, nb);
+  const E* A = reinterpret_cast<const E*>(f);
+#pragma unroll
+  for (int i = 0; i < Q; ++i) {
+    const E e = A[load_slot<L>(g, nb, parity, i)];
+    if (out) out[n * Q + i] = (double)to_real(e);
+    else reinterpret_cast<E*>(raw)[n * Q + i] = e;
+  }
+}
+
+// compute_macroscopic (FluidSolver.hpp:1041-1179): rho, u of every interior
+// node at the current parity; non-fluid nodes report zeros.
+template <class L, int ST, int OP, bool SH, bool FORCE>
+__global__ void macro_kernel(StepArgs a) {
+  using E = typename StoreT<ST>::elem;
+  using R = typename StoreT<ST>::real;
+  constexpr int Q = L::Q;
+  const Geo& g = a.g;
+  const long long nint = (long long)g.nx * g.ny * g.nz;
+  const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nint) return;
+  const int xi = (int)(k % g.nx), yi = (int)((k / g.nx) % g.ny), zi = (int)(k / ((long long)g.nx * g.ny));
+  const int x = xi + g.hx, y = yi + g.hy, z = zi + g.hz;
+  R* rho = reinterpret_cast<R*>(a.rho);
+  R* ux = reinterpret_cast<R*>(a.ux);
+  R* uy = reinterpret_cast<R*>(a.uy);
+  R* uz = reinterpret_cast<R*>(a.uz);
+  if (a.flags && a.flags[((long long)z * g.sy + y) * g.sx + x] != 0) {
+    rho[k] = ux[k] = uy[k] = uz[k] = R(0);
+    return;
+  }
+  NodeNb<L> nb;
+  node_neighbours<L>(g, x, y, z, nb);
+  const E* A = reinterpret_cast<const E*>(a.f);
+  R f[Q];
+#pragma unroll
+  for (int i = 0; i < Q; ++i) f[i] = to_real(A[load_slot<L>(g, nb, a.parity, i)]);
+  const CollideParams<R> prm{(R)a.omega, (R)a.omega2, (R)a.fx, (R)a.fy, (R)a.fz};
+  const Macro<R> m = macroscopic<L, OP, SH, FORCE>(f, prm);
+  rho[k] = m.rho; ux[k] = m.ux; uy[k] = m.uy; uz[k] = m.uz;
+}
+
+// ------------------------------------------------------------ reductions
+// Global sums in FP64 (total_mass / total_momentum, FluidSolver.hpp:601-606,
+// 1205-1229, plus kinetic energy and the sum over every stored slot).
+// Stage 1 writes one partial per block into a scratch array, stage 2 sums
+// the partials in a fixed order: no atomics, deterministic for a fixed grid.
+
+__device__ __forceinline__ double block_sum(double v, double* sh) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0) sh[w] = v;
+  __syncthreads();
+  double r = 0;
+  if (threadIdx.x == 0)
+    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) r += sh[i];
+  return r;
+}
+
+template <class L, int ST, int OP, bool SH, bool FORCE>
+__global__ void __launch_bounds__(kReduceThreads)
+reduce_kernel(StepArgs a, double* partials) {
+  using E = typename StoreT<ST>::elem;
+  using R = typename StoreT<ST>::real;
+  constexpr int Q = L::Q;
+  __shared__ double sh[kReduceThreads / 32];
+  const Geo& g = a.g;
+  const E* A = reinterpret_cast<const E*>(a.f);
+  double acc[kReduceVals] = {0, 0, 0, 0, 0, 0};
+  const long long nint = (long long)g.nx * g.ny * g.nz;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  const CollideParams<R> prm{(R)a.omega, (R)a.omega2, (R)a.fx, (R)a.fy, (R)a.fz};
+  for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < nint; k += stride) {
+    const int xi = (int)(k % g.nx), yi = (int)((k / g.nx) % g.ny), zi = (int)(k / ((long long)g.nx * g.ny));
+    const int x = xi + g.hx, y = yi + g.hy, z = zi + g.hz;
+    if (a.flags && a.flags[((long long)z * g.sy + y) * g.sx + x] != 0) continue;
+    NodeNb<L> nb;
+    node_neighbours<L>(g, x, y, z, nb);
+    R f[Q];
+#pragma unroll
+    for (int i = 0; i < Q; ++i) f[i] = to_real(A[load_slot<L>(g, nb, a.parity, i)]);
+    const Macro<R> m = macroscopic<L, OP, SH, FORCE>(f, prm);
+    const double r = (double)m.rho, u = (double)m.ux, v = (double)m.uy, w = (double)m.uz;
+    acc[0] += r;
+    acc[1] += r * u;
+    acc[2] += r * v;
+    acc[3] += r * w;
+    acc[4] += 0.5 * r * (u * u + v * v + w * w);
+  }
+  // every stored slot (all padded rows and chunks, all directions, x < sx)
+  const long long nseg = (long long)g.sz * g.sy * g.nch * Q;
+  const long long nslot = nseg * kChunk;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < nslot; e += stride) {
+    const long long seg = e >> 6;
+    const int x = (int)(((seg / Q) % g.nch) * kChunk + (e & 63));
+    if (x < g.sx) acc[5] += (double)to_real(A[e]);
+  }
+#pragma unroll
+  for (int v = 0; v < kReduceVals; ++v) {
+    const double s = block_sum(acc[v], sh);
+    if (threadIdx.x == 0) partials[(size_t)blockIdx.x * kReduceVals + v] = s;
+  }
+}
+
+static __global__ void reduce_finish(const double* partials, int nblocks, double* out) {
+  const int v = threadIdx.x;
+  if (v >= kReduceVals) return;
+  double s = 0;
+  for (int b = 0; b < nblocks; ++b) s += partials[(size_t)b * kReduceVals + v];
+  out[v] = s;
+}
+
+}  // namespace m3lb

@@ -1,0 +1,481 @@
+"""Python mirror of the reference's solver / collision-policy API, on libm3lb.
+
+The names, defaults and argument meanings follow M3LB's C++ headers
+(src/lattice/Lattices.hpp, src/grid/Domain.hpp, src/memory/*,
+src/collision/{BGK,TRT,MomentCollision}.hpp, src/forcing/Forcing.hpp,
+src/boundary/Flags.hpp, src/solver/FluidSolver.hpp), so a reference test or
+driver reads the same here.  Compile-time policies there become constructor
+arguments here; every time step runs in one fused CUDA kernel on the device.
+
+Added over the reference: the storage precision of the populations
+(``storage="f32" | "f16" | "bf16" | "f64"``; arithmetic is FP32, or FP64 for
+"f64"), and a CUDA stream to queue the work on.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import enum
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import capi
+
+# ---------------------------------------------------------------- lattices
+# Lattices.hpp:75-159: rest first, opposite directions at adjacent indices.
+
+
+class D2Q9:
+    name = "D2Q9"
+    D, Q = 2, 9
+    cs2 = 1.0 / 3.0
+    cx = (0, 1, -1, 0, 0, 1, -1, 1, -1)
+    cy = (0, 0, 0, 1, -1, 1, -1, -1, 1)
+    cz = (0,) * 9
+    w = tuple(v / 36.0 for v in (16, 4, 4, 4, 4, 1, 1, 1, 1))
+
+
+class D3Q27:
+    name = "D3Q27"
+    D, Q = 3, 27
+    cs2 = 1.0 / 3.0
+    cx = (0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, -1, 1)
+    cy = (0, 0, 0, 1, -1, 0, 0, 1, -1, -1, 1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, -1, 1, 1, -1)
+    cz = (0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, -1, -1, 1, 1, -1, -1, 1, 1, -1, -1, 1, 1, -1, 1, -1)
+    w = tuple(v / 216.0 for v in (64, 16, 16, 16, 16, 16, 16, 4, 4, 4, 4, 4, 4, 4,
+                                  4, 4, 4, 4, 4, 1, 1, 1, 1, 1, 1, 1, 1))
+
+
+def opp(i: int) -> int:
+    """Esoteric-Pull pairing rule (Lattices.hpp:43-45)."""
+    return 0 if i == 0 else (i + 1 if i & 1 else i - 1)
+
+
+# ---------------------------------------------------------------- domain
+class Domain:
+    """Cartesian block (Domain.hpp:37-123): halo only along non-periodic axes,
+    padded index idp = (pz*sy + py)*sx + px."""
+
+    def __init__(self, nx, ny, nz=1, px=True, py=True, pz=True, mpi_halo=0):
+        if mpi_halo:
+            raise NotImplementedError("mpi_halo: distributed slabs are not offered")
+        self.nx, self.ny, self.nz = int(nx), int(ny), int(nz)
+        self.periodic = [bool(px), bool(py), bool(pz)]
+
+        def halo(n, per):
+            return 0 if n <= 1 else (0 if per else 1)
+
+        self.hx, self.hy, self.hz = halo(nx, px), halo(ny, py), halo(nz, pz)
+        self.sx, self.sy, self.sz = nx + 2 * self.hx, ny + 2 * self.hy, nz + 2 * self.hz
+        self.n_padded = self.sx * self.sy * self.sz
+
+    def n_interior(self):
+        return self.nx * self.ny * self.nz
+
+    def idp(self, px, py, pz=0):
+        return (pz * self.sy + py) * self.sx + px
+
+    def id(self, x, y, z=0):
+        return self.idp(x + self.hx, y + self.hy, z + self.hz)
+
+    def coords(self, n):
+        return n % self.sx, (n // self.sx) % self.sy, n // (self.sx * self.sy)
+
+    def is_interior(self, px, py, pz):
+        return (self.hx <= px < self.hx + self.nx and self.hy <= py < self.hy + self.ny
+                and self.hz <= pz < self.hz + self.nz)
+
+
+class CellType(enum.IntEnum):
+    """Flags.hpp:20-33."""
+    Fluid = 0
+    Solid = 1
+    Excluded = 2
+    RegWall = 3
+    SpecWall = 4
+    SpecNode = 5
+
+
+# ---------------------------------------------------------------- policies
+class RawPopulations:
+    name, shifted = "raw", False
+
+
+class ShiftedPopulations:
+    name, shifted = "shifted", True
+
+
+class EsotericPull:
+    """In-place single-array streaming (EsotericPull.hpp); the only scheme the
+    device path runs."""
+    name = "EsotericPull"
+    implicit_bounce_back = True
+
+
+class SecondOrderEquilibrium:
+    name, code = "SecondOrder", capi.EQ_SECOND_ORDER
+
+
+class ProductFormEquilibrium:
+    name, code = "ProductForm", capi.EQ_PRODUCT_FORM
+
+
+HighOrderEquilibrium = ProductFormEquilibrium
+
+
+@dataclass
+class NoForcing:
+    name = "None"
+    active = False
+
+
+@dataclass
+class Guo:
+    """Uniform Guo body force (Forcing.hpp:58-82)."""
+    fx: float = 0.0
+    fy: float = 0.0
+    fz: float = 0.0
+    name = "Guo"
+    active = True
+
+
+def _store(s):
+    return s.shifted if hasattr(s, "shifted") else bool(s)
+
+
+@dataclass
+class BGK:
+    """BGK.hpp:33-102.  Defaults as the reference template arguments."""
+    lattice: type = D3Q27
+    equilibrium: type = SecondOrderEquilibrium
+    forcing: object = field(default_factory=NoForcing)
+    storage: type = RawPopulations
+    omega: float = 1.0
+    name = "BGK"
+    op = capi.OP_BGK
+
+    @staticmethod
+    def omega_from_viscosity(nu, lattice=D3Q27):
+        return 1.0 / (nu / lattice.cs2 + 0.5)
+
+    @staticmethod
+    def viscosity_from_omega(w, lattice=D3Q27):
+        return (1.0 / w - 0.5) * lattice.cs2
+
+    def rates(self):
+        return self.omega, -1.0
+
+
+@dataclass
+class TRT:
+    """TRT.hpp:35-136."""
+    lattice: type = D3Q27
+    equilibrium: type = SecondOrderEquilibrium
+    forcing: object = field(default_factory=NoForcing)
+    storage: type = RawPopulations
+    omega_p: float = 1.0
+    omega_m: float = 1.0
+    name = "TRT"
+    op = capi.OP_TRT
+    magic_3_16 = 3.0 / 16.0
+
+    omega_from_viscosity = BGK.omega_from_viscosity
+    viscosity_from_omega = BGK.viscosity_from_omega
+
+    @staticmethod
+    def omega_minus_for(omega_plus, lam):
+        return 1.0 / (lam / (1.0 / omega_plus - 0.5) + 0.5)
+
+    @staticmethod
+    def magic_parameter(omega_plus, omega_minus):
+        return (1.0 / omega_plus - 0.5) * (1.0 / omega_minus - 0.5)
+
+    def rates(self):
+        return self.omega_p, self.omega_m
+
+
+@dataclass
+class MomentCollision:
+    """MomentCollision.hpp:66-376: central moments (central=True) or raw MRT."""
+    lattice: type = D3Q27
+    forcing: object = field(default_factory=NoForcing)
+    storage: type = RawPopulations
+    central: bool = True
+    omega: float = 1.0
+    omega_bulk: float = -1.0
+    equilibrium = SecondOrderEquilibrium  # unused: closed form in moment space
+
+    omega_from_viscosity = BGK.omega_from_viscosity
+    viscosity_from_omega = BGK.viscosity_from_omega
+
+    @property
+    def name(self):
+        return "CentralMoments" if self.central else "MRT"
+
+    @property
+    def op(self):
+        return capi.OP_CM if self.central else capi.OP_MRT
+
+    def bulk(self):
+        return self.omega if self.omega_bulk < 0 else self.omega_bulk
+
+    def rates(self):
+        return self.omega, self.omega_bulk
+
+
+def CentralMoments(lattice=D3Q27, forcing=None, storage=RawPopulations, **kw):
+    return MomentCollision(lattice, forcing or NoForcing(), storage, True, **kw)
+
+
+def MRT(lattice=D3Q27, forcing=None, storage=RawPopulations, **kw):
+    return MomentCollision(lattice, forcing or NoForcing(), storage, False, **kw)
+
+
+@dataclass
+class NullCollision:
+    """Collision that does nothing (tests/test_streaming.cpp:28-38): pure streaming."""
+    lattice: type = D3Q27
+    forcing: object = field(default_factory=NoForcing)
+    storage: type = RawPopulations
+    equilibrium = SecondOrderEquilibrium
+    name = "None"
+    op = capi.OP_NONE
+
+    def rates(self):
+        return 1.0, -1.0
+
+
+# ---------------------------------------------------------------- solver
+def _ptr(a):
+    return C.c_void_p(a.ctypes.data)
+
+
+class FluidSolver:
+    """FluidSolver<L, EsotericPull<L>, Collision> (FluidSolver.hpp:34-637),
+    resident on the current CUDA device."""
+
+    def __init__(self, domain: Domain, collision, streaming=EsotericPull, storage="f32",
+                 stream=None):
+        if streaming is not EsotericPull:
+            raise NotImplementedError("only Esoteric Pull streaming runs on the device")
+        self.dom = domain
+        self.coll = collision
+        L = collision.lattice
+        self.L = L
+        self.Q = L.Q
+        self.storage = capi.STORAGE_NAMES[storage] if isinstance(storage, str) else int(storage)
+        self.real = np.float64 if self.storage == capi.STORE_F64 else np.float32
+        lib = capi.lib()
+        h = C.c_void_p()
+        d = domain
+        capi.check(lib.m3lb_create(L.Q, d.nx, d.ny, d.nz, int(d.periodic[0]), int(d.periodic[1]),
+                                   int(d.periodic[2]), collision.op,
+                                   collision.equilibrium.code, self.storage,
+                                   int(_store(collision.storage)),
+                                   int(collision.forcing.active), C.byref(h)))
+        self._h = h
+        self._flags = np.zeros((d.nz, d.ny, d.nx), np.uint8)
+        self._push_params()
+        if stream is not None:
+            self.set_stream(stream)
+
+    # -- plumbing
+    @property
+    def handle(self):
+        return self._h
+
+    def _push_params(self):
+        w1, w2 = self.coll.rates()
+        f = self.coll.forcing
+        fx, fy, fz = (f.fx, f.fy, f.fz) if f.active else (0.0, 0.0, 0.0)
+        capi.check(capi.lib().m3lb_set_params(self._h, w1, w2, fx, fy, fz))
+
+    def set_stream(self, stream):
+        """Queue work on a CUDA stream (a torch.cuda.Stream or a raw handle)."""
+        raw = getattr(stream, "cuda_stream", stream)
+        capi.check(capi.lib().m3lb_set_stream(self._h, C.c_void_p(raw)))
+
+    def set_option(self, option, value):
+        capi.check(capi.lib().m3lb_set_option(self._h, option, int(value)))
+
+    def sync(self):
+        capi.check(capi.lib().m3lb_sync(self._h))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            capi.lib().m3lb_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- reference API
+    def set_geometry(self, fn_or_flags):
+        """fn(x, y, z) -> CellType over interior coordinates (:74-82), or an
+        array of flags shaped (nz, ny, nx)."""
+        d = self.dom
+        if callable(fn_or_flags):
+            z, y, x = np.meshgrid(np.arange(d.nz), np.arange(d.ny), np.arange(d.nx), indexing="ij")
+            fl = np.vectorize(lambda a, b, c: int(fn_or_flags(a, b, c)), otypes=[np.uint8])(x, y, z)
+        else:
+            fl = np.asarray(fn_or_flags)
+        fl = np.ascontiguousarray(fl, dtype=np.uint8).reshape(d.nz, d.ny, d.nx)
+        capi.check(capi.lib().m3lb_set_flags(self._h, _ptr(fl)))
+        self._flags = fl.copy()
+
+    def initialize(self, rho0=1.0, ux0=0.0, uy0=0.0, uz0=0.0):
+        self._push_params()
+        capi.check(capi.lib().m3lb_init_eq(self._h, rho0, ux0, uy0, uz0))
+
+    def initialize_field(self, fn_or_arrays):
+        """fn(x, y, z) -> (rho, ux, uy, uz) vectorised over interior coordinate
+        arrays, or the four arrays themselves (:568-579)."""
+        d = self.dom
+        if callable(fn_or_arrays):
+            z, y, x = np.meshgrid(np.arange(d.nz), np.arange(d.ny), np.arange(d.nx), indexing="ij")
+            fields = fn_or_arrays(x, y, z)
+        else:
+            fields = fn_or_arrays
+        arrs = [np.ascontiguousarray(np.broadcast_to(np.asarray(a, np.float64), (d.nz, d.ny, d.nx)))
+                for a in fields]
+        self._push_params()
+        capi.check(capi.lib().m3lb_init_field_f64(self._h, *[_ptr(a) for a in arrs]))
+
+    @staticmethod
+    def _addr(a):
+        if hasattr(a, "data_ptr"):
+            return C.c_void_p(a.data_ptr())
+        if isinstance(a, np.ndarray):
+            return C.c_void_p(a.ctypes.data)
+        return C.c_void_p(int(a))
+
+    def initialize_field_f32(self, rho, ux, uy, uz):
+        """Four host float32 arrays (numpy, or pinned torch tensors) over the
+        interior, copied as they are (m3lb_init_field_f32)."""
+        self._push_params()
+        capi.check(capi.lib().m3lb_init_field_f32(self._h, *[self._addr(a) for a in
+                                                             (rho, ux, uy, uz)]))
+
+    def compute_macroscopic_f32(self, rho, ux, uy, uz):
+        """compute_macroscopic() into four host float32 buffers."""
+        capi.check(capi.lib().m3lb_macro_f32(self._h, *[self._addr(a) for a in
+                                                        (rho, ux, uy, uz)]))
+
+    def initialize_field_device(self, rho, ux, uy, uz):
+        """Four device arrays (data pointers) of the arithmetic type."""
+        ptrs = [C.c_void_p(getattr(a, "data_ptr", lambda: a)()) for a in (rho, ux, uy, uz)]
+        self._push_params()
+        capi.check(capi.lib().m3lb_init_field_device(self._h, *ptrs))
+
+    def step(self, store_macroscopic=False):
+        capi.check(capi.lib().m3lb_step(self._h, 1, int(store_macroscopic)))
+
+    def steps(self, n, store_macroscopic=False):
+        capi.check(capi.lib().m3lb_step(self._h, int(n), int(store_macroscopic)))
+
+    def compute_macroscopic(self):
+        d = self.dom
+        out = [np.empty((d.nz, d.ny, d.nx), np.float64) for _ in range(4)]
+        capi.check(capi.lib().m3lb_macro_f64(self._h, *[_ptr(a) for a in out]))
+        self._macro = out
+        return tuple(out)
+
+    def stored_macroscopic(self):
+        d = self.dom
+        out = [np.empty((d.nz, d.ny, d.nx), np.float64) for _ in range(4)]
+        capi.check(capi.lib().m3lb_stored_macro_f64(self._h, *[_ptr(a) for a in out]))
+        self._macro = out
+        return tuple(out)
+
+    def _field(self, k):
+        if not hasattr(self, "_macro"):
+            self.stored_macroscopic()
+        return self._macro[k]
+
+    def rho(self):
+        return self._field(0)
+
+    def ux(self):
+        return self._field(1)
+
+    def uy(self):
+        return self._field(2)
+
+    def uz(self):
+        return self._field(3)
+
+    def reduce(self):
+        out = np.zeros(6, np.float64)
+        capi.check(capi.lib().m3lb_reduce(self._h, _ptr(out)))
+        return out
+
+    def total_mass(self):
+        return float(self.reduce()[0])
+
+    def total_momentum(self, a):
+        return float(self.reduce()[1 + a])
+
+    def flags(self):
+        return self._flags
+
+    def timestep(self):
+        t = C.c_longlong()
+        capi.check(capi.lib().m3lb_timestep(self._h, C.byref(t)))
+        return int(t.value)
+
+    def domain(self):
+        return self.dom
+
+    def collision(self):
+        return self.coll
+
+    def gather_populations(self):
+        out = np.empty((self.dom.n_padded, self.Q), np.float64)
+        capi.check(capi.lib().m3lb_gather(self._h, _ptr(out)))
+        return out
+
+    def gather_raw(self):
+        dt = {capi.STORE_F32: np.float32, capi.STORE_F64: np.float64,
+              capi.STORE_F16: np.uint16, capi.STORE_BF16: np.uint16}[self.storage]
+        out = np.empty((self.dom.n_padded, self.Q), dt)
+        capi.check(capi.lib().m3lb_gather_raw(self._h, _ptr(out)))
+        return out
+
+    def seed_populations(self, fn_or_array):
+        """fn(n, i) -> value over padded node indices, or an (n_padded, Q) array."""
+        if callable(fn_or_array):
+            n = np.arange(self.dom.n_padded)
+            arr = np.stack([np.broadcast_to(fn_or_array(n, i), n.shape) for i in range(self.Q)], 1)
+        else:
+            arr = fn_or_array
+        arr = np.ascontiguousarray(arr, dtype=np.float64).reshape(self.dom.n_padded, self.Q)
+        capi.check(capi.lib().m3lb_scatter(self._h, _ptr(arr)))
+
+    def seed_raw(self, arr):
+        arr = np.ascontiguousarray(arr)
+        assert arr.size == self.dom.n_padded * self.Q
+        capi.check(capi.lib().m3lb_scatter_raw(self._h, _ptr(arr)))
+
+    def dims(self):
+        d = (C.c_int * 12)()
+        capi.check(capi.lib().m3lb_dims(self._h, d))
+        return list(d)
+
+    def populations(self):
+        p, b = C.c_void_p(), C.c_size_t()
+        capi.check(capi.lib().m3lb_populations(self._h, C.byref(p), C.byref(b)))
+        return p.value, b.value
+
+    def launch_count(self):
+        n = C.c_longlong()
+        capi.check(capi.lib().m3lb_launch_count(self._h, C.byref(n)))
+        return int(n.value)
