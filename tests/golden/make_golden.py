@@ -1,0 +1,92 @@
+"""Generate the golden fixtures in this folder from the REFERENCE build.
+
+Runs M3LB's own FluidSolver (oracle/_ref, the reference's src/ headers built
+unmodified against the host Kokkos stand-in) on small seeded cases and saves
+the resulting populations and fields.  Needs the reference build, i.e. run it
+where the reference sources were available:
+
+    make -C oracle ref && python tests/golden/make_golden.py
+
+The fixtures then pin the C oracle (bit for bit) and the GPU path (within the
+parity tolerances) on machines without the reference.
+"""
+from __future__ import annotations
+
+import sys
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+sys.path.insert(0, str(HERE.parent.parent))
+
+import oracle as O  # noqa: E402
+
+# name -> (lattice, op, eq, shifted, forcing, shape, periodic, omega, omega2, F, steps, precision)
+CASES = {
+    "d3q27_cm_guo_walls_f64": (27, "cm", 0, 1, 1, (12, 10, 8), (True, False, True), 1.7, -1.0,
+                               (2e-5, -1e-5, 3e-6), 10, "f64"),
+    "d3q27_trt_pf_walls_f64": (27, "trt", 1, 1, 1, (10, 8, 6), (True, False, False), 1.4, 1.1,
+                               (1e-5, 0.0, 0.0), 10, "f64"),
+    "d3q27_mrt_raw_f32": (27, "mrt", 0, 0, 0, (8, 8, 8), (True, True, True), 1.2, 1.6,
+                          (0.0, 0.0, 0.0), 7, "f32"),
+    "d3q27_bgk_f32": (27, "bgk", 0, 1, 0, (9, 7, 6), (False, False, False), 1.3, -1.0,
+                      (0.0, 0.0, 0.0), 6, "f32"),
+    "d2q9_bgk_guo_walls_f64": (9, "bgk", 0, 1, 1, (16, 12, 1), (True, False, True), 1.25, -1.0,
+                               (1e-5, -2e-6, 0.0), 25, "f64"),
+    "d2q9_cm_f32": (9, "cm", 0, 1, 0, (12, 10, 1), (True, True, True), 1.6, -1.0,
+                    (0.0, 0.0, 0.0), 9, "f32"),
+}
+
+
+def initial_field(shape, seed):
+    nx, ny, nz = shape
+    rng = np.random.default_rng(seed)
+    sh = (nz, ny, nx)
+    rho = 1 + 0.01 * rng.standard_normal(sh)
+    u = [0.03 * rng.standard_normal(sh) for _ in range(3)]
+    if nz == 1:
+        u[2] = np.zeros(sh)
+    # representable in FP32, so every precision starts from the same values
+    return [np.asarray(a, np.float32).astype(np.float64) for a in [rho] + u]
+
+
+def solid_mask(shape, walls):
+    nx, ny, nz = shape
+    fl = np.zeros((nz, ny, nx), np.uint8)
+    if walls:
+        fl[:, 0, :] = 1
+    fl.flat[fl.size // 2] = 1
+    return fl
+
+
+def run(backend, case, seed, quant=None):
+    lat, op, eq, sh, fo, shape, per, om, om2, F, steps, prec = case
+    nx, ny, nz = shape
+    s = O.CpuSolver(backend, lattice=lat, op=op, eq=eq, shifted=sh, forcing=fo, nx=nx, ny=ny,
+                    nz=nz, px=per[0], py=per[1], pz=per[2], omega=om, omega2=om2, fx=F[0],
+                    fy=F[1], fz=F[2], precision=prec, quant=quant)
+    s.set_geometry(solid_mask(shape, not per[1]))
+    s.initialize_field(*initial_field(shape, seed))
+    p0 = s.gather()
+    s.step(steps, store_macro=True)
+    out = {"pops0": p0, "pops": s.gather(), "stored": np.stack(s.stored_macro()),
+           "macro": np.stack(s.macro()), "mass": s.total_mass(),
+           "mom": np.array([s.total_momentum(a) for a in range(3)]), "slots": s.slot_sum()}
+    s.close()
+    return out
+
+
+def main():
+    if not O.ref_available("f64"):
+        raise SystemExit("reference build missing: make -C oracle ref")
+    O.set_ref_threads(1, "f64")
+    O.set_ref_threads(1, "f32")
+    for k, (name, case) in enumerate(CASES.items()):
+        r = run("ref", case, seed=100 + k)
+        np.savez_compressed(HERE / f"{name}.npz", case=np.array(repr(case)), seed=100 + k, **r)
+        print(name, "mass", r["mass"])
+
+
+if __name__ == "__main__":
+    main()

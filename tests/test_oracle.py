@@ -1,0 +1,191 @@
+"""The CPU oracle, pinned to the reference (no GPU).
+
+1. Golden fixtures made by the reference build (tests/golden/make_golden.py):
+   the oracle must reproduce them bit for bit.
+2. Where the reference build is present (oracle/_ref), the oracle against it,
+   live, over every operator / storage / forcing / wall combination.
+3. The reference's own known answers for this path:
+   - the streaming permutation (tests/test_streaming.cpp:42-77, 129-137),
+   - Esoteric Pull against two-lattice streaming (test_streaming.cpp:80-124),
+   - plane Poiseuille, D2Q9 BGK tau = 0.8, H = 32: relative L2 6.95e-4 and the
+     magic-parameter exactness of BGK / TRT / CM / MRT (README.md:173-276,
+     validation/poiseuille.cpp:72-140).
+"""
+import itertools
+import math
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import oracle as O
+from tests.golden import make_golden as G
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+
+
+@pytest.mark.parametrize("name", list(G.CASES))
+def test_oracle_reproduces_golden(name):
+    d = np.load(GOLDEN / f"{name}.npz")
+    r = G.run("oracle", G.CASES[name], seed=int(d["seed"]))
+    for k in ("pops0", "pops", "stored", "macro"):
+        np.testing.assert_array_equal(r[k], d[k], err_msg=k)
+    assert r["mass"] == float(d["mass"])
+    np.testing.assert_array_equal(r["mom"], d["mom"])
+    assert r["slots"] == float(d["slots"])
+
+
+needs_ref = pytest.mark.skipif(not O.ref_available("f64") or not O.ref_available("f32"),
+                               reason="reference build (oracle/_ref) not present")
+
+
+@needs_ref
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+@pytest.mark.parametrize("lat", [9, 27])
+def test_oracle_bit_identical_to_reference(prec, lat):
+    O.set_ref_threads(1, prec)
+    rng = np.random.default_rng(0)
+    ops = [("none", 0), ("bgk", 0), ("bgk", 1), ("trt", 0), ("trt", 1), ("mrt", 0), ("cm", 0)]
+    for (op, eq), shifted, forcing, walls in itertools.product(ops, [1, 0], [0, 1], [0, 1]):
+        nx, ny, nz = (7, 6, 1) if lat == 9 else (5, 6, 4)
+        kw = dict(lattice=lat, op=op, eq=eq, shifted=shifted, forcing=forcing, nx=nx, ny=ny,
+                  nz=nz, px=True, py=not walls, pz=True, omega=1.3,
+                  omega2=(1.1 if op == "trt" else -1.0), fx=2e-5, fy=-1e-5,
+                  fz=3e-6 if lat == 27 else 0.0, precision=prec)
+        a, b = O.CpuSolver("oracle", **kw), O.CpuSolver("ref", **kw)
+        fl = np.zeros((nz, ny, nx), np.uint8)
+        if walls:
+            fl[:, 0, :] = 1
+            fl[:, -1, :] = 1
+        a.set_geometry(fl)
+        b.set_geometry(fl)
+        sh = (nz, ny, nx)
+        rho = 1 + 0.01 * rng.standard_normal(sh)
+        u = [0.03 * rng.standard_normal(sh) for _ in range(3)]
+        if lat == 9:
+            u[2] = np.zeros(sh)
+        a.initialize_field(rho, *u)
+        b.initialize_field(rho, *u)
+        for t in range(5):
+            a.step(1, store_macro=(t == 4))
+            b.step(1, store_macro=(t == 4))
+        case = (prec, lat, op, eq, shifted, forcing, walls)
+        np.testing.assert_array_equal(a.gather(), b.gather(), err_msg=str(case))
+        for x, y in zip(a.macro(), b.macro()):
+            np.testing.assert_array_equal(x, y, err_msg=str(case))
+        for x, y in zip(a.stored_macro(), b.stored_macro()):
+            np.testing.assert_array_equal(x, y, err_msg=str(case))
+        assert a.total_mass() == b.total_mass(), case
+        assert a.total_momentum(0) == b.total_momentum(0), case
+        assert a.slot_sum() == b.slot_sum(), case
+        a.close()
+        b.close()
+
+
+# ------------------------------------------------------- streaming known answers
+def _permutation(lat, shape, steps, backend="oracle", streaming=0):
+    nx, ny, nz = shape
+    Q = lat
+    s = O.CpuSolver(backend, lattice=lat, op="none", nx=nx, ny=ny, nz=nz, precision="f64",
+                    streaming=streaming)
+    tags = (np.arange(s.n_padded * Q, dtype=np.float64) + 1).reshape(s.n_padded, Q)
+    s.seed(tags)
+    s.step(steps)
+    got = s.gather()
+    from m3lb_b200.solver import D2Q9, D3Q27
+    L = D3Q27 if lat == 27 else D2Q9
+    bad = 0
+    for z in range(nz):
+        for y in range(ny):
+            for x in range(nx):
+                n = (z * ny + y) * nx + x
+                for i in range(Q):
+                    src = (((z - steps * L.cz[i]) % nz) * ny + (y - steps * L.cy[i]) % ny) * nx + \
+                          (x - steps * L.cx[i]) % nx
+                    bad += got[n, i] != tags[src, i]
+    s.close()
+    return bad
+
+
+@pytest.mark.parametrize("lat,shape,steps", [
+    (9, (8, 6, 1), 1), (9, (8, 6, 1), 2), (9, (8, 6, 1), 7), (9, (8, 6, 1), 24),
+    (27, (5, 4, 3), 1), (27, (5, 4, 3), 13)])
+def test_oracle_permutation(lat, shape, steps):
+    assert _permutation(lat, shape, steps) == 0
+
+
+@needs_ref
+@pytest.mark.parametrize("lat", [9, 27])
+@pytest.mark.parametrize("shifted", [0, 1])
+def test_esoteric_pull_matches_two_lattice(lat, shifted):
+    """Oracle (Esoteric Pull) against the reference's two-lattice streaming,
+    every step, walls + Guo (test_streaming.cpp:80-124, tolerance 1e-13)."""
+    O.set_ref_threads(1, "f64")
+    nx, ny, nz = (12, 10, 8 if lat == 27 else 1)
+    kw = dict(lattice=lat, op="bgk", shifted=shifted, forcing=1, nx=nx, ny=ny, nz=nz, px=True,
+              py=False, pz=True, omega=1.4, fx=2e-5, fy=-1e-5, fz=0.0, precision="f64")
+    a = O.CpuSolver("oracle", **kw)
+    b = O.CpuSolver("ref", streaming=1, **kw)
+    fl = np.zeros((nz, ny, nx), np.uint8)
+    fl[:, 0, :] = 1
+    fl[:, -1, :] = 1
+    a.set_geometry(fl)
+    b.set_geometry(fl)
+    a.initialize(1.0, 0.03, 0.01, 0.0)
+    b.initialize(1.0, 0.03, 0.01, 0.0)
+    padded_fluid = None
+    for _ in range(40 if lat == 9 else 20):
+        a.step()
+        b.step()
+        ga, gb = a.gather(), b.gather()
+        if padded_fluid is None:
+            sx, sy, sz = nx, ny + 2, nz
+            f3 = np.full((sz, sy, sx), 2, np.uint8)
+            f3[:, 1:-1, :] = fl
+            padded_fluid = (f3.reshape(-1) == 0)
+        assert np.max(np.abs(ga[padded_fluid] - gb[padded_fluid])) <= 1e-13
+
+
+# ------------------------------------------------------- Poiseuille known answers
+def poiseuille(op, tau, H=32, umax=0.01, nx=8, steps=60000, lam=None, precision="f64",
+               backend="oracle"):
+    """validation/poiseuille.cpp:72-140: periodic x, solid rows y = 0 and
+    y = H + 1 (ny = H + 2), uniform Guo force G = 8 rho nu umax / H^2."""
+    nu = (tau - 0.5) / 3.0
+    omega = 1.0 / tau
+    G = 8.0 * nu * umax / (H * H)
+    ny = H + 2
+    omega2 = -1.0
+    if op == "trt":
+        omega2 = 1.0 / (lam / (1.0 / omega - 0.5) + 0.5)
+    s = O.CpuSolver(backend, lattice=9, op=op, shifted=True, forcing=True, nx=nx, ny=ny, nz=1,
+                    px=True, py=False, pz=True, omega=omega, omega2=omega2, fx=G,
+                    precision=precision)
+    fl = np.zeros((1, ny, nx), np.uint8)
+    fl[:, 0, :] = 1
+    fl[:, -1, :] = 1
+    s.set_geometry(fl)
+    s.initialize(1.0)
+    s.step(steps)
+    rho, ux, _, _ = s.macro()
+    s.close()
+    j = np.arange(1, H + 1)
+    u = ux[0, 1:H + 1, nx // 2]
+    rm = rho[0, 1:H + 1, nx // 2].mean()
+    A = G / (2 * rm * nu)
+    ana = A * (j - 0.5) * (H + 0.5 - j)
+    return math.sqrt(np.sum((u - ana) ** 2) / np.sum(ana ** 2))
+
+
+def test_poiseuille_bgk_tau08_known_answer():
+    """README.md:178-186: D2Q9 BGK, H = 32, tau = 0.8 -> L2 relative 6.95e-4."""
+    assert poiseuille("bgk", 0.8) == pytest.approx(6.95e-4, rel=0.01)
+
+
+@pytest.mark.parametrize("op,tau,lam", [("bgk", 0.5 + math.sqrt(3) / 4, None),
+                                        ("trt", 0.8, 3.0 / 16.0),
+                                        ("cm", 7.0 / 8.0, None), ("mrt", 7.0 / 8.0, None)])
+def test_poiseuille_magic_parameter_is_exact(op, tau, lam):
+    """README.md:240-276: at the magic parameter the halfway wall sits exactly
+    midway; the discrete solution is the parabola to round-off (~1e-14)."""
+    assert poiseuille(op, tau, lam=lam) < 1e-11
