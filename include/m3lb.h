@@ -148,6 +148,23 @@ int m3lb_set_option(m3lb_solver* h, int option, int value);
 /* Kernel launches queued by this handle since creation. */
 int m3lb_launch_count(const m3lb_solver* h, long long* n);
 
+/* No counterpart in the reference: an addition of this library.
+ * The reduction of m3lb_reduce for callers that cannot allocate device memory
+ * (who therefore cannot create a handle, which allocates): the caller passes
+ * the population array and flags it holds (device pointers, the layout of
+ * m3lb_populations; flags per padded node, or NULL for an all-fluid interior),
+ * the lattice description, the time step (for the parity) and a device array
+ * `out` of six doubles receiving the same sums as m3lb_reduce.  Queued on
+ * `stream`; returns without waiting.  Allocates nothing: the partial sums use
+ * a fixed 768 KiB array inside the library, so at most 4,194,304 interior
+ * nodes are accepted (M3LB_ERR_INVALID beyond).  The first call on a device
+ * looks that array's address up; make it before any stream capture.  Calls
+ * share the array: calls that overlap on the GPU race. */
+int m3lb_reduce_static(int lattice, int nx, int ny, int nz, int px, int py, int pz, int op,
+                       int storage, int shifted, int forcing, double fx, double fy, double fz,
+                       const void* populations, const uint8_t* flags, long long timestep,
+                       void* stream, double* out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -40,6 +40,7 @@ def _units():
         defs = [f"-DM3LB_LAT={lat}", f"-DM3LB_ST=k{st}", f"-DM3LB_NAME=launchers_{lat}_{st}"]
         units.append((CSRC / "lbm_inst.cu", obj, defs))
     units.append((CSRC / "lbm_capi.cu", BUILD / "capi.o", []))
+    units.append((CSRC / "lbm_noalloc.cu", BUILD / "noalloc.o", []))
     return units
 
 
@@ -56,7 +57,8 @@ def up_to_date() -> bool:
     if not LIB.exists():
         return False
     t = LIB.stat().st_mtime
-    srcs = [CSRC / "lbm_inst.cu", CSRC / "lbm_capi.cu", *[CSRC / h for h in HEADERS],
+    srcs = [CSRC / "lbm_inst.cu", CSRC / "lbm_capi.cu", CSRC / "lbm_noalloc.cu",
+            *[CSRC / h for h in HEADERS],
             PKG.parent / "include" / "m3lb.h"]
     return all(p.stat().st_mtime <= t for p in srcs if p.exists())
 

@@ -66,6 +66,7 @@ SIGNATURES = {
     "m3lb_sync": (_i, [_vp]),
     "m3lb_set_option": (_i, [_vp, _i, _i]),
     "m3lb_launch_count": (_i, [_vp, C.POINTER(C.c_longlong)]),
+    "m3lb_reduce_static": (_i, [_i] * 11 + [_d] * 3 + [_vp, _vp, C.c_longlong, _vp, _vp]),
 }
 
 _lib = None

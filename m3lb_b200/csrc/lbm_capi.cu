@@ -104,6 +104,11 @@ struct DeviceGuard {
 
 }  // namespace
 
+namespace m3lb {
+// Lets other translation units of the library report through m3lb_last_error().
+void set_last_error(const char* msg) { g_last_error = msg ? msg : ""; }
+}  // namespace m3lb
+
 struct m3lb_solver {
   int lattice = 27, Q = 27, op = 0, eq = 0, storage = 0, shifted = 1, forcing = 0;
   Geo g{};
