@@ -1,0 +1,106 @@
+"""The C++ drop-in headers (m3lb_b200/facade).
+
+Reference-style C++ call sites compile against the facade and run on the
+device through libm3lb.so:
+  * tests/cpp/facade_poiseuille.cpp (this repository's driver, written the way
+    the reference's validation/poiseuille.cpp drives its solver) reproduces
+    the Poiseuille known answers of README.md:178-276;
+  * the reference's own src/app/main.cpp (lbm_app) and
+    examples/flow_past_square.cpp, compiled unmodified against the facade by
+    `make -C oracle facade-drivers`, run to completion.
+"""
+import os
+import re
+import shutil
+import subprocess
+from pathlib import Path
+
+import pytest
+
+ROOT = Path(__file__).resolve().parent.parent
+FACADE = ROOT / "m3lb_b200" / "facade"
+LIBDIR = ROOT / "m3lb_b200"
+REF_APP = ROOT / "oracle" / "_ref" / "lbm_app_b200"
+REF_EXAMPLE = ROOT / "oracle" / "_ref" / "flow_past_square_b200"
+
+
+def _compile(src: Path, out: Path):
+    cxx = shutil.which("g++") or "g++"
+    cmd = [cxx, "-std=c++20", "-O2", "-Wall", "-Werror", f"-I{FACADE}", f"-I{ROOT / 'include'}",
+           str(src), "-o", str(out), f"-L{LIBDIR}", "-lm3lb", f"-Wl,-rpath,{LIBDIR}"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr[-3000:]
+    return out
+
+
+def test_facade_driver_compiles(tmp_path):
+    _compile(ROOT / "tests" / "cpp" / "facade_poiseuille.cpp", tmp_path / "fp")
+
+
+@pytest.mark.skipif(not Path("/root/reference/src/app/main.cpp").exists(),
+                    reason="reference sources not present")
+@pytest.mark.parametrize("src", ["src/app/main.cpp", "examples/flow_past_square.cpp"])
+def test_reference_drivers_compile_unmodified(tmp_path, src):
+    cxx = shutil.which("g++") or "g++"
+    r = subprocess.run([cxx, "-std=c++20", "-O2", "-fsyntax-only", f"-I{FACADE}",
+                        f"-I{ROOT / 'include'}", f"/root/reference/{src}"],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr[-3000:]
+
+
+@pytest.fixture(scope="module")
+def poiseuille_bin(tmp_path_factory):
+    return _compile(ROOT / "tests" / "cpp" / "facade_poiseuille.cpp",
+                    tmp_path_factory.mktemp("facade") / "facade_poiseuille")
+
+
+def _run_poiseuille(binary, *args):
+    r = subprocess.run([str(binary), *map(str, args)], capture_output=True, text=True,
+                       timeout=600)
+    assert r.returncode == 0, r.stderr
+    m = re.search(r"l2 (\S+) rho_mean (\S+) mass_drift (\S+) steps (\d+)", r.stdout)
+    assert m, r.stdout
+    return float(m.group(1)), float(m.group(2)), float(m.group(3)), int(m.group(4))
+
+
+@pytest.mark.gpu
+def test_facade_poiseuille_known_answer(cuda_device, poiseuille_bin):
+    """D2Q9 BGK, H = 32, tau = 0.8, FP64 storage: L2 6.95e-4 (README.md:178-186)."""
+    l2, rho, drift, steps = _run_poiseuille(poiseuille_bin, "bgk", 0.8, 60000)
+    assert steps == 60000
+    assert l2 == pytest.approx(6.95e-4, rel=0.01)
+    assert abs(drift) < 1e-12
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("op,tau", [("bgk", 0.5 + 3 ** 0.5 / 4), ("trt", 0.8), ("cm", 0.875),
+                                    ("mrt", 0.875)])
+def test_facade_poiseuille_magic_parameter(cuda_device, poiseuille_bin, op, tau):
+    """At the magic parameter the wall sits exactly midway (README.md:240-276)."""
+    l2, _, _, _ = _run_poiseuille(poiseuille_bin, op, tau, 60000)
+    assert l2 < 1e-10
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not REF_APP.exists(), reason="facade build of the reference lbm_app absent")
+def test_reference_lbm_app_runs_on_device(cuda_device):
+    """The reference's benchmark harness, unmodified: every operator and
+    streaming/storage combination runs, and mass is conserved to its own
+    tolerance (src/app/main.cpp:56-59)."""
+    r = subprocess.run([str(REF_APP), "-n", "64", "-steps", "20"], capture_output=True,
+                       text=True, timeout=600)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "MASS NOT CONSERVED" not in r.stdout
+    rows = [ln for ln in r.stdout.splitlines() if ln.startswith("D3Q27")]
+    assert len(rows) == 7
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not REF_EXAMPLE.exists(), reason="facade build of the reference example absent")
+def test_reference_example_runs_on_device(cuda_device, tmp_path):
+    out = tmp_path / "profile.csv"
+    r = subprocess.run([str(REF_EXAMPLE), "-n", "48", "-steps", "2000", "-out", str(out)],
+                       capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "DIVERGED" not in r.stdout
+    assert out.exists() and len(out.read_text().splitlines()) == 49
