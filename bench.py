@@ -35,6 +35,9 @@ sys.path.insert(0, str(ROOT))
 import numpy as np  # noqa: E402
 
 N_DEFAULT = 256
+KERNELS = {"auto": 0, "nodes": 1, "pairs": 2, "stream": 3}
+KERNEL_NAMES = {"auto": "step_pairs", "pairs": "step_pairs", "stream": "step_stream",
+                "nodes": "step_nodes"}
 U0 = 0.05
 RE = 1600.0
 Q = 27
@@ -168,6 +171,7 @@ def gpu_arm(args, rank, world, dist):
         coll = S.CentralMoments(S.D3Q27, S.NoForcing(), S.ShiftedPopulations, omega=omega)
         s = S.FluidSolver(dom, coll, storage=storage)
         s.set_stream(stream)
+        s.set_option(capi.OPT_KERNEL, KERNELS[args.kernel])
         rho, ux, uy, uz = [t.to(torch.float32).contiguous()
                            for t in tgv_fields(n, _TorchNp(dev))]
         s.initialize_field_device(rho, ux, uy, uz)
@@ -239,7 +243,7 @@ def gpu_arm(args, rank, world, dist):
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
                      "unit": "GB/s", "frac": round(achieved / peak, 4),
                      "peak_kind": f"{peak_kind} (copy bandwidth)",
-                     "kernel": "step_pairs<D3Q27, F16, CM>",
+                     "kernel": f"{KERNEL_NAMES[args.kernel]}<D3Q27, {args.storage.upper()}, CM>",
                      "algorithmic_bytes_per_launch": bytes_per_launch,
                      "traffic": traffic_record(f"D3Q27_CM_{args.storage}_{n}")},
         "gpu_launches": launches,
@@ -285,6 +289,7 @@ def e2e_arm(args, dev, stream, omega):
     copies the initial field from pinned host memory, advances
     args.e2e_lbm_steps time steps and reads rho, u back to pinned memory."""
     import torch
+    from m3lb_b200 import capi
     from m3lb_b200 import solver as S
 
     n = args.size
@@ -293,6 +298,7 @@ def e2e_arm(args, dev, stream, omega):
     coll = S.CentralMoments(S.D3Q27, S.NoForcing(), S.ShiftedPopulations, omega=omega)
     s = S.FluidSolver(dom, coll, storage=args.storage)
     s.set_stream(stream)
+    s.set_option(capi.OPT_KERNEL, KERNELS[args.kernel])
     host_in = [torch.from_numpy(a.astype(np.float32)).pin_memory() for a in tgv_fields(n)]
     host_out = [torch.empty((n, n, n), dtype=torch.float32).pin_memory() for _ in range(4)]
     S_lbm = args.e2e_lbm_steps
@@ -400,6 +406,7 @@ def main():
     ap.add_argument("--impl", default="m3lb", choices=["m3lb", "reference"])
     ap.add_argument("--storage", default="f16", choices=["f16", "bf16", "f32"])
     ap.add_argument("--size", type=int, default=N_DEFAULT)
+    ap.add_argument("--kernel", default="auto", choices=list(KERNELS))
     ap.add_argument("--cpu-size", type=int, default=128)
     ap.add_argument("--e2e-lbm-steps", type=int, default=100)
     ap.add_argument("--e2e-reps", type=int, default=3)

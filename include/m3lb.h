@@ -57,6 +57,16 @@ extern "C" {
 #define M3LB_STORE_F64 3
 
 #define M3LB_OPT_NODE_KERNEL 1 /* value 1: always use the one-node step kernel */
+#define M3LB_OPT_KERNEL 2      /* value: one of M3LB_KERNEL_* below */
+
+/* Step kernel choice (M3LB_OPT_KERNEL).  The chunk kernels (pairs, stream)
+ * need a periodic x axis and even nx; elsewhere every choice runs the
+ * one-node kernel.  All choices give identical stored bits for BGK/TRT and
+ * agree to a few ulp for the moment operators (different FMA contraction). */
+#define M3LB_KERNEL_AUTO 0   /* the fastest kernel for the lattice */
+#define M3LB_KERNEL_NODES 1  /* one node per thread */
+#define M3LB_KERNEL_PAIRS 2  /* one warp per 64-node chunk, two nodes per lane */
+#define M3LB_KERNEL_STREAM 3 /* persistent chunk kernel, asynchronous copy pipeline */
 
 typedef struct m3lb_solver m3lb_solver;
 

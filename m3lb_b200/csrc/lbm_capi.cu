@@ -129,6 +129,7 @@ struct m3lb_solver {
   long long launches = 0;
   double omega = 1, omega2 = -1, fx = 0, fy = 0, fz = 0;
   bool node_kernel = false;
+  int kernel = M3LB_KERNEL_AUTO;     // M3LB_OPT_KERNEL
   const Launchers* L = nullptr;
 
   long long n_interior() const { return (long long)g.nx * g.ny * g.nz; }
@@ -142,7 +143,21 @@ struct m3lb_solver {
     a.fx = forcing ? fx : 0; a.fy = forcing ? fy : 0; a.fz = forcing ? fz : 0;
     return a;
   }
-  bool pairs() const { return !node_kernel && g.px && g.hx == 0 && (g.nx % 2) == 0; }
+  // The chunk kernels need a periodic x axis (no x halo) and even nx; the
+  // one-node kernel runs everything.
+  bool chunk_ok() const { return g.px && g.hx == 0 && (g.nx % 2) == 0; }
+  int step_kernel() const {
+    if (node_kernel || !chunk_ok() || kernel == M3LB_KERNEL_NODES) return kKernelNodes;
+    // the streamed kernel addresses rows with 32-bit element counts
+    const bool rows32 = (long long)g.nch * Q * 64 < (1LL << 31);
+    if (kernel == M3LB_KERNEL_STREAM && rows32) return kKernelStream;
+    // auto: measured on B200 at 192^3 and 256^3, the streamed kernel is the
+    // faster one for the 16-bit BGK/TRT steps and for pure streaming; the
+    // paired kernel for the moment operators and for 32/64-bit storage
+    const bool narrow = storage == M3LB_STORE_F16 || storage == M3LB_STORE_BF16;
+    if (kernel == M3LB_KERNEL_AUTO && rows32 && narrow && op <= M3LB_OP_TRT) return kKernelStream;
+    return kKernelPairs;
+  }
 };
 
 extern "C" {
@@ -348,14 +363,14 @@ int m3lb_step(m3lb_solver* h, int nsteps, int store_macro) {
   if (!h) return fail(M3LB_ERR_INVALID, "step: null handle");
   if (nsteps < 0) return fail(M3LB_ERR_INVALID, "step: negative step count");
   DeviceGuard dg(h->device);
-  const bool pairs = h->pairs();
+  const int kernel = h->step_kernel();
   for (int s = 0; s < nsteps; ++s) {
     StepArgs a = h->args();
     if (store_macro && s == nsteps - 1) {
       a.rho = h->macro[0]; a.ux = h->macro[1]; a.uy = h->macro[2]; a.uz = h->macro[3];
     }
     int n = 0;
-    CUDA_TRY(h->L->step(a, h->op, h->eq, h->shifted != 0, h->forcing != 0, pairs, h->stream, &n));
+    CUDA_TRY(h->L->step(a, h->op, h->eq, h->shifted != 0, h->forcing != 0, kernel, h->stream, &n));
     h->launches += n;
     ++h->t;
   }
@@ -527,6 +542,12 @@ int m3lb_set_option(m3lb_solver* h, int option, int value) {
   if (!h) return fail(M3LB_ERR_INVALID, "set_option: null handle");
   if (option == M3LB_OPT_NODE_KERNEL) {
     h->node_kernel = value != 0;
+    return M3LB_OK;
+  }
+  if (option == M3LB_OPT_KERNEL) {
+    if (value < M3LB_KERNEL_AUTO || value > M3LB_KERNEL_STREAM)
+      return fail(M3LB_ERR_INVALID, "set_option: bad kernel %d", value);
+    h->kernel = value;
     return M3LB_OK;
   }
   return fail(M3LB_ERR_INVALID, "set_option: unknown option %d", option);

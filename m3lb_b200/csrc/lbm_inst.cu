@@ -2,6 +2,7 @@
 // selected at compile time:
 //   -DM3LB_LAT=D2Q9|D3Q27 -DM3LB_ST=kF32|kF16|kBF16|kF64 -DM3LB_NAME=launchers_<...>
 #include "lbm_kernels.cuh"
+#include "lbm_stream.cuh"
 #include "lbm_launch.h"
 
 #ifndef M3LB_LAT
@@ -20,10 +21,42 @@ inline unsigned blocks_for(long long n, int threads) {
   return (unsigned)((n + threads - 1) / threads);
 }
 
+// Persistent grid of the streamed kernel: the resident blocks of every SM
+// (occupancy queried once per device), never more warps than chunks.
 template <int OP, int EQ, bool SH, bool FORCE>
-cudaError_t step_t(const StepArgs& a, bool pairs, cudaStream_t s) {
+cudaError_t launch_stream(const StepArgs& a, cudaStream_t s) {
+  using Cfg = StreamCfg<L, ST>;
+  auto kern = step_stream<L, ST, OP, EQ, SH, FORCE>;
+  constexpr int kMaxDev = 64;
+  static int cached[kMaxDev];  // resident blocks per SM x SMs, 0 = not yet known
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= kMaxDev) return cudaErrorInvalidDevice;
+  if (cached[dev] == 0) {
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, Cfg::SMEM);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0, nsm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kPairThreads, Cfg::SMEM);
+    if (e != cudaSuccess) return e;
+    e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) return cudaErrorInvalidConfiguration;
+    cached[dev] = per_sm * nsm;
+  }
   const Geo& g = a.g;
-  if (pairs) {
+  const long long units = (long long)g.ny * g.nz * g.nch;
+  const long long need = (units + Cfg::WARPS - 1) / Cfg::WARPS;
+  const unsigned grid = (unsigned)(need < cached[dev] ? need : cached[dev]);
+  kern<<<grid, kPairThreads, Cfg::SMEM, s>>>(a);
+  return cudaGetLastError();
+}
+
+template <int OP, int EQ, bool SH, bool FORCE>
+cudaError_t step_t(const StepArgs& a, int kernel, cudaStream_t s) {
+  const Geo& g = a.g;
+  if (kernel == kKernelStream) return launch_stream<OP, EQ, SH, FORCE>(a, s);
+  if (kernel == kKernelPairs) {
     // one warp per 64-node chunk of every interior row
     const long long nthreads = (long long)g.ny * g.nz * g.nch * 32;
     step_pairs<L, ST, OP, EQ, SH, FORCE><<<blocks_for(nthreads, kPairThreads), kPairThreads, 0, s>>>(a);
@@ -35,25 +68,25 @@ cudaError_t step_t(const StepArgs& a, bool pairs, cudaStream_t s) {
 }
 
 template <int OP, int EQ, bool SH>
-cudaError_t step_f(const StepArgs& a, bool force, bool pairs, cudaStream_t s) {
-  return force ? step_t<OP, EQ, SH, true>(a, pairs, s) : step_t<OP, EQ, SH, false>(a, pairs, s);
+cudaError_t step_f(const StepArgs& a, bool force, int kernel, cudaStream_t s) {
+  return force ? step_t<OP, EQ, SH, true>(a, kernel, s) : step_t<OP, EQ, SH, false>(a, kernel, s);
 }
 template <int OP, int EQ>
-cudaError_t step_s(const StepArgs& a, bool sh, bool force, bool pairs, cudaStream_t s) {
-  if (sh) return step_f<OP, EQ, true>(a, force, pairs, s);
-  if constexpr (kRawOK) return step_f<OP, EQ, false>(a, force, pairs, s);
+cudaError_t step_s(const StepArgs& a, bool sh, bool force, int kernel, cudaStream_t s) {
+  if (sh) return step_f<OP, EQ, true>(a, force, kernel, s);
+  if constexpr (kRawOK) return step_f<OP, EQ, false>(a, force, kernel, s);
   return cudaErrorInvalidValue;
 }
 
-cudaError_t step(const StepArgs& a, int op, int eq, bool sh, bool force, bool pairs,
+cudaError_t step(const StepArgs& a, int op, int eq, bool sh, bool force, int kernel,
                  cudaStream_t s, int* launches) {
   if (launches) *launches += 1;
   switch (op) {
-    case 0: return step_t<0, 0, true, false>(a, pairs, s);
-    case 1: return eq ? step_s<1, 1>(a, sh, force, pairs, s) : step_s<1, 0>(a, sh, force, pairs, s);
-    case 2: return eq ? step_s<2, 1>(a, sh, force, pairs, s) : step_s<2, 0>(a, sh, force, pairs, s);
-    case 3: return step_s<3, 0>(a, sh, force, pairs, s);
-    case 4: return step_s<4, 0>(a, sh, force, pairs, s);
+    case 0: return step_t<0, 0, true, false>(a, kernel, s);
+    case 1: return eq ? step_s<1, 1>(a, sh, force, kernel, s) : step_s<1, 0>(a, sh, force, kernel, s);
+    case 2: return eq ? step_s<2, 1>(a, sh, force, kernel, s) : step_s<2, 0>(a, sh, force, kernel, s);
+    case 3: return step_s<3, 0>(a, sh, force, kernel, s);
+    case 4: return step_s<4, 0>(a, sh, force, kernel, s);
     default: return cudaErrorInvalidValue;
   }
 }

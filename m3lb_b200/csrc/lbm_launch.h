@@ -8,9 +8,14 @@
 
 namespace m3lb {
 
+// Step kernels: one node per thread (any geometry), and, for a periodic x
+// axis with even nx, the paired kernel (one warp per 64-node chunk) or its
+// persistent, copy-pipelined form.
+enum StepKernel { kKernelNodes = 1, kKernelPairs = 2, kKernelStream = 3 };
+
 struct Launchers {
-  // one step; pairs selects the paired kernel (periodic x, even nx)
-  cudaError_t (*step)(const StepArgs& a, int op, int eq, bool sh, bool force, bool pairs,
+  // one step with the given StepKernel
+  cudaError_t (*step)(const StepArgs& a, int op, int eq, bool sh, bool force, int kernel,
                       cudaStream_t s, int* launches);
   cudaError_t (*seed)(const SeedArgs& a, int op, int eq, bool sh, cudaStream_t s);
   cudaError_t (*gather)(const Geo& g, const void* f, int parity, double* out, void* raw,
