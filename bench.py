@@ -257,7 +257,48 @@ def gpu_arm(args, rank, world, dist):
         out["e2e"] = e2e_arm(args, dev, stream, omega)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(args)
+    if rank == 0 and world == 1 and args.serve_requests > 0:
+        out["serving"] = serving_arm(args)
     return out
+
+
+def serving_arm(args):
+    """The serving stream: seeded Poisson arrivals (mean 50/s) of periodic
+    Taylor-Green boxes, N in {32, 48, ..., 160}, BGK / TRT / CM, u0 in
+    [0.02, 0.08], 200-2000 steps, FP16 storage, tau = 0.6.  The offered load
+    is above one GPU's capacity, so a finite stream is served and the latency
+    (arrival to result) includes the queueing."""
+    from m3lb_b200 import serve as SV
+
+    reqs = SV.request_stream(count=args.serve_requests, rate=50.0, seed=0)
+    srv = SV.Server(hbm_budget=args.serve_budget_gb << 30, max_resident=args.serve_resident,
+                    round_steps=args.serve_round, storage="f16")
+    for r in reqs:
+        srv.submit(r)
+    srv.run(time_limit=900)
+    res = srv.results()
+    st = srv.stats()
+    srv.close()
+    s = SV.summary(res, reqs)
+    return {
+        "metric": "p50 / p99 request latency (arrival to result, queueing included)",
+        "p50_ms": round(s["latency_p50_s"] * 1e3, 1),
+        "p99_ms": round(s["latency_p99_s"] * 1e3, 1),
+        "max_ms": round(s["latency_max_s"] * 1e3, 1),
+        "requests": s["requests"],
+        "offered_rate_per_s": round(s["offered_rate_per_s"], 2),
+        "served_rate_per_s": round(s["served_rate_per_s"], 2),
+        "offered_mlups": round(s["offered_mlups"], 1),
+        "aggregate_mlups": round(s["aggregate_mlups"], 1),
+        "makespan_s": round(s["makespan_s"], 2),
+        "all_finite": bool(all(np.isfinite(r.mass) for r in res)),
+        "loop": {"rounds": st.rounds, "launches": st.launches,
+                 "graph_captures": st.graph_captures, "graph_launches": st.graph_launches,
+                 "hbm_budget_gib": args.serve_budget_gb, "max_resident": args.serve_resident,
+                 "round_steps": args.serve_round},
+        "workload": "seed 0, Poisson 50/s, N in {32..160 step 16}, op in {BGK, TRT, CM}, "
+                    "u0 ~ U[0.02, 0.08], steps ~ U[200, 2000], FP16, tau 0.6",
+    }
 
 
 class _TorchNp:
@@ -412,6 +453,11 @@ def main():
     ap.add_argument("--e2e-reps", type=int, default=3)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--serve-requests", type=int, default=500,
+                    help="requests of the serving stream (0: skip it)")
+    ap.add_argument("--serve-budget-gb", type=int, default=4)
+    ap.add_argument("--serve-resident", type=int, default=16)
+    ap.add_argument("--serve-round", type=int, default=100)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

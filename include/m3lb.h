@@ -175,6 +175,76 @@ int m3lb_reduce_static(int lattice, int nx, int ny, int nz, int px, int py, int 
                        const void* populations, const uint8_t* flags, long long timestep,
                        void* stream, double* out);
 
+/* ------------------------------------------------------------ serving loop
+ * Many independent lattices resident on one GPU and advanced together (no
+ * counterpart in the reference, which runs one solver per process).  A
+ * request is a periodic D3Q27 Taylor-Green box of extent N (even) with one of
+ * the BGK, TRT, MRT or CM operators (shifted populations, no force), an
+ * amplitude u0, relaxation rates and a step count.  Requests are admitted in
+ * arrival order while their footprint (populations plus 16 B per node of
+ * seed/readout fields) fits hbm_budget; every admitted lattice stays resident
+ * until its last step.  Each time step of a round is one batched launch per
+ * operator over all resident lattices, replayed from a CUDA graph while the
+ * resident set repeats.  Results are FP64 mass, momentum and energy of
+ * the final state (and rho, u with keep_fields); a request's result is
+ * bit-identical alone, in any mix, and through m3lb_step with
+ * M3LB_KERNEL_PAIRS. */
+typedef struct m3lb_server m3lb_server;
+
+typedef struct {
+  size_t hbm_budget;  /* bytes the resident lattices may hold */
+  int max_resident;   /* most lattices resident at once (0: budget only; at most 1024) */
+  int round_steps;    /* most time steps per scheduling round (>= 1) */
+  int storage;        /* M3LB_STORE_F16, _BF16 or _F32, for every request */
+  int keep_fields;    /* 1: keep rho, u of finished requests for m3lb_serve_fields */
+} m3lb_serve_config;
+
+typedef struct {
+  long long id;         /* caller's tag */
+  double arrival;       /* seconds after m3lb_serve_run starts */
+  int n;                /* extent of the N^3 periodic box */
+  int op;               /* M3LB_OP_BGK, _TRT, _MRT or _CM */
+  int steps;            /* time steps */
+  double u0;            /* Taylor-Green amplitude (the field of m3lb_tgv_field) */
+  double omega, omega2; /* rates as in m3lb_set_params */
+} m3lb_request;
+
+typedef struct {
+  long long id;
+  double arrival, admitted, finished; /* seconds after the run started */
+  int n, op, steps, status;
+  long long node_steps;               /* n^3 * steps */
+  double mass, momentum[3], energy;   /* FP64 reductions of the final state */
+} m3lb_result;
+
+typedef struct {
+  long long rounds;         /* scheduling rounds */
+  long long launches;       /* batched kernel launches (direct or in graphs) */
+  long long graph_captures; /* rounds captured into a CUDA graph */
+  long long graph_launches; /* rounds replayed from a graph */
+  long long finished;       /* requests completed */
+  long long node_steps;     /* sum of n^3 * steps over completed requests */
+  double makespan;          /* seconds from the start of the last run to its end */
+} m3lb_serve_stats;
+
+int m3lb_serve_create(const m3lb_serve_config* cfg, m3lb_server** out);
+/* Queue a request for the next m3lb_serve_run. */
+int m3lb_serve_submit(m3lb_server* s, const m3lb_request* r);
+/* Serve every submitted request, honouring arrival times (the loop waits for
+ * them in real time); time_limit > 0 bounds the run in seconds. */
+int m3lb_serve_run(m3lb_server* s, double time_limit);
+/* Finished requests in completion order; *count = how many exist. */
+int m3lb_serve_results(const m3lb_server* s, m3lb_result* out, int cap, int* count);
+/* Host copies (n^3 floats each, x fastest) of a finished request's rho, u. */
+int m3lb_serve_fields(const m3lb_server* s, long long id, float* rho, float* ux, float* uy,
+                      float* uz);
+int m3lb_serve_get_stats(const m3lb_server* s, m3lb_serve_stats* st);
+int m3lb_serve_destroy(m3lb_server* s);
+/* The serving loop's initial field into device arrays (n^3 floats each):
+ * Taylor-Green u = u0 sin x cos y cos z, v = -u0 cos x sin y cos z, w = 0,
+ * rho = 1 + 3 u0^2 / 16 (cos 2x + cos 2y)(cos 2z + 2), x = 2 pi i / n. */
+int m3lb_tgv_field(int n, double u0, float* rho, float* ux, float* uy, float* uz, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,7 +1,8 @@
 """Build libm3lb.so in-tree with nvcc for sm_100a.
 
 The kernel instantiations are split over one translation unit per
-(lattice, storage format) and compiled in parallel; the C ABI is a ninth unit.
+(lattice, storage format) and compiled in parallel; the C ABI, the
+allocation-free reduction and the serving loop are three more units.
 Usage: ``python -m m3lb_b200.build [--jobs N] [--verbose]``.
 """
 from __future__ import annotations
@@ -23,7 +24,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2"]
 
 SLICES = [(lat, st) for lat in ("D2Q9", "D3Q27") for st in ("F32", "F16", "BF16", "F64")]
-HEADERS = ["lbm_common.cuh", "lbm_collide.cuh", "lbm_kernels.cuh", "lbm_stream.cuh", "lbm_launch.h"]
+HEADERS = ["lbm_common.cuh", "lbm_collide.cuh", "lbm_kernels.cuh", "lbm_stream.cuh", "lbm_launch.h",
+           "lbm_host.h"]
 
 
 def nvcc() -> str:
@@ -41,6 +43,7 @@ def _units():
         units.append((CSRC / "lbm_inst.cu", obj, defs))
     units.append((CSRC / "lbm_capi.cu", BUILD / "capi.o", []))
     units.append((CSRC / "lbm_noalloc.cu", BUILD / "noalloc.o", []))
+    units.append((CSRC / "lbm_serve.cu", BUILD / "serve.o", []))
     return units
 
 
@@ -58,6 +61,7 @@ def up_to_date() -> bool:
         return False
     t = LIB.stat().st_mtime
     srcs = [CSRC / "lbm_inst.cu", CSRC / "lbm_capi.cu", CSRC / "lbm_noalloc.cu",
+            CSRC / "lbm_serve.cu", CSRC / "lbm_host.h",
             *[CSRC / h for h in HEADERS],
             PKG.parent / "include" / "m3lb.h"]
     return all(p.stat().st_mtime <= t for p in srcs if p.exists())

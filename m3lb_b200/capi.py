@@ -34,6 +34,35 @@ class M3lbError(RuntimeError):
         self.code = code
 
 
+class ServeConfig(C.Structure):
+    """m3lb_serve_config."""
+    _fields_ = [("hbm_budget", C.c_size_t), ("max_resident", C.c_int),
+                ("round_steps", C.c_int), ("storage", C.c_int), ("keep_fields", C.c_int)]
+
+
+class Request(C.Structure):
+    """m3lb_request."""
+    _fields_ = [("id", C.c_longlong), ("arrival", C.c_double), ("n", C.c_int), ("op", C.c_int),
+                ("steps", C.c_int), ("u0", C.c_double), ("omega", C.c_double),
+                ("omega2", C.c_double)]
+
+
+class Result(C.Structure):
+    """m3lb_result."""
+    _fields_ = [("id", C.c_longlong), ("arrival", C.c_double), ("admitted", C.c_double),
+                ("finished", C.c_double), ("n", C.c_int), ("op", C.c_int), ("steps", C.c_int),
+                ("status", C.c_int), ("node_steps", C.c_longlong), ("mass", C.c_double),
+                ("momentum", C.c_double * 3), ("energy", C.c_double)]
+
+
+class ServeStats(C.Structure):
+    """m3lb_serve_stats."""
+    _fields_ = [("rounds", C.c_longlong), ("launches", C.c_longlong),
+                ("graph_captures", C.c_longlong), ("graph_launches", C.c_longlong),
+                ("finished", C.c_longlong), ("node_steps", C.c_longlong),
+                ("makespan", C.c_double)]
+
+
 _vp = C.c_void_p
 _i = C.c_int
 _d = C.c_double
@@ -69,6 +98,14 @@ SIGNATURES = {
     "m3lb_set_option": (_i, [_vp, _i, _i]),
     "m3lb_launch_count": (_i, [_vp, C.POINTER(C.c_longlong)]),
     "m3lb_reduce_static": (_i, [_i] * 11 + [_d] * 3 + [_vp, _vp, C.c_longlong, _vp, _vp]),
+    "m3lb_serve_create": (_i, [C.POINTER(ServeConfig), _pp]),
+    "m3lb_serve_submit": (_i, [_vp, C.POINTER(Request)]),
+    "m3lb_serve_run": (_i, [_vp, _d]),
+    "m3lb_serve_results": (_i, [_vp, C.POINTER(Result), _i, C.POINTER(_i)]),
+    "m3lb_serve_fields": (_i, [_vp, C.c_longlong] + [_vp] * 4),
+    "m3lb_serve_get_stats": (_i, [_vp, C.POINTER(ServeStats)]),
+    "m3lb_serve_destroy": (_i, [_vp]),
+    "m3lb_tgv_field": (_i, [_i, _d] + [_vp] * 4 + [_vp]),
 }
 
 _lib = None

@@ -10,7 +10,7 @@
 #include <vector>
 
 #include "../../include/m3lb.h"
-#include "lbm_launch.h"
+#include "lbm_host.h"
 
 using namespace m3lb;
 
@@ -35,6 +35,26 @@ int fail(int code, const char* fmt, ...) {
       return fail(M3LB_ERR_CUDA, "%s: %s (%s)", #call, cudaGetErrorString(e_),      \
                   cudaGetErrorName(e_));                                            \
   } while (0)
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    int cur = -1;
+    if (cudaGetDevice(&cur) == cudaSuccess && cur != dev) {
+      prev = cur;
+      cudaSetDevice(dev);
+    }
+  }
+  ~DeviceGuard() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
+
+}  // namespace
+
+namespace m3lb {
+// Lets other translation units of the library report through m3lb_last_error().
+void set_last_error(const char* msg) { g_last_error = msg ? msg : ""; }
 
 int elem_bytes(int storage) {
   switch (storage) {
@@ -87,26 +107,6 @@ const Launchers* table_for(int lattice, int storage) {
   }
   return nullptr;
 }
-
-struct DeviceGuard {
-  int prev = -1;
-  explicit DeviceGuard(int dev) {
-    int cur = -1;
-    if (cudaGetDevice(&cur) == cudaSuccess && cur != dev) {
-      prev = cur;
-      cudaSetDevice(dev);
-    }
-  }
-  ~DeviceGuard() {
-    if (prev >= 0) cudaSetDevice(prev);
-  }
-};
-
-}  // namespace
-
-namespace m3lb {
-// Lets other translation units of the library report through m3lb_last_error().
-void set_last_error(const char* msg) { g_last_error = msg ? msg : ""; }
 }  // namespace m3lb
 
 struct m3lb_solver {

@@ -168,9 +168,11 @@ constexpr int pair_min_blocks() {
   return ST == kF64 ? 2 : ((OP == 1 || OP == 2 || (OP == 0 && ST == kF32)) ? 3 : 4);
 }
 
+// One 64-node chunk (unit `warp` of the lattice's ny * nz * nch chunks) by
+// one warp.  Shared by the paired kernel and the batched kernel of the
+// serving loop, so a lattice gets the same arithmetic in both.
 template <class L, int ST, int OP, int EQ, bool SH, bool FORCE>
-__global__ void __launch_bounds__(kPairThreads, pair_min_blocks<OP, ST>())
-step_pairs(StepArgs a) {
+__device__ __forceinline__ void pairs_unit(const StepArgs& a, long long warp, int lane) {
   using WO = WordOps<ST>;
   using W = typename WO::W;
   using E = typename WO::E;
@@ -179,8 +181,6 @@ step_pairs(StepArgs a) {
   constexpr int Q = L::Q;
   const Geo& g = a.g;
 
-  const int lane = threadIdx.x & 31;
-  const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const long long nrows = (long long)g.ny * g.nz;
   const bool warp_ok = warp < nrows * g.nch;
   const long long wsafe = warp_ok ? warp : 0;
@@ -286,6 +286,13 @@ step_pairs(StepArgs a) {
       }
     }
   }
+}
+
+template <class L, int ST, int OP, int EQ, bool SH, bool FORCE>
+__global__ void __launch_bounds__(kPairThreads, pair_min_blocks<OP, ST>())
+step_pairs(StepArgs a) {
+  const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  pairs_unit<L, ST, OP, EQ, SH, FORCE>(a, warp, threadIdx.x & 31);
 }
 
 // -------------------------------------------------- one-node step kernel

@@ -1,0 +1,639 @@
+// Serving loop: many independent lattices resident in HBM, advanced together.
+//
+// A request is one periodic D3Q27 Taylor-Green lattice (size N, operator,
+// amplitude u0, step count).  The server admits queued requests in arrival
+// order while their device footprint fits the HBM budget, keeps every
+// admitted lattice resident until its last step, and advances all of them in
+// scheduling rounds.  A round runs R time steps of every resident lattice
+// (R = the smallest remaining step count, capped by the configured round
+// length); each time step is one launch of the batched kernel per operator,
+// over a device table of (lattice, first chunk) items, and the launches of a
+// round are captured once into a CUDA graph and replayed while the resident
+// set does not change.  Finished lattices are reduced (FP64 mass, momentum,
+// energy) and, optionally, their rho and u copied out; their memory returns
+// to the stream-ordered pool and the next requests are admitted.
+//
+// Each lattice chunk is updated by pairs_unit, the same device code as the
+// single-lattice paired kernel, so a request's result does not depend on
+// what else is resident: it is bit-identical alone, in any mix, and through
+// the single-lattice C ABI with the same kernel.
+//
+// The reference has no serving loop; this file has no counterpart there.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cstdarg>
+#include <cstdint>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <deque>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/m3lb.h"
+#include "lbm_host.h"
+#include "lbm_kernels.cuh"
+
+using namespace m3lb;
+
+namespace {
+
+// ------------------------------------------------------------------ device
+struct BatchItem {
+  StepArgs a;             // geometry, populations, rates (parity set per step)
+  long long first_unit;   // first chunk of this lattice in the launch
+  long long t0;           // lattice time at the start of the round
+};
+
+constexpr int kBatchThreads = 128;
+constexpr int kMaxItems = 1024;  // lattices in one launch (shared-memory search table)
+
+// One time step of every lattice in `items` (all with operator OP): warp u
+// of the grid updates chunk u - first_unit of the item whose range holds u.
+template <int ST, int OP, int EQ>
+__global__ void __launch_bounds__(kBatchThreads, pair_min_blocks<OP, ST>())
+batch_step(const BatchItem* __restrict__ items, int n_items, long long n_units, int s) {
+  __shared__ long long first[kMaxItems];
+  for (int i = threadIdx.x; i < n_items; i += blockDim.x) first[i] = items[i].first_unit;
+  __syncthreads();
+  const long long u = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (u >= n_units) return;  // whole warp (uniform)
+  int lo = 0, hi = n_items - 1;  // last item with first <= u
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (first[mid] <= u) lo = mid; else hi = mid - 1;
+  }
+  StepArgs a = items[lo].a;
+  a.parity = (int)((items[lo].t0 + s) & 1);
+  pairs_unit<D3Q27, ST, OP, EQ, true, false>(a, u - first[lo], threadIdx.x & 31);
+}
+
+// Taylor-Green benchmark initial field (the analytic pressure in rho, w = 0)
+// on an N^3 periodic box, in FP64, rounded to the FP32 fields the seed reads.
+__global__ void tgv_field_kernel(int n, double u0, float* rho, float* ux, float* uy, float* uz) {
+  const long long nn = (long long)n * n * n;
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nn) return;
+  const int x = (int)(i % n), y = (int)((i / n) % n), z = (int)(i / ((long long)n * n));
+  const double k = 2.0 * 3.14159265358979323846 / n;
+  const double X = x * k, Y = y * k, Z = z * k;
+  const double dr = 3.0 * u0 * u0 / 16.0;
+  rho[i] = (float)(1.0 + dr * (cos(2 * X) + cos(2 * Y)) * (cos(2 * Z) + 2.0));
+  ux[i] = (float)(u0 * sin(X) * cos(Y) * cos(Z));
+  uy[i] = (float)(-u0 * cos(X) * sin(Y) * cos(Z));
+  uz[i] = 0.0f;
+}
+
+using BatchFn = void (*)(const BatchItem*, int, long long, int);
+
+template <int ST>
+BatchFn batch_fn_st(int op) {
+  switch (op) {
+    case M3LB_OP_BGK: return batch_step<ST, 1, 0>;
+    case M3LB_OP_TRT: return batch_step<ST, 2, 0>;
+    case M3LB_OP_MRT: return batch_step<ST, 3, 0>;
+    case M3LB_OP_CM: return batch_step<ST, 4, 0>;
+    default: return nullptr;
+  }
+}
+BatchFn batch_fn(int storage, int op) {
+  switch (storage) {
+    case M3LB_STORE_F16: return batch_fn_st<kF16>(op);
+    case M3LB_STORE_BF16: return batch_fn_st<kBF16>(op);
+    case M3LB_STORE_F32: return batch_fn_st<kF32>(op);
+    default: return nullptr;
+  }
+}
+
+// -------------------------------------------------------------------- host
+int fail(int code, const char* fmt, ...) __attribute__((format(printf, 2, 3)));
+int fail(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  std::vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  set_last_error(buf);
+  return code;
+}
+
+#define SRV_TRY(call)                                                             \
+  do {                                                                            \
+    cudaError_t e_ = (call);                                                      \
+    if (e_ != cudaSuccess)                                                        \
+      return fail(M3LB_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_));        \
+  } while (0)
+
+using Clock = std::chrono::steady_clock;
+
+struct Lattice {
+  m3lb_request req;
+  Geo g{};
+  const Launchers* L = nullptr;
+  void* f = nullptr;
+  size_t bytes = 0;         // admission footprint
+  long long t = 0;          // time steps done
+  long long units = 0;      // chunks per time step
+  double admitted = 0;
+};
+
+struct Finished {
+  m3lb_result res;
+  std::vector<float> fields;  // rho, ux, uy, uz (keep_fields)
+};
+
+constexpr int kOps[4] = {M3LB_OP_BGK, M3LB_OP_TRT, M3LB_OP_MRT, M3LB_OP_CM};
+
+// A launched round: its end event and the requests whose readout it carries.
+struct Inflight {
+  cudaEvent_t end = nullptr;
+  std::vector<size_t> finishing;  // indices into done
+};
+
+}  // namespace
+
+struct m3lb_server {
+  m3lb_serve_config cfg{};
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaMemPool_t pool = nullptr;
+  std::vector<m3lb_request> submitted;
+  std::deque<m3lb_request> queue;   // arrived, not admitted
+  std::vector<Lattice> active;
+  std::vector<Finished> done;
+  size_t resident = 0;              // bytes held by active lattices
+  uint8_t* zero_flags = nullptr;    // all-fluid flags for seeding and readout
+  long long zero_flags_bytes = 0;
+  double* partials = nullptr;       // reduction scratch (one lattice at a time)
+  int partial_blocks = 0;
+  double* red_out = nullptr;
+  BatchItem* items_dev = nullptr;   // [4][kMaxItems]
+  BatchItem* items_host = nullptr;  // pinned, two of that shape: a round's table is
+                                    // still to be copied while the next is built
+  int flip = 0;
+  int n_items[4] = {0, 0, 0, 0};
+  long long n_units[4] = {0, 0, 0, 0};
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t graph_exec = nullptr;
+  long long set_version = 0, graph_version = -1;
+  int graph_R = -1;
+  long long prev_version = -1;      // resident set and R of the previous round
+  int prev_R = -1;
+  double* red_slots = nullptr;      // pinned, kReduceVals per request of a run
+  int red_cap = 0;
+  std::deque<Inflight> inflight;    // launched rounds not yet observed complete
+  std::vector<cudaEvent_t> free_events;
+  m3lb_serve_stats stats{};
+};
+
+namespace {
+
+struct SrvGuard {
+  int prev = -1;
+  explicit SrvGuard(int dev) {
+    int cur = -1;
+    if (cudaGetDevice(&cur) == cudaSuccess && cur != dev) {
+      prev = cur;
+      cudaSetDevice(dev);
+    }
+  }
+  ~SrvGuard() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
+
+// Device bytes a request holds while resident: populations, the FP32 seed /
+// readout fields, the reduction scratch share.
+size_t footprint(const m3lb_serve_config& c, int n) {
+  const Geo g = make_geo(n, n, n, 1, 1, 1);
+  return pop_elems(g, 27) * (size_t)elem_bytes(c.storage) + 16 * (size_t)n * n * n;
+}
+
+double now_s(Clock::time_point t0) {
+  return std::chrono::duration<double>(Clock::now() - t0).count();
+}
+
+int ensure_zero_flags(m3lb_server* s, long long bytes) {
+  if (bytes <= s->zero_flags_bytes) return M3LB_OK;
+  SRV_TRY(cudaStreamSynchronize(s->stream));
+  if (s->zero_flags) SRV_TRY(cudaFree(s->zero_flags));
+  s->zero_flags = nullptr;
+  SRV_TRY(cudaMalloc((void**)&s->zero_flags, (size_t)bytes));
+  SRV_TRY(cudaMemset(s->zero_flags, 0, (size_t)bytes));
+  s->zero_flags_bytes = bytes;
+  return M3LB_OK;
+}
+
+int ensure_partials(m3lb_server* s, int blocks) {
+  if (blocks <= s->partial_blocks) return M3LB_OK;
+  SRV_TRY(cudaStreamSynchronize(s->stream));
+  if (s->partials) SRV_TRY(cudaFree(s->partials));
+  s->partials = nullptr;
+  SRV_TRY(cudaMalloc((void**)&s->partials, ((size_t)blocks + 1) * kReduceVals * sizeof(double)));
+  s->partial_blocks = blocks;
+  s->red_out = s->partials + (size_t)blocks * kReduceVals;
+  return M3LB_OK;
+}
+
+StepArgs lattice_args(const m3lb_server* s, const Lattice& l) {
+  StepArgs a{};
+  a.g = l.g;
+  a.f = l.f;
+  a.flags = nullptr;
+  a.parity = (int)(l.t & 1);
+  a.omega = l.req.omega;
+  a.omega2 = l.req.omega2;
+  (void)s;
+  return a;
+}
+
+// Admit one request: allocate its populations from the pool and seed the
+// Taylor-Green equilibrium through the single-lattice seed path.
+int admit(m3lb_server* s, const m3lb_request& r, double t_now) {
+  Lattice l;
+  l.req = r;
+  l.g = make_geo(r.n, r.n, r.n, 1, 1, 1);
+  l.L = table_for(27, s->cfg.storage);
+  l.bytes = footprint(s->cfg, r.n);
+  l.units = (long long)l.g.ny * l.g.nz * l.g.nch;
+  l.admitted = t_now;
+  int rc = ensure_zero_flags(s, l.g.n_padded);
+  if (rc) return rc;
+  SRV_TRY(cudaMallocAsync(&l.f, pop_elems(l.g, 27) * (size_t)elem_bytes(s->cfg.storage),
+                          s->stream));
+  const size_t nn = (size_t)r.n * r.n * r.n;
+  float* fld = nullptr;
+  SRV_TRY(cudaMallocAsync((void**)&fld, 4 * nn * sizeof(float), s->stream));
+  tgv_field_kernel<<<(unsigned)((nn + 255) / 256), 256, 0, s->stream>>>(r.n, r.u0, fld, fld + nn,
+                                                                          fld + 2 * nn, fld + 3 * nn);
+  SRV_TRY(cudaGetLastError());
+  SeedArgs sa{};
+  sa.g = l.g;
+  sa.f = l.f;
+  sa.flags = s->zero_flags;
+  sa.parity = 0;
+  sa.mode = 1;
+  sa.rho0 = 1;
+  // the seed reads fields of the arithmetic type: FP32 except for FP64 storage
+  sa.rho = fld; sa.ux = fld + nn; sa.uy = fld + 2 * nn; sa.uz = fld + 3 * nn;
+  SRV_TRY(l.L->seed(sa, r.op, 0, true, s->stream));
+  SRV_TRY(cudaFreeAsync(fld, s->stream));
+  s->resident += l.bytes;
+  s->active.push_back(l);
+  ++s->set_version;
+  return M3LB_OK;
+}
+
+// Enqueue the readout of a finished lattice (FP64 reductions into its pinned
+// slot; rho, u when kept) and the release of its memory.  The result is
+// complete when the round's end event is.
+int finish(m3lb_server* s, Lattice& l) {
+  Finished fin;
+  std::memset(&fin.res, 0, sizeof fin.res);
+  fin.res.id = l.req.id;
+  fin.res.arrival = l.req.arrival;
+  fin.res.admitted = l.admitted;
+  fin.res.n = l.req.n;
+  fin.res.op = l.req.op;
+  fin.res.steps = l.req.steps;
+  const size_t slot = s->done.size();
+  if ((int)slot >= s->red_cap) return fail(M3LB_ERR_INVALID, "serve: result slots exhausted");
+  StepArgs a = lattice_args(s, l);
+  const int nb = reduce_blocks(l.g);
+  int rc = ensure_partials(s, nb);
+  if (rc) return rc;
+  SRV_TRY(l.L->reduce(a, l.req.op, true, false, s->partials, nb, s->red_out, s->stream));
+  SRV_TRY(cudaMemcpyAsync(s->red_slots + slot * kReduceVals, s->red_out,
+                          kReduceVals * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+  const size_t nn = (size_t)l.req.n * l.req.n * l.req.n;
+  if (s->cfg.keep_fields) {
+    float* fld = nullptr;
+    SRV_TRY(cudaMallocAsync((void**)&fld, 4 * nn * sizeof(float), s->stream));
+    StepArgs m = a;
+    m.flags = s->zero_flags;
+    m.rho = fld; m.ux = fld + nn; m.uy = fld + 2 * nn; m.uz = fld + 3 * nn;
+    SRV_TRY(l.L->macro(m, l.req.op, true, false, s->stream));
+    fin.fields.resize(4 * nn);
+    SRV_TRY(cudaMemcpyAsync(fin.fields.data(), fld, 4 * nn * sizeof(float),
+                            cudaMemcpyDeviceToHost, s->stream));
+    SRV_TRY(cudaFreeAsync(fld, s->stream));
+  }
+  SRV_TRY(cudaFreeAsync(l.f, s->stream));
+  fin.res.node_steps = (long long)nn * l.req.steps;
+  fin.res.status = M3LB_ERR_INVALID;  // until observed complete
+  s->resident -= l.bytes;
+  s->done.push_back(std::move(fin));
+  return M3LB_OK;
+}
+
+// Wait for the oldest launched round; stamp the requests it finished.
+int retire_oldest(m3lb_server* s, Clock::time_point t0) {
+  Inflight f = s->inflight.front();
+  s->inflight.pop_front();
+  SRV_TRY(cudaEventSynchronize(f.end));
+  const double t = now_s(t0);
+  for (size_t i : f.finishing) {
+    m3lb_result& r = s->done[i].res;
+    const double* v = s->red_slots + i * kReduceVals;
+    r.mass = v[0];
+    for (int k = 0; k < 3; ++k) r.momentum[k] = v[1 + k];
+    r.energy = v[4];
+    r.finished = t;
+    r.status = M3LB_OK;
+    s->stats.node_steps += r.node_steps;
+    s->stats.finished += 1;
+  }
+  s->free_events.push_back(f.end);
+  return M3LB_OK;
+}
+
+// Item tables of the resident set, one per operator, for a round starting
+// now; returns through n_items / n_units.
+BatchItem* host_table(m3lb_server* s) { return s->items_host + (size_t)s->flip * 4 * kMaxItems; }
+
+void build_items(m3lb_server* s) {
+  BatchItem* tab = host_table(s);
+  for (int o = 0; o < 4; ++o) {
+    s->n_items[o] = 0;
+    s->n_units[o] = 0;
+  }
+  for (const Lattice& l : s->active) {
+    int o = 0;
+    while (kOps[o] != l.req.op) ++o;
+    BatchItem& it = tab[o * kMaxItems + s->n_items[o]++];
+    it.a = lattice_args(s, l);
+    it.first_unit = s->n_units[o];
+    it.t0 = l.t;
+    s->n_units[o] += l.units;
+  }
+}
+
+int launch_round(m3lb_server* s, int R) {
+  for (int step = 0; step < R; ++step)
+    for (int o = 0; o < 4; ++o) {
+      if (!s->n_items[o]) continue;
+      BatchFn fn = batch_fn(s->cfg.storage, kOps[o]);
+      const long long threads = s->n_units[o] * 32;
+      const unsigned blocks = (unsigned)((threads + kBatchThreads - 1) / kBatchThreads);
+      void* args[4];
+      const BatchItem* ip = s->items_dev + (size_t)o * kMaxItems;
+      int ni = s->n_items[o];
+      long long nu = s->n_units[o];
+      int st = step;
+      args[0] = (void*)&ip; args[1] = &ni; args[2] = &nu; args[3] = &st;
+      SRV_TRY(cudaLaunchKernel((const void*)fn, dim3(blocks), dim3(kBatchThreads), args, 0,
+                               s->stream));
+    }
+  return M3LB_OK;
+}
+
+// One round: R steps of every resident lattice.  A round whose resident set
+// and R repeat the previous one's is captured into a CUDA graph (or replays
+// the graph already captured for them); a round after a change launches
+// directly, since its graph would be used once.
+int run_round(m3lb_server* s, int R) {
+  // at most two rounds are in flight and the older one has completed before
+  // a new table is built, so alternating host tables never overwrites one
+  // whose copy is still queued
+  s->flip ^= 1;
+  build_items(s);
+  const BatchItem* tab = host_table(s);
+  for (int o = 0; o < 4; ++o)
+    if (s->n_items[o])
+      SRV_TRY(cudaMemcpyAsync(s->items_dev + (size_t)o * kMaxItems, tab + (size_t)o * kMaxItems,
+                              s->n_items[o] * sizeof(BatchItem), cudaMemcpyHostToDevice, s->stream));
+  const bool cached = s->graph_exec && s->graph_version == s->set_version && s->graph_R == R;
+  const bool repeat = s->prev_version == s->set_version && s->prev_R == R;
+  s->prev_version = s->set_version;
+  s->prev_R = R;
+  if (!cached && !repeat) {
+    const int rc = launch_round(s, R);
+    if (rc) return rc;
+  } else {
+    if (!cached) {
+      if (s->graph_exec) cudaGraphExecDestroy(s->graph_exec);
+      if (s->graph) cudaGraphDestroy(s->graph);
+      s->graph_exec = nullptr;
+      s->graph = nullptr;
+      SRV_TRY(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+      const int rc = launch_round(s, R);
+      cudaGraph_t g = nullptr;
+      const cudaError_t e = cudaStreamEndCapture(s->stream, &g);
+      if (rc) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+      }
+      SRV_TRY(e);
+      s->graph = g;
+      SRV_TRY(cudaGraphInstantiate(&s->graph_exec, s->graph, 0));
+      s->graph_version = s->set_version;
+      s->graph_R = R;
+      s->stats.graph_captures += 1;
+    }
+    SRV_TRY(cudaGraphLaunch(s->graph_exec, s->stream));
+    s->stats.graph_launches += 1;
+  }
+  for (Lattice& l : s->active) l.t += R;
+  s->stats.rounds += 1;
+  for (int o = 0; o < 4; ++o) s->stats.launches += (long long)R * (s->n_items[o] ? 1 : 0);
+  return M3LB_OK;
+}
+
+bool fits(const m3lb_server* s, const m3lb_request& r) {
+  if (s->cfg.max_resident > 0 && (int)s->active.size() >= s->cfg.max_resident) return false;
+  if ((int)s->active.size() >= kMaxItems) return false;
+  return s->resident + footprint(s->cfg, r.n) <= s->cfg.hbm_budget;
+}
+
+}  // namespace
+
+extern "C" {
+
+int m3lb_serve_create(const m3lb_serve_config* cfg, m3lb_server** out) {
+  if (!cfg || !out) return fail(M3LB_ERR_INVALID, "serve_create: null argument");
+  *out = nullptr;
+  if (!batch_fn(cfg->storage, M3LB_OP_CM))
+    return fail(M3LB_ERR_UNSUPPORTED, "serve_create: storage %d is not served (F16, BF16, F32)",
+                cfg->storage);
+  if (cfg->round_steps < 1) return fail(M3LB_ERR_INVALID, "serve_create: round_steps must be >= 1");
+  auto* s = new m3lb_server();
+  s->cfg = *cfg;
+  cudaGetDevice(&s->device);
+  auto bail = [&](int rc) { m3lb_serve_destroy(s); return rc; };
+  if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess)
+    return bail(fail(M3LB_ERR_CUDA, "serve_create: cannot create a stream"));
+  if (cudaDeviceGetDefaultMemPool(&s->pool, s->device) == cudaSuccess) {
+    // keep freed lattice memory in the pool for the next admissions
+    uint64_t keep = UINT64_MAX;
+    cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
+  if (cudaMalloc((void**)&s->items_dev, 4 * kMaxItems * sizeof(BatchItem)) != cudaSuccess ||
+      cudaMallocHost((void**)&s->items_host, 2 * 4 * kMaxItems * sizeof(BatchItem)) != cudaSuccess)
+    return bail(fail(M3LB_ERR_MEMORY, "serve_create: cannot allocate the item tables"));
+  std::memset(s->items_host, 0, 2 * 4 * kMaxItems * sizeof(BatchItem));
+  *out = s;
+  return M3LB_OK;
+}
+
+int m3lb_serve_submit(m3lb_server* s, const m3lb_request* r) {
+  if (!s || !r) return fail(M3LB_ERR_INVALID, "serve_submit: null argument");
+  if (r->n < 2 || (r->n % 2) != 0)
+    return fail(M3LB_ERR_INVALID, "serve_submit: N must be even and >= 2 (got %d)", r->n);
+  if (r->steps < 0) return fail(M3LB_ERR_INVALID, "serve_submit: negative step count");
+  if (!batch_fn(s->cfg.storage, r->op))
+    return fail(M3LB_ERR_UNSUPPORTED, "serve_submit: operator %d is not served", r->op);
+  if (footprint(s->cfg, r->n) > s->cfg.hbm_budget)
+    return fail(M3LB_ERR_MEMORY, "serve_submit: N=%d needs %zu bytes, above the budget %zu",
+                r->n, footprint(s->cfg, r->n), s->cfg.hbm_budget);
+  s->submitted.push_back(*r);
+  return M3LB_OK;
+}
+
+int m3lb_serve_run(m3lb_server* s, double time_limit) {
+  if (!s) return fail(M3LB_ERR_INVALID, "serve_run: null handle");
+  SrvGuard dg(s->device);
+  std::vector<m3lb_request> pending = s->submitted;
+  s->submitted.clear();
+  std::stable_sort(pending.begin(), pending.end(),
+                   [](const m3lb_request& a, const m3lb_request& b) { return a.arrival < b.arrival; });
+  // pinned result slots for every request of this run (and those before)
+  const int need = (int)(s->done.size() + pending.size() + s->queue.size() + s->active.size());
+  if (need > s->red_cap) {
+    double* p = nullptr;
+    SRV_TRY(cudaStreamSynchronize(s->stream));
+    SRV_TRY(cudaMallocHost((void**)&p, (size_t)std::max(need, 1) * kReduceVals * sizeof(double)));
+    if (s->red_slots) {
+      std::memcpy(p, s->red_slots, (size_t)s->red_cap * kReduceVals * sizeof(double));
+      cudaFreeHost(s->red_slots);
+    }
+    s->red_slots = p;
+    s->red_cap = std::max(need, 1);
+  }
+  size_t next = 0;
+  const Clock::time_point t0 = Clock::now();
+  while (next < pending.size() || !s->queue.empty() || !s->active.empty() || !s->inflight.empty()) {
+    const double t = now_s(t0);
+    if (time_limit > 0 && t > time_limit)
+      return fail(M3LB_ERR_INVALID, "serve_run: time limit %.1f s reached with %zu queued, %zu resident",
+                  time_limit, s->queue.size() + (pending.size() - next), s->active.size());
+    while (next < pending.size() && pending[next].arrival <= t) s->queue.push_back(pending[next++]);
+    while (!s->queue.empty() && fits(s, s->queue.front())) {
+      const int rc = admit(s, s->queue.front(), t);
+      if (rc) return rc;
+      s->queue.pop_front();
+    }
+    if (s->active.empty()) {
+      if (!s->inflight.empty()) {
+        const int rc = retire_oldest(s, t0);
+        if (rc) return rc;
+      } else if (next < pending.size()) {
+        const double wait = pending[next].arrival - now_s(t0);
+        if (wait > 0) std::this_thread::sleep_for(std::chrono::duration<double>(std::min(wait, 0.005)));
+      }
+      continue;
+    }
+    long long R = s->cfg.round_steps;
+    for (const Lattice& l : s->active) R = std::min<long long>(R, l.req.steps - l.t);
+    if (R > 0) {
+      const int rc = run_round(s, (int)R);
+      if (rc) return rc;
+    }
+    // lattices done after this round: readout and release follow it on the stream
+    Inflight f;
+    for (size_t i = 0; i < s->active.size();) {
+      Lattice& l = s->active[i];
+      if (l.t >= l.req.steps) {
+        const int rc = finish(s, l);
+        if (rc) return rc;
+        f.finishing.push_back(s->done.size() - 1);
+        s->active.erase(s->active.begin() + (long)i);
+        ++s->set_version;
+      } else {
+        ++i;
+      }
+    }
+    if (s->free_events.empty()) {
+      cudaEvent_t e = nullptr;
+      SRV_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+      s->free_events.push_back(e);
+    }
+    f.end = s->free_events.back();
+    s->free_events.pop_back();
+    SRV_TRY(cudaEventRecord(f.end, s->stream));
+    s->inflight.push_back(std::move(f));
+    // at most two rounds queued: wait for the older one while the newer runs
+    while (s->inflight.size() > 1) {
+      const int rc = retire_oldest(s, t0);
+      if (rc) return rc;
+    }
+  }
+  s->stats.makespan = now_s(t0);
+  return M3LB_OK;
+}
+
+int m3lb_serve_results(const m3lb_server* s, m3lb_result* out, int cap, int* count) {
+  if (!s || !count) return fail(M3LB_ERR_INVALID, "serve_results: null argument");
+  int n = 0;
+  for (const Finished& f : s->done)
+    if (f.res.status == M3LB_OK) {
+      if (out && n < cap) out[n] = f.res;
+      ++n;
+    }
+  *count = n;
+  return M3LB_OK;
+}
+
+int m3lb_serve_fields(const m3lb_server* s, long long id, float* rho, float* ux, float* uy,
+                      float* uz) {
+  if (!s || !rho || !ux || !uy || !uz) return fail(M3LB_ERR_INVALID, "serve_fields: null argument");
+  for (const Finished& f : s->done)
+    if (f.res.id == id) {
+      if (f.fields.empty())
+        return fail(M3LB_ERR_INVALID, "serve_fields: fields of %lld were not kept", id);
+      const size_t nn = f.fields.size() / 4;
+      float* dst[4] = {rho, ux, uy, uz};
+      for (int k = 0; k < 4; ++k) std::memcpy(dst[k], f.fields.data() + k * nn, nn * sizeof(float));
+      return M3LB_OK;
+    }
+  return fail(M3LB_ERR_INVALID, "serve_fields: no finished request %lld", id);
+}
+
+int m3lb_serve_get_stats(const m3lb_server* s, m3lb_serve_stats* st) {
+  if (!s || !st) return fail(M3LB_ERR_INVALID, "serve_stats: null argument");
+  *st = s->stats;
+  return M3LB_OK;
+}
+
+int m3lb_serve_destroy(m3lb_server* s) {
+  if (!s) return M3LB_OK;
+  SrvGuard dg(s->device);
+  if (s->stream) cudaStreamSynchronize(s->stream);
+  for (Lattice& l : s->active)
+    if (l.f) cudaFree(l.f);
+  if (s->graph_exec) cudaGraphExecDestroy(s->graph_exec);
+  if (s->graph) cudaGraphDestroy(s->graph);
+  if (s->zero_flags) cudaFree(s->zero_flags);
+  if (s->partials) cudaFree(s->partials);
+  if (s->items_dev) cudaFree(s->items_dev);
+  if (s->items_host) cudaFreeHost(s->items_host);
+  if (s->red_slots) cudaFreeHost(s->red_slots);
+  for (Inflight& f : s->inflight) cudaEventDestroy(f.end);
+  for (cudaEvent_t e : s->free_events) cudaEventDestroy(e);
+  if (s->stream) cudaStreamDestroy(s->stream);
+  delete s;
+  return M3LB_OK;
+}
+
+int m3lb_tgv_field(int n, double u0, float* rho, float* ux, float* uy, float* uz, void* stream) {
+  if (n < 1 || !rho || !ux || !uy || !uz) return fail(M3LB_ERR_INVALID, "tgv_field: bad argument");
+  const long long nn = (long long)n * n * n;
+  tgv_field_kernel<<<(unsigned)((nn + 255) / 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+      n, u0, rho, ux, uy, uz);
+  SRV_TRY(cudaGetLastError());
+  return M3LB_OK;
+}
+
+}  // extern "C"
