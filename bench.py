@@ -257,6 +257,8 @@ def gpu_arm(args, rank, world, dist):
         out["e2e"] = e2e_arm(args, dev, stream, omega)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(args)
+    if rank == 0 and world == 1 and args.acc_steps > 0:
+        out["accuracy"] = accuracy_arm(args, dev, stream, omega)
     if rank == 0 and world == 1 and args.serve_requests > 0:
         out["serving"] = serving_arm(args)
     return out
@@ -391,6 +393,54 @@ def _ref_rate(n, steps, threads, warm=1):
     return n ** 3 * steps / dt / 1e6, dt
 
 
+def accuracy_arm(args, dev, stream, omega):
+    """Storage precision against FP64 storage on the same workload: the
+    Taylor-Green vortex at args.size^3 after args.acc_steps steps, seeded from
+    the same FP64 field.  Velocity: relative L2 over all components and max
+    |error| / u0; density: relative L2 and max of rho - 1; mass drift from
+    the FP64 device reduction."""
+    import torch
+    from m3lb_b200 import capi
+    from m3lb_b200 import solver as S
+
+    n = args.size
+
+    def run(storage):
+        dom = S.Domain(n, n, n, True, True, True)
+        coll = S.CentralMoments(S.D3Q27, S.NoForcing(), S.ShiftedPopulations, omega=omega)
+        s = S.FluidSolver(dom, coll, storage=storage)
+        s.set_stream(stream)
+        s.set_option(capi.OPT_KERNEL, KERNELS[args.kernel])
+        dt = torch.float64 if storage == "f64" else torch.float32
+        f = [t.to(dt).contiguous() for t in tgv_fields(n, _TorchNp(dev))]
+        s.initialize_field_device(*f)
+        del f
+        m0 = s.reduce()[0]
+        s.steps(args.acc_steps)
+        m1 = s.reduce()[0]
+        rho, ux, uy, uz = s.compute_macroscopic()
+        s.close()
+        return rho, np.stack([ux, uy, uz]), (m1 - m0) / m0
+
+    rho_r, u_r, drift_r = run("f64")
+    out = {"workload": f"D3Q27 CM Taylor-Green {n}^3, {args.acc_steps} steps, u0 {U0}, Re {RE}",
+           "reference": "FP64 storage (FP64 arithmetic), same seed field",
+           "f64": {"mass_drift": float(drift_r)}}
+    du = float(np.sqrt(np.sum(u_r * u_r)))
+    dr = float(np.sqrt(np.sum((rho_r - 1) ** 2)))
+    for st in ("f32", "bf16", "f16"):
+        rho, u, drift = run(st)
+        eu = u - u_r
+        er = rho - rho_r
+        out[st] = {"u_rel_l2": float(np.sqrt(np.sum(eu * eu)) / du),
+                   "u_max_over_u0": float(np.max(np.abs(eu)) / U0),
+                   "rho_rel_l2": float(np.sqrt(np.sum(er * er)) / dr),
+                   "rho_max": float(np.max(np.abs(er))),
+                   "mass_drift": float(drift)}
+        del rho, u, eu, er
+    return out
+
+
 def cpu_baseline(args):
     import oracle as O
     if not O.ref_available("f32"):
@@ -453,6 +503,8 @@ def main():
     ap.add_argument("--e2e-reps", type=int, default=3)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--acc-steps", type=int, default=500,
+                    help="steps of the storage-precision comparison (0: skip it)")
     ap.add_argument("--serve-requests", type=int, default=500,
                     help="requests of the serving stream (0: skip it)")
     ap.add_argument("--serve-budget-gb", type=int, default=4)
