@@ -35,9 +35,10 @@ sys.path.insert(0, str(ROOT))
 import numpy as np  # noqa: E402
 
 N_DEFAULT = 256
-KERNELS = {"auto": 0, "nodes": 1, "pairs": 2, "stream": 3}
-KERNEL_NAMES = {"auto": "step_pairs", "pairs": "step_pairs", "stream": "step_stream",
-                "nodes": "step_nodes"}
+KERNELS = {"auto": 0, "nodes": 1, "pairs": 2, "stream": 3, "rows": 4}
+# what auto runs for the 256^3 FP16 workload (FP32 storage runs step_pairs)
+KERNEL_NAMES = {"auto": "step_rows", "pairs": "step_pairs", "stream": "step_stream",
+                "nodes": "step_nodes", "rows": "step_rows"}
 U0 = 0.05
 RE = 1600.0
 Q = 27

@@ -22,7 +22,7 @@ EQ_SECOND_ORDER, EQ_PRODUCT_FORM = 0, 1
 STORE_F32, STORE_F16, STORE_BF16, STORE_F64 = 0, 1, 2, 3
 OPT_NODE_KERNEL = 1
 OPT_KERNEL = 2
-KERNEL_AUTO, KERNEL_NODES, KERNEL_PAIRS, KERNEL_STREAM = 0, 1, 2, 3
+KERNEL_AUTO, KERNEL_NODES, KERNEL_PAIRS, KERNEL_STREAM, KERNEL_ROWS = 0, 1, 2, 3, 4
 
 STORAGE_NAMES = {"f32": STORE_F32, "f16": STORE_F16, "bf16": STORE_BF16, "f64": STORE_F64}
 STORAGE_BYTES = {STORE_F32: 4, STORE_F16: 2, STORE_BF16: 2, STORE_F64: 8}

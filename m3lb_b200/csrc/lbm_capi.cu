@@ -124,6 +124,7 @@ struct m3lb_solver {
   void* staging = nullptr;           // init_field uploads (4 interior arrays)
   double* partials = nullptr;        // reduction scratch
   double* red_out = nullptr;
+  int* err = nullptr;                // device status word (after red_out)
   int nblocks = 0;
   long long t = 0;
   long long launches = 0;
@@ -141,6 +142,7 @@ struct m3lb_solver {
     a.parity = (int)(t & 1);
     a.omega = omega; a.omega2 = omega2;
     a.fx = forcing ? fx : 0; a.fy = forcing ? fy : 0; a.fz = forcing ? fz : 0;
+    a.err = err;
     return a;
   }
   // The chunk kernels need a periodic x axis (no x halo) and even nx; the
@@ -150,11 +152,18 @@ struct m3lb_solver {
     if (node_kernel || !chunk_ok() || kernel == M3LB_KERNEL_NODES) return kKernelNodes;
     // the streamed kernel addresses rows with 32-bit element counts
     const bool rows32 = (long long)g.nch * Q * 64 < (1LL << 31);
+    // the row kernel: whole rows of at most 8 full chunks
+    const bool rows_ok = (g.nx % 64) == 0 && g.nch <= 4 &&
+                         4LL * Q * 256 * elem_bytes(storage) + 64 <= 227LL * 1024;
+    if (kernel == M3LB_KERNEL_ROWS && rows_ok) return kKernelRows;
     if (kernel == M3LB_KERNEL_STREAM && rows32) return kKernelStream;
-    // auto: measured on B200 at 192^3 and 256^3, the streamed kernel is the
-    // faster one for the 16-bit BGK/TRT steps and for pure streaming; the
-    // paired kernel for the moment operators and for 32/64-bit storage
+    // auto, from measurements on B200: with 16-bit storage the row kernel
+    // for rows of 3 or 4 full chunks (256^3 CM: 0.34 ms against 0.49 ms for
+    // the paired kernel), else the streamed kernel for BGK/TRT and pure
+    // streaming; the paired kernel for everything else (32/64-bit storage
+    // is already near the copy bandwidth with it)
     const bool narrow = storage == M3LB_STORE_F16 || storage == M3LB_STORE_BF16;
+    if (kernel == M3LB_KERNEL_AUTO && narrow && rows_ok && g.nch >= 3) return kKernelRows;
     if (kernel == M3LB_KERNEL_AUTO && rows32 && narrow && op <= M3LB_OP_TRT) return kKernelStream;
     return kKernelPairs;
   }
@@ -212,6 +221,9 @@ int m3lb_create(int lattice, int nx, int ny, int nz, int px, int py, int pz, int
   if (cudaMalloc((void**)&h->partials, (size_t)h->nblocks * kReduceVals * 8 + 64) != cudaSuccess)
     return cleanup(fail(M3LB_ERR_MEMORY, "create: cannot allocate reduction scratch"));
   h->red_out = h->partials + (size_t)h->nblocks * kReduceVals;
+  h->err = reinterpret_cast<int*>(h->red_out + kReduceVals);
+  if (cudaMemset(h->err, 0, sizeof(int)) != cudaSuccess)
+    return cleanup(fail(M3LB_ERR_CUDA, "create: cannot clear the status word"));
   if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess)
     return cleanup(fail(M3LB_ERR_CUDA, "create: cannot create stream"));
   h->own_stream = true;
@@ -536,6 +548,15 @@ int m3lb_sync(m3lb_solver* h) {
   if (!h) return fail(M3LB_ERR_INVALID, "sync: null handle");
   DeviceGuard dg(h->device);
   CUDA_TRY(cudaStreamSynchronize(h->stream));
+  // a kernel whose bounded wait expired leaves a status in the word and
+  // returns; report it once
+  int st = 0;
+  CUDA_TRY(cudaMemcpy(&st, h->err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (st != 0) {
+    CUDA_TRY(cudaMemset(h->err, 0, sizeof(int)));
+    return fail(M3LB_ERR_CUDA, "sync: a step kernel gave up waiting for its copies (status %d); "
+                "the populations of that step are not valid", st);
+  }
   return M3LB_OK;
 }
 int m3lb_set_option(m3lb_solver* h, int option, int value) {
@@ -545,7 +566,7 @@ int m3lb_set_option(m3lb_solver* h, int option, int value) {
     return M3LB_OK;
   }
   if (option == M3LB_OPT_KERNEL) {
-    if (value < M3LB_KERNEL_AUTO || value > M3LB_KERNEL_STREAM)
+    if (value < M3LB_KERNEL_AUTO || value > M3LB_KERNEL_ROWS)
       return fail(M3LB_ERR_INVALID, "set_option: bad kernel %d", value);
     h->kernel = value;
     return M3LB_OK;

@@ -197,6 +197,7 @@ struct StepArgs {
   int parity;              // t % 2
   double omega, omega2;    // BGK/TRT/MRT/CM rates (TRT: omega_p, omega_m; moments: omega, bulk)
   double fx, fy, fz;       // uniform Guo body force
+  int* err;                // device status word: a kernel whose bounded wait ran out sets it
 };
 
 // Scatter (Access::scatter, EsotericPull.hpp:104-111): write, for node n and

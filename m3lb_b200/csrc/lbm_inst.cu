@@ -2,7 +2,10 @@
 // selected at compile time:
 //   -DM3LB_LAT=D2Q9|D3Q27 -DM3LB_ST=kF32|kF16|kBF16|kF64 -DM3LB_NAME=launchers_<...>
 #include "lbm_kernels.cuh"
+#include <cudaTypedefs.h>
+
 #include "lbm_stream.cuh"
+#include "lbm_rows.cuh"
 #include "lbm_launch.h"
 
 #ifndef M3LB_LAT
@@ -23,10 +26,10 @@ inline unsigned blocks_for(long long n, int threads) {
 
 // Persistent grid of the streamed kernel: the resident blocks of every SM
 // (occupancy queried once per device), never more warps than chunks.
-template <int OP, int EQ, bool SH, bool FORCE>
-cudaError_t launch_stream(const StepArgs& a, cudaStream_t s) {
+template <int OP, int EQ, bool SH, bool FORCE, bool FULL>
+cudaError_t launch_stream_t(const StepArgs& a, cudaStream_t s) {
   using Cfg = StreamCfg<L, ST>;
-  auto kern = step_stream<L, ST, OP, EQ, SH, FORCE>;
+  auto kern = step_stream<L, ST, OP, EQ, SH, FORCE, FULL>;
   constexpr int kMaxDev = 64;
   static int cached[kMaxDev];  // resident blocks per SM x SMs, 0 = not yet known
   int dev = 0;
@@ -51,10 +54,90 @@ cudaError_t launch_stream(const StepArgs& a, cudaStream_t s) {
   kern<<<grid, kPairThreads, Cfg::SMEM, s>>>(a);
   return cudaGetLastError();
 }
+// Every chunk full (nx a multiple of 64) and at least two chunks per row:
+// the lane layout of the chunk edges is fixed at compile time.
+template <int OP, int EQ, bool SH, bool FORCE>
+cudaError_t launch_stream(const StepArgs& a, cudaStream_t s) {
+  if ((a.g.nx % kChunk) == 0 && a.g.nch >= 2) return launch_stream_t<OP, EQ, SH, FORCE, true>(a, s);
+  return launch_stream_t<OP, EQ, SH, FORCE, false>(a, s);
+}
+
+// The 3-D tensor maps of the population array for the row kernel: x (64
+// elements of a chunk), direction (Q), chunk (sz * sy * nch); one map per
+// copy shape of the row plan, box (64, span, nch) with traversal stride s
+// along the direction axis (span = (count - 1) * s + 1).
+cudaError_t rows_maps(const StepArgs& a, RowMaps<L>* maps) {
+  static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+  if (!encode) {
+    cudaDriverEntryPointQueryResult q;
+    void* fn = nullptr;
+    cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q);
+    if (e != cudaSuccess) return e;
+    if (q != cudaDriverEntryPointSuccess || !fn) return cudaErrorNotSupported;
+    encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+  }
+  using E = typename WordOps<ST>::E;
+  using Pl = RowPlan<L>;
+  constexpr int EB = (int)sizeof(E);
+  const Geo& g = a.g;
+  const CUtensorMapDataType dt = EB == 2 ? CU_TENSOR_MAP_DATA_TYPE_UINT16
+                                 : EB == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
+                                           : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
+  const cuuint64_t dims[3] = {(cuuint64_t)kChunk, (cuuint64_t)L::Q,
+                              (cuuint64_t)g.sz * g.sy * g.nch};
+  const cuuint64_t strides[2] = {(cuuint64_t)kChunk * EB, (cuuint64_t)L::Q * kChunk * EB};
+  for (int m = 0; m < Pl::NMAPS; ++m) {
+    const int span = (Pl::map_count[m] - 1) * Pl::map_stride[m] + 1;
+    const cuuint32_t box[3] = {(cuuint32_t)kChunk, (cuuint32_t)span, (cuuint32_t)g.nch};
+    const cuuint32_t estr[3] = {1u, (cuuint32_t)Pl::map_stride[m], 1u};
+    const CUresult r = encode(&maps->m[m], dt, 3, a.f, dims, strides, box, estr,
+                              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                              CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return cudaErrorInvalidValue;
+  }
+  return cudaSuccess;
+}
+
+// Persistent row kernel: one CTA of nch warps per row, as many CTAs as are
+// resident (occupancy queried once per device and row width).
+template <int OP, int EQ, bool SH, bool FORCE>
+cudaError_t launch_rows(const StepArgs& a, cudaStream_t s) {
+  using Cfg = RowsCfg<L, ST>;
+  const Geo& g = a.g;
+  if (g.nch < 1 || g.nch > kRowsMaxWarps || (g.nx % kChunk) != 0 || Cfg::SMEM > kRowsSmemMax)
+    return cudaErrorInvalidValue;
+  auto kern = step_rows<L, ST, OP, EQ, SH, FORCE>;
+  const int threads = g.nch * 32;
+  constexpr int kMaxDev = 64;
+  static int cached[kMaxDev][kRowsMaxWarps + 1];
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= kMaxDev) return cudaErrorInvalidDevice;
+  if (cached[dev][g.nch] == 0) {
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, Cfg::SMEM);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0, nsm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, Cfg::SMEM);
+    if (e != cudaSuccess) return e;
+    e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) return cudaErrorInvalidConfiguration;
+    cached[dev][g.nch] = per_sm * nsm;
+  }
+  RowMaps<L> maps;
+  e = rows_maps(a, &maps);
+  if (e != cudaSuccess) return e;
+  const long long rows = (long long)g.ny * g.nz;
+  const unsigned grid = (unsigned)(rows < cached[dev][g.nch] ? rows : cached[dev][g.nch]);
+  kern<<<grid, threads, Cfg::SMEM, s>>>(a, maps);
+  return cudaGetLastError();
+}
 
 template <int OP, int EQ, bool SH, bool FORCE>
 cudaError_t step_t(const StepArgs& a, int kernel, cudaStream_t s) {
   const Geo& g = a.g;
+  if (kernel == kKernelRows) return launch_rows<OP, EQ, SH, FORCE>(a, s);
   if (kernel == kKernelStream) return launch_stream<OP, EQ, SH, FORCE>(a, s);
   if (kernel == kKernelPairs) {
     // one warp per 64-node chunk of every interior row

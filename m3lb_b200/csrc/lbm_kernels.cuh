@@ -165,7 +165,7 @@ __device__ __forceinline__ int chunk_delta(int Q, int xa, int xb) {
 // two for FP64 pairs, which need twice the registers per value.
 template <int OP, int ST>
 constexpr int pair_min_blocks() {
-  return ST == kF64 ? 2 : ((OP == 1 || OP == 2 || (OP == 0 && ST == kF32)) ? 3 : 4);
+  return ST == kF64 ? 2 : ((OP == 1 || OP == 2 || (OP == 0 && ST == kF32)) ? 3 : (OP >= 3 && ST != kF32 ? 5 : 4));
 }
 
 // One 64-node chunk (unit `warp` of the lattice's ny * nz * nch chunks) by

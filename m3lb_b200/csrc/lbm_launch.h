@@ -11,7 +11,9 @@ namespace m3lb {
 // Step kernels: one node per thread (any geometry), and, for a periodic x
 // axis with even nx, the paired kernel (one warp per 64-node chunk) or its
 // persistent, copy-pipelined form.
-enum StepKernel { kKernelNodes = 1, kKernelPairs = 2, kKernelStream = 3 };
+// The row kernel moves whole rows with the tensor-memory accelerator (nx a
+// multiple of 64, at most 8 chunks per row).
+enum StepKernel { kKernelNodes = 1, kKernelPairs = 2, kKernelStream = 3, kKernelRows = 4 };
 
 struct Launchers {
   // one step with the given StepKernel

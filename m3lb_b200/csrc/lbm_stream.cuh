@@ -69,15 +69,15 @@ struct XWord {
 };
 
 // Shared-memory ring of the streamed kernel, per warp: STAGES buffers of
-// Q * 32 words (one per lane and direction) plus 16 chunk-edge words.
+// (Q + NX) * 32 words: word q of lane l at [q * 32 + l], then the lane's
+// chunk-edge word of x-shifted direction e at [(Q + e) * 32 + l].
 template <class L, int ST>
 struct StreamCfg {
   using W = typename WordOps<ST>::W;
   static constexpr int WARPS = kPairThreads / 32;
-  static constexpr int STAGES = sizeof(W) == 4 ? 3 : 2;
-  static constexpr int EDGE_WORDS = 16;
-  static_assert(xshift_count<L>() <= EDGE_WORDS, "edge region too small");
-  static constexpr int STAGE_WORDS = L::Q * 32 + EDGE_WORDS;
+  static constexpr int STAGES = 2;
+  static constexpr int NX = xshift_count<L>();
+  static constexpr int STAGE_WORDS = (L::Q + NX) * 32;
   static constexpr int WARP_BYTES = STAGES * STAGE_WORDS * (int)sizeof(W);
   static constexpr int SMEM = WARPS * WARP_BYTES;
 };
@@ -108,8 +108,10 @@ struct Cursor {
 // Position of one lane in chunk k of a row: its node pair and how the ±1 x
 // shift reaches the neighbouring pairs (lane shuffle inside the chunk, or an
 // element of the adjacent chunk at the chunk edge and the periodic wrap).
-// `full` (nx a multiple of 64, at least two chunks per row: every chunk is
-// full and only lanes 31 and 0 cross a chunk edge) takes a short path.
+// FULL (nx a multiple of 64, at least two chunks per row: every chunk is
+// full and only lanes 31 and 0 cross a chunk edge) fixes all but the two
+// edge offsets at compile time.
+template <bool FULL>
 struct LaneX {
   int x0;
   int nxt_off;      // element offset from this lane's word to x0 + 2 (wrapped), same direction
@@ -117,9 +119,9 @@ struct LaneX {
   int nxt_src, prv_src;
   bool active, nxt_in, prv_in;
 
-  __device__ __forceinline__ void set(int Q, int nx, int nch, int k, int lane, bool full) {
+  __device__ __forceinline__ void set(int Q, int nx, int nch, int k, int lane) {
     x0 = k * kChunk + 2 * lane;
-    if (full) {
+    if constexpr (FULL) {
       active = true;
       nxt_in = lane != 31;
       prv_in = lane != 0;
@@ -129,18 +131,18 @@ struct LaneX {
       // 63 of chunk k - 1 (or of chunk nch - 1); other lanes do not use them
       nxt_off = (k == nch - 1 ? -(nch - 1) * Q * kChunk : Q * kChunk) - 62;
       prv_off = (k == 0 ? (nch - 1) * Q * kChunk : -Q * kChunk) + 63;
-      return;
+    } else {
+      active = x0 < nx;
+      int xn = x0 + 2; if (xn >= nx) xn -= nx;
+      int xp = x0 - 2; if (xp < 0) xp += nx;
+      nxt_in = (xn >> 6) == k;
+      prv_in = (xp >> 6) == k;
+      nxt_src = nxt_in ? ((xn & 63) >> 1) : lane;
+      prv_src = prv_in ? ((xp & 63) >> 1) : lane;
+      int xm = x0 - 1; if (xm < 0) xm += nx;
+      nxt_off = chunk_delta(Q, x0, xn);
+      prv_off = chunk_delta(Q, x0, xm);
     }
-    active = x0 < nx;
-    int xn = x0 + 2; if (xn >= nx) xn -= nx;
-    int xp = x0 - 2; if (xp < 0) xp += nx;
-    nxt_in = (xn >> 6) == k;
-    prv_in = (xp >> 6) == k;
-    nxt_src = nxt_in ? ((xn & 63) >> 1) : lane;
-    prv_src = prv_in ? ((xp & 63) >> 1) : lane;
-    int xm = x0 - 1; if (xm < 0) xm += nx;
-    nxt_off = chunk_delta(Q, x0, xn);
-    prv_off = chunk_delta(Q, x0, xm);
   }
 };
 
@@ -156,20 +158,31 @@ struct ChunkPtrs {
   E* own;
   E* rem[3][3];
 
-  // Al: the populations plus this lane's element offset 2 * lane
+  // Al: the populations plus this lane's element offset 2 * lane.  An
+  // interior row's neighbours are padded rows on a non-periodic axis (the
+  // halo), so only a periodic axis wraps.
   __device__ __forceinline__ void set(const Geo& g, E* Al, int P, const Cursor& c) {
     constexpr int Q = L::Q;
     const int py = c.yi + g.hy, pz = c.zi + g.hz;
     const unsigned rowel = (unsigned)g.nch * (unsigned)(Q * kChunk);
     E* kb = Al + c.k * (Q * kChunk);
-    own = kb + (size_t)(unsigned)(pz * g.sy + py) * rowel + P * kChunk;
-    E* kb1 = kb + (1 - P) * kChunk;
-    int yy[3], zs[3];
-#pragma unroll
-    for (int d = -1; d <= 1; ++d) {
-      yy[d + 1] = d == 0 ? py : shift_coord(py + d, g.hy, g.ny, g.sy, g.py);
-      zs[d + 1] = (L::D == 3 && d != 0 ? shift_coord(pz + d, g.hz, g.nz, g.sz, g.pz) : pz) * g.sy;
+    int ym = py - 1, yp = py + 1;
+    if (ym < 0) ym += g.ny;
+    if (yp >= g.sy) yp -= g.ny;
+    const int yy[3] = {ym, py, yp};
+    int zs[3];
+    zs[1] = pz * g.sy;
+    if constexpr (L::D == 3) {
+      int zm = pz - 1, zp = pz + 1;
+      if (zm < 0) zm += g.nz;
+      if (zp >= g.sz) zp -= g.nz;
+      zs[0] = zm * g.sy;
+      zs[2] = zp * g.sy;
+    } else {
+      zs[0] = zs[2] = zs[1];
     }
+    own = kb + (size_t)(unsigned)(zs[1] + py) * rowel + P * kChunk;
+    E* kb1 = kb + (1 - P) * kChunk;
 #pragma unroll
     for (int dz = 0; dz < 3; ++dz)
 #pragma unroll
@@ -248,7 +261,7 @@ constexpr int stream_min_blocks() {
   return ST == kF64 ? 2 : pair_min_blocks<OP, ST>();
 }
 
-template <class L, int ST, int OP, int EQ, bool SH, bool FORCE>
+template <class L, int ST, int OP, int EQ, bool SH, bool FORCE, bool FULL>
 __global__ void __launch_bounds__(kPairThreads, stream_min_blocks<OP, ST>())
 step_stream(StepArgs a) {
   using WO = WordOps<ST>;
@@ -258,9 +271,11 @@ step_stream(StepArgs a) {
   using V = typename WO::V;
   using S = typename Lanes<V>::S;
   using Cfg = StreamCfg<L, ST>;
+  using XW = XWord<ST>;
   constexpr int Q = L::Q;
   constexpr int NS = Cfg::STAGES;
   constexpr int WB = (int)sizeof(W);
+  constexpr int EB = (int)sizeof(E);
   const Geo& g = a.g;
 
   extern __shared__ __align__(16) unsigned char stream_smem[];
@@ -278,42 +293,38 @@ step_stream(StepArgs a) {
 
   E* Al = reinterpret_cast<E*>(a.f) + 2 * lane;
   const int P = a.parity;
-  const bool full = (g.nx & 63) == 0 && g.nch >= 2;
   const CollideParams<S> prm{(S)a.omega, (S)a.omega2, (S)a.fx, (S)a.fy, (S)a.fz};
 
   unsigned char* ring = stream_smem + wib * Cfg::WARP_BYTES;
-  const uint32_t ring_base = (uint32_t)__cvta_generic_to_shared(ring);
-  const uint32_t ring_s = ring_base + (uint32_t)(lane * WB);  // this lane's word 0, stage 0
-  const uint32_t edge_s = ring_base + (uint32_t)(Q * 32 * WB);
+  // this lane's word 0 of stage 0, in the shared window
+  const uint32_t ring_s = (uint32_t)__cvta_generic_to_shared(ring) + (uint32_t)(lane * WB);
 
-  // Copy one chunk into stage buffer `st`: the lane's Q words (zero fill on
-  // lanes past the end of a partial chunk) and, on the chunk-edge lane, the
+  // Copy one chunk into stage buffer `st`: the lane's Q words, and the
   // neighbouring chunk's word of each x-shifted direction (the word holding
-  // element x0 + 2, or x0 - 1).  At most one lane of a chunk lacks its x + 2
-  // neighbour in the chunk, and at most one its x - 1 neighbour, so each
-  // edge slot has a single writer.
+  // element x0 + 2, or x0 - 1), read only on the chunk-edge lane; every
+  // other copy of an edge word, and every copy on a lane past the end of a
+  // partial chunk, reads nothing and fills zeros.
   auto issue = [&](const Cursor& cu, int st) {
-    LaneX lx;
-    lx.set(Q, g.nx, g.nch, cu.k, lane, full);
+    LaneX<FULL> lx;
+    lx.set(Q, g.nx, g.nch, cu.k, lane);
     ChunkPtrs<L, ST> cp;
     cp.set(g, Al, P, cu);
     const uint32_t sb = ring_s + (uint32_t)(st * Cfg::STAGE_WORDS * WB);
-    const uint32_t se = edge_s + (uint32_t)(st * Cfg::STAGE_WORDS * WB);
     const int nb = lx.active ? WB : 0;
-    const bool en = lx.active && !lx.nxt_in, ep = lx.active && !lx.prv_in;
-    constexpr int EB = (int)sizeof(E);
-    const E* rest = cp.own - P * kChunk;
-    copy_async<WB, 0, 0>(sb, rest, nb);
+    const int nbn = (lx.active && !lx.nxt_in) ? WB : 0;
+    const int nbp = (lx.active && !lx.prv_in) ? WB : 0;
+    copy_async<WB, 0, 0>(sb, cp.own - P * kChunk, nb);
     static_for<1, Q, 2>([&](auto I) {
       constexpr int i = decltype(I)::value;
       constexpr int cx = L::cx[i], cy = L::cy[i], cz = L::cz[i];
       const E* rp = cp.rem[cz + 1][cy + 1];
       copy_async<WB, i * 32 * WB, i * kChunk * EB>(sb, cp.own, nb);
       copy_async<WB, (i + 1) * 32 * WB, i * kChunk * EB>(sb, rp, nb);
+      constexpr int ed = (Q + (xshift_index<L>(i) < 0 ? 0 : xshift_index<L>(i))) * 32 * WB;
       if constexpr (cx > 0) {
-        copy_async_if<WB, xshift_index<L>(i) * WB>(en, se, rp + i * kChunk + lx.nxt_off);
+        copy_async<WB, ed, i * kChunk * EB>(sb, rp + lx.nxt_off, nbn);
       } else if constexpr (cx < 0) {
-        copy_async_if<WB, xshift_index<L>(i) * WB>(ep, se, rp + i * kChunk + lx.prv_off - 1);
+        copy_async<WB, ed, i * kChunk * EB>(sb, rp + lx.prv_off - 1, nbp);
       }
     });
   };
@@ -341,26 +352,26 @@ step_stream(StepArgs a) {
     }
     // this chunk's copies (the oldest pending group) have landed
     copy_wait<NS - 1>();
-    const W* sw = reinterpret_cast<const W*>(ring + st * Cfg::STAGE_WORDS * WB);
+    const W* sw = reinterpret_cast<const W*>(ring + st * Cfg::STAGE_WORDS * WB) + lane;
     W w[Q];
 #pragma unroll
-    for (int q = 0; q < Q; ++q) w[q] = sw[q * 32 + lane];
+    for (int q = 0; q < Q; ++q) w[q] = sw[q * 32];
 
-    LaneX lx;
-    lx.set(Q, g.nx, g.nch, cur.k, lane, full);
+    LaneX<FULL> lx;
+    lx.set(Q, g.nx, g.nch, cur.k, lane);
     // ±1 x shift of the remote words (shuffle, or the chunk-edge word)
-    using XW = XWord<ST>;
     static_for<1, Q, 2>([&](auto I) {
       constexpr int i = decltype(I)::value;
       constexpr int cx = L::cx[i];
-      if constexpr (cx > 0) {
-        const W nw = XW::shfl_lo(w[i + 1], lx.nxt_src);
-        const W ew = sw[Q * 32 + xshift_index<L>(i)];
-        w[i + 1] = XW::join(w[i + 1], lx.nxt_in ? nw : ew);
-      } else if constexpr (cx < 0) {
-        const W pw = XW::shfl_hi(w[i + 1], lx.prv_src);
-        const W ew = sw[Q * 32 + xshift_index<L>(i)];
-        w[i + 1] = XW::join(lx.prv_in ? pw : ew, w[i + 1]);
+      if constexpr (cx != 0) {
+        const W ew = sw[(Q + xshift_index<L>(i)) * 32];
+        if constexpr (cx > 0) {
+          const W nw = XW::shfl_lo(w[i + 1], lx.nxt_src);
+          w[i + 1] = XW::join(w[i + 1], lx.nxt_in ? nw : ew);
+        } else {
+          const W pw = XW::shfl_hi(w[i + 1], lx.prv_src);
+          w[i + 1] = XW::join(lx.prv_in ? pw : ew, w[i + 1]);
+        }
       }
     });
 
@@ -417,27 +428,25 @@ step_stream(StepArgs a) {
     // belongs to the adjacent chunk goes out on its own
     const bool st_w_n = lx.active && lx.nxt_in, st_h_n = lx.active && !lx.nxt_in;
     const bool st_w_p = lx.active && lx.prv_in, st_h_p = lx.active && !lx.prv_in;
-    constexpr int EB = (int)sizeof(E);
-    st_if<0>(lx.active, cp.own - P * kChunk, w[0]);
+    if (lx.active) *reinterpret_cast<W*>(cp.own - P * kChunk) = w[0];
     static_for<1, Q, 2>([&](auto I) {
       constexpr int i = decltype(I)::value;
       constexpr int cx = L::cx[i], cy = L::cy[i], cz = L::cz[i];
-      constexpr int off = i * kChunk * EB;
       const W oi = w[i], oj = w[i + 1];
-      st_if<off>(lx.active, cp.own, oj);
-      E* rb = cp.rem[cz + 1][cy + 1];
+      if (lx.active) *reinterpret_cast<W*>(cp.own + i * kChunk) = oj;
+      E* rp = cp.rem[cz + 1][cy + 1] + i * kChunk;
       if constexpr (cx == 0) {
-        st_if<off>(lx.active, rb, oi);
+        if (lx.active) *reinterpret_cast<W*>(rp) = oi;
       } else if constexpr (cx > 0) {
         const W pw = XW::shfl_hi(oi, lx.prv_src);
-        st_if<off>(st_w_p, rb, XW::join(pw, oi));
-        st_if<off + EB>(st_h_p, rb, WO::lo(oi));
-        st_if<off>(st_h_n, rb + lx.nxt_off, WO::hi(oi));
+        if (st_w_p) *reinterpret_cast<W*>(rp) = XW::join(pw, oi);
+        if (st_h_p) *reinterpret_cast<H*>(rp + 1) = WO::lo(oi);
+        if (st_h_n) *reinterpret_cast<H*>(rp + lx.nxt_off) = WO::hi(oi);
       } else {
         const W nw = XW::shfl_lo(oi, lx.nxt_src);
-        st_if<off>(st_w_n, rb, XW::join(oi, nw));
-        st_if<off>(st_h_n, rb, WO::hi(oi));
-        st_if<off>(st_h_p, rb + lx.prv_off, WO::lo(oi));
+        if (st_w_n) *reinterpret_cast<W*>(rp) = XW::join(oi, nw);
+        if (st_h_n) *reinterpret_cast<H*>(rp) = WO::hi(oi);
+        if (st_h_p) *reinterpret_cast<H*>(rp + lx.prv_off) = WO::lo(oi);
       }
     });
 
