@@ -97,9 +97,47 @@ int m3lb_set_params(m3lb_solver* h, double omega, double omega2, double fx, doub
                     double fz);
 
 /* set_geometry(fn(x, y, z) -> CellType) (:74-82), the result of fn given as
- * an array over interior nodes.  RegWall / SpecWall / SpecNode cells are not
- * offered (M3LB_ERR_UNSUPPORTED). */
+ * an array over interior nodes: 0 Fluid, 1 Solid, 2 Excluded.  Resets every
+ * interior flag, specular ones included; RegWall (3) is not offered and the
+ * specular types (4, 5) are set by the two calls below (M3LB_ERR_UNSUPPORTED
+ * for any value above 2). */
 int m3lb_set_flags(m3lb_solver* h, const uint8_t* flags);
+
+/* Normal codes of set_specular_walls (src/boundary/Regularized.hpp:97-102):
+ * the outward normal of the wall. */
+#define M3LB_NRM_NONE 0
+#define M3LB_NRM_XP 1
+#define M3LB_NRM_XM 2
+#define M3LB_NRM_YP 3
+#define M3LB_NRM_YM 4
+#define M3LB_NRM_ZP 5
+#define M3LB_NRM_ZM 6
+/* Face bits of set_specular_nodes (src/boundary/Specular.hpp:226-234). */
+#define M3LB_SPEC_XP 0x01
+#define M3LB_SPEC_XM 0x02
+#define M3LB_SPEC_YP 0x04
+#define M3LB_SPEC_YM 0x08
+#define M3LB_SPEC_ZP 0x10
+#define M3LB_SPEC_ZM 0x20
+
+/* set_specular_walls(fn(x, y, z) -> NormalCode) (FluidSolver.hpp:193-218),
+ * one code per interior node: 0 leaves the node as it is, 1..6 marks it a
+ * SpecWall, a free-slip GHOST that reflects its incoming populations about
+ * that axis (f_i <- f_m(i)) and does not collide (Specular.hpp:1-90); the
+ * plane lies halfway between it and the last fluid node.  Codes above 6
+ * (corner, outflow) are rejected with M3LB_ERR_INVALID and nothing changes
+ * (the reference aborts).  Call after m3lb_set_flags, which resets flags. */
+int m3lb_set_specular_walls(m3lb_solver* h, const uint8_t* normal_codes);
+
+/* set_specular_nodes(fn(x, y, z) -> SpecFace mask) (FluidSolver.hpp:236-268),
+ * one mask per interior node: 0 leaves the node, any other mask marks it a
+ * SpecNode, a fluid node that replaces each direction pointing into the
+ * domain across a masked face by its mirror image (composed over the masked
+ * axes, so edges and corners work) and then collides (Specular.hpp:186-278).
+ * Masks above 0x3F or with both faces of one axis are rejected with
+ * M3LB_ERR_INVALID and nothing changes.  While any specular node exists the
+ * step runs in the one-node kernel.  Call after m3lb_set_flags. */
+int m3lb_set_specular_nodes(m3lb_solver* h, const uint8_t* face_masks);
 
 /* initialize(rho0, ux, uy, uz) (:553-561): equilibrium on fluid nodes, rest
  * equilibrium at rho0 elsewhere; resets the time step to 0. */
@@ -164,7 +202,8 @@ int m3lb_launch_count(const m3lb_solver* h, long long* n);
  * The reduction of m3lb_reduce for callers that cannot allocate device memory
  * (who therefore cannot create a handle, which allocates): the caller passes
  * the population array and flags it holds (device pointers, the layout of
- * m3lb_populations; flags per padded node, or NULL for an all-fluid interior),
+ * m3lb_populations; flags per padded node, or NULL for an all-fluid interior;
+ * any nonzero flag, specular ones included, excludes the node from the sums),
  * the lattice description, the time step (for the parity) and a device array
  * `out` of six doubles receiving the same sums as m3lb_reduce.  Queued on
  * `stream`; returns without waiting.  Allocates nothing: the partial sums use

@@ -76,6 +76,8 @@ SIGNATURES = {
     "m3lb_destroy": (_i, [_vp]),
     "m3lb_set_params": (_i, [_vp] + [_d] * 5),
     "m3lb_set_flags": (_i, [_vp, _vp]),
+    "m3lb_set_specular_walls": (_i, [_vp, _vp]),
+    "m3lb_set_specular_nodes": (_i, [_vp, _vp]),
     "m3lb_init_eq": (_i, [_vp] + [_d] * 4),
     "m3lb_init_field_f32": (_i, [_vp] + [_vp] * 4),
     "m3lb_init_field_f64": (_i, [_vp] + [_vp] * 4),

@@ -120,6 +120,12 @@ struct m3lb_solver {
   uint8_t* flags = nullptr;          // per padded node
   std::vector<uint8_t> flags_host;   // per padded node
   bool has_geometry = false;
+  // specular walls (FluidSolver.hpp:193-268): per padded node the SpecWall
+  // normal code and the SpecNode face mask, and on the device one byte per
+  // node holding whichever the node's flag selects
+  std::vector<uint8_t> spec_nrm_host, spec_faces_host;
+  uint8_t* spec = nullptr;
+  bool has_spec = false;
   void* macro[4] = {nullptr, nullptr, nullptr, nullptr};  // interior, arithmetic type
   void* staging = nullptr;           // init_field uploads (4 interior arrays)
   double* partials = nullptr;        // reduction scratch
@@ -139,6 +145,7 @@ struct m3lb_solver {
     a.g = g;
     a.f = f;
     a.flags = has_geometry ? flags : nullptr;
+    a.spec = has_spec ? spec : nullptr;
     a.parity = (int)(t & 1);
     a.omega = omega; a.omega2 = omega2;
     a.fx = forcing ? fx : 0; a.fy = forcing ? fy : 0; a.fz = forcing ? fz : 0;
@@ -149,7 +156,8 @@ struct m3lb_solver {
   // one-node kernel runs everything.
   bool chunk_ok() const { return g.px && g.hx == 0 && (g.nx % 2) == 0; }
   int step_kernel() const {
-    if (node_kernel || !chunk_ok() || kernel == M3LB_KERNEL_NODES) return kKernelNodes;
+    // specular nodes run in the one-node kernel
+    if (node_kernel || has_spec || !chunk_ok() || kernel == M3LB_KERNEL_NODES) return kKernelNodes;
     // the streamed kernel addresses rows with 32-bit element counts
     const bool rows32 = (long long)g.nch * Q * 64 < (1LL << 31);
     // the row kernel: whole rows of at most 8 full chunks
@@ -257,6 +265,7 @@ int m3lb_destroy(m3lb_solver* h) {
   if (h->stream) cudaStreamSynchronize(h->stream);
   cudaFree(h->f);
   cudaFree(h->flags);
+  cudaFree(h->spec);
   for (void* p : h->macro) cudaFree(p);
   cudaFree(h->staging);
   cudaFree(h->partials);
@@ -271,27 +280,118 @@ int m3lb_set_params(m3lb_solver* h, double omega, double omega2, double fx, doub
   return M3LB_OK;
 }
 
+}  // extern "C"
+
+// Upload the host flags and, where specular nodes exist, their per-node
+// normal / mask byte; recompute which kernels the geometry allows.
+static int upload_geometry(m3lb_solver* h) {
+  const Geo& g = h->g;
+  bool any = false, spec = false;
+  for (int z = 0; z < g.nz; ++z)
+    for (int y = 0; y < g.ny; ++y)
+      for (int x = 0; x < g.nx; ++x) {
+        const uint8_t v = h->flags_host[((size_t)(z + g.hz) * g.sy + (y + g.hy)) * g.sx + (x + g.hx)];
+        any |= v != 0;
+        spec |= v == kSpecWall || v == kSpecNode;
+      }
+  DeviceGuard dg(h->device);
+  CUDA_TRY(cudaMemcpyAsync(h->flags, h->flags_host.data(), (size_t)g.n_padded,
+                           cudaMemcpyHostToDevice, h->stream));
+  std::vector<uint8_t> sp;
+  if (spec) {
+    if (!h->spec && cudaMalloc((void**)&h->spec, (size_t)g.n_padded) != cudaSuccess) {
+      h->spec = nullptr;
+      return fail(M3LB_ERR_MEMORY, "specular: cannot allocate %lld bytes", g.n_padded);
+    }
+    sp.assign((size_t)g.n_padded, 0);
+    for (size_t n = 0; n < sp.size(); ++n) {
+      const uint8_t v = h->flags_host[n];
+      if (v == kSpecWall && !h->spec_nrm_host.empty()) sp[n] = h->spec_nrm_host[n];
+      if (v == kSpecNode && !h->spec_faces_host.empty()) sp[n] = h->spec_faces_host[n];
+    }
+    CUDA_TRY(cudaMemcpyAsync(h->spec, sp.data(), sp.size(), cudaMemcpyHostToDevice, h->stream));
+  }
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  h->has_geometry = any;
+  h->has_spec = spec;
+  return M3LB_OK;
+}
+
+extern "C" {
 int m3lb_set_flags(m3lb_solver* h, const uint8_t* fl) {
   if (!h || !fl) return fail(M3LB_ERR_INVALID, "set_flags: null argument");
   const Geo& g = h->g;
-  bool any = false;
   for (int z = 0; z < g.nz; ++z)
     for (int y = 0; y < g.ny; ++y)
       for (int x = 0; x < g.nx; ++x) {
         const uint8_t v = fl[((size_t)z * g.ny + y) * g.nx + x];
         if (v > 2)
           return fail(M3LB_ERR_UNSUPPORTED,
-                      "set_flags: cell type %u at (%d,%d,%d): only Fluid, Solid and Excluded "
-                      "are offered", (unsigned)v, x, y, z);
-        any |= v != 0;
-        h->flags_host[((size_t)(z + g.hz) * g.sy + (y + g.hy)) * g.sx + (x + g.hx)] = v;
+                      "set_flags: cell type %u at (%d,%d,%d): Fluid, Solid and Excluded are set "
+                      "here, specular walls by m3lb_set_specular_walls / _nodes", (unsigned)v, x,
+                      y, z);
       }
-  DeviceGuard dg(h->device);
-  CUDA_TRY(cudaMemcpyAsync(h->flags, h->flags_host.data(), (size_t)g.n_padded,
-                           cudaMemcpyHostToDevice, h->stream));
-  CUDA_TRY(cudaStreamSynchronize(h->stream));
-  h->has_geometry = any;
-  return M3LB_OK;
+  for (int z = 0; z < g.nz; ++z)
+    for (int y = 0; y < g.ny; ++y)
+      for (int x = 0; x < g.nx; ++x)
+        h->flags_host[((size_t)(z + g.hz) * g.sy + (y + g.hy)) * g.sx + (x + g.hx)] =
+            fl[((size_t)z * g.ny + y) * g.nx + x];
+  return upload_geometry(h);
+}
+
+int m3lb_set_specular_walls(m3lb_solver* h, const uint8_t* codes) {
+  if (!h || !codes) return fail(M3LB_ERR_INVALID, "set_specular_walls: null argument");
+  const Geo& g = h->g;
+  for (int z = 0; z < g.nz; ++z)
+    for (int y = 0; y < g.ny; ++y)
+      for (int x = 0; x < g.nx; ++x) {
+        const unsigned c = codes[((size_t)z * g.ny + y) * g.nx + x];
+        if (c > 6)
+          return fail(M3LB_ERR_INVALID,
+                      "set_specular_walls: normal code %u at (%d,%d,%d) is not an axis normal; "
+                      "specular reflection is defined for codes 1..6 only", c, x, y, z);
+      }
+  h->spec_nrm_host.assign((size_t)g.n_padded, 0);
+  for (int z = 0; z < g.nz; ++z)
+    for (int y = 0; y < g.ny; ++y)
+      for (int x = 0; x < g.nx; ++x) {
+        const uint8_t c = codes[((size_t)z * g.ny + y) * g.nx + x];
+        if (!c) continue;
+        const size_t n = ((size_t)(z + g.hz) * g.sy + (y + g.hy)) * g.sx + (x + g.hx);
+        h->spec_nrm_host[n] = c;
+        h->flags_host[n] = kSpecWall;
+      }
+  return upload_geometry(h);
+}
+
+int m3lb_set_specular_nodes(m3lb_solver* h, const uint8_t* masks) {
+  if (!h || !masks) return fail(M3LB_ERR_INVALID, "set_specular_nodes: null argument");
+  const Geo& g = h->g;
+  for (int z = 0; z < g.nz; ++z)
+    for (int y = 0; y < g.ny; ++y)
+      for (int x = 0; x < g.nx; ++x) {
+        const unsigned m = masks[((size_t)z * g.ny + y) * g.nx + x];
+        if (m > 0x3F)
+          return fail(M3LB_ERR_INVALID,
+                      "set_specular_nodes: mask %u at (%d,%d,%d) has bits outside the six faces",
+                      m, x, y, z);
+        for (int a = 0; a < 3; ++a)
+          if ((m & (1u << (2 * a))) && (m & (1u << (2 * a + 1))))
+            return fail(M3LB_ERR_INVALID,
+                        "set_specular_nodes: mask %u at (%d,%d,%d) carries both faces of axis %d; "
+                        "an on-node mirror needs one plane per axis", m, x, y, z, a);
+      }
+  h->spec_faces_host.assign((size_t)g.n_padded, 0);
+  for (int z = 0; z < g.nz; ++z)
+    for (int y = 0; y < g.ny; ++y)
+      for (int x = 0; x < g.nx; ++x) {
+        const uint8_t m = masks[((size_t)z * g.ny + y) * g.nx + x];
+        if (!m) continue;
+        const size_t n = ((size_t)(z + g.hz) * g.sy + (y + g.hy)) * g.sx + (x + g.hx);
+        h->spec_faces_host[n] = m;
+        h->flags_host[n] = kSpecNode;
+      }
+  return upload_geometry(h);
 }
 
 static int seed(m3lb_solver* h, SeedArgs& a) {

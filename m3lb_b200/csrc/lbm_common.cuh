@@ -185,11 +185,17 @@ __host__ __device__ __forceinline__ int shift_coord(int v, int h, int n, int s, 
   return v;
 }
 
+// Cell types (src/boundary/Flags.hpp:20-32): 0 Fluid, 1 Solid, 2 Excluded,
+// 4 SpecWall (free-slip ghost), 5 SpecNode (on-node free slip).
+constexpr uint8_t kSpecWall = 4, kSpecNode = 5;
+
 // Parameters of one step launch, passed by value.
 struct StepArgs {
   Geo g;
   void* f;                 // populations
   const uint8_t* flags;    // per padded node (0 fluid); nullptr: all interior fluid
+  const uint8_t* spec;     // per padded node: SpecWall normal code / SpecNode face mask;
+                           // nullptr: no specular nodes (flags 4 and 5 then act as solid)
   void* rho;               // macroscopic outputs, per padded node, or nullptr
   void* ux;
   void* uy;

@@ -325,6 +325,109 @@ __device__ __forceinline__ size_t load_slot(const Geo& g, const NodeNb<L>& nb, i
   return slot<L::Q>(g, m[0], m[1], m[2], par == 0 ? i : i - 1);
 }
 
+// ------------------------------------------------------- specular walls
+// Free-slip cell types (src/boundary/Flags.hpp:20-32): a SpecWall node is a
+// ghost that reflects its whole incoming set about one axis and does not
+// collide; a SpecNode is a fluid node whose unknown directions take their
+// mirror images before it collides.  Both only permute values among the Q
+// slots the node already reads and writes, so they need no extra buffer.
+
+// Direction whose velocity is c_i with the components in `flip` (bit a =
+// axis a) negated: the axis mirrors of src/boundary/Specular.hpp:104-118,
+// composed as mirror_unknowns_faces (:263-278) composes them.
+template <class L>
+__host__ __device__ constexpr int mirror_of(int i, int flip) {
+  const int j = dir_of<L>((flip & 1) ? -L::cx[i] : L::cx[i], (flip & 2) ? -L::cy[i] : L::cy[i],
+                          (flip & 4) ? -L::cz[i] : L::cz[i]);
+  return j < 0 ? i : j;
+}
+template <class L>
+__host__ __device__ constexpr bool mirrors_are_permutations() {  // Specular.hpp:356-375
+  for (int a = 0; a < 3; ++a)
+    for (int i = 0; i < L::Q; ++i) {
+      const int j = mirror_of<L>(i, 1 << a);
+      if (mirror_of<L>(j, 1 << a) != i) return false;
+      const int c[3] = {L::cx[i], L::cy[i], L::cz[i]}, d[3] = {L::cx[j], L::cy[j], L::cz[j]};
+      for (int b = 0; b < 3; ++b)
+        if (d[b] != (b == a ? -c[b] : c[b])) return false;
+    }
+  return true;
+}
+static_assert(mirrors_are_permutations<D2Q9>() && mirrors_are_permutations<D3Q27>(),
+              "axis mirrors must permute the velocity set");
+// Axes a velocity has a nonzero component on (bit a = axis a).
+template <class L>
+__host__ __device__ constexpr int moving_axes(int i) {
+  return (L::cx[i] != 0 ? 1 : 0) | (L::cy[i] != 0 ? 2 : 0) | (L::cz[i] != 0 ? 4 : 0);
+}
+
+// mirror_axis (Specular.hpp:124-128): 0 for +-x, 1 for +-y, 2 otherwise.
+__device__ __forceinline__ int spec_axis(unsigned code) {
+  return (code == 1 || code == 2) ? 0 : ((code == 3 || code == 4) ? 1 : 2);
+}
+
+// SpecWall: f_i <- f_{m(i)} about one axis (FluidSolver.hpp:745-757).
+template <class L, class R>
+__device__ __forceinline__ void spec_wall_permute(R* f, int ax) {
+  R h[L::Q];
+#pragma unroll
+  for (int i = 0; i < L::Q; ++i) h[i] = f[i];
+  static_for<0, L::Q>([&](auto I) {
+    constexpr int i = decltype(I)::value;
+    f[i] = ax == 0 ? h[mirror_of<L>(i, 1)] : (ax == 1 ? h[mirror_of<L>(i, 2)] : h[mirror_of<L>(i, 4)]);
+  });
+}
+
+// SpecNode: mirror_unknowns_faces (Specular.hpp:263-278).  A direction
+// pointing into the domain across a masked face (c_ia * face_sign(a) < 0)
+// takes the value of its image over every such axis; the others are kept.
+template <class L, class R>
+__device__ __forceinline__ void spec_node_mirror(R* f, unsigned faces) {
+  int sg[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a)  // face_sign (:238-243): +x wins if both were set
+    sg[a] = ((faces >> (2 * a)) & 1u) ? 1 : (((faces >> (2 * a + 1)) & 1u) ? -1 : 0);
+  R h[L::Q];
+#pragma unroll
+  for (int i = 0; i < L::Q; ++i) h[i] = f[i];
+  static_for<1, L::Q>([&](auto I) {
+    constexpr int i = decltype(I)::value;
+    constexpr int cx = L::cx[i], cy = L::cy[i], cz = L::cz[i];
+    const int flip = (sg[0] * cx < 0 ? 1 : 0) | (sg[1] * cy < 0 ? 2 : 0) | (sg[2] * cz < 0 ? 4 : 0);
+    R v = h[i];
+    static_for<1, 8>([&](auto M) {
+      constexpr int m = decltype(M)::value;
+      if constexpr ((m & moving_axes<L>(i)) == m)
+        if (flip == m) v = h[mirror_of<L>(i, m)];
+    });
+    f[i] = v;
+  });
+}
+
+// Raw moments of a SpecNode after its mirror (compute_macroscopic,
+// FluidSolver.hpp:1061-1080): populations unshifted, rho = sum f_i, u =
+// sum f_i c_i / rho, no force correction.
+template <class L, int OP, bool SH, class R>
+__device__ __forceinline__ Macro<R> spec_node_moments(R* f) {
+  static_for<0, L::Q>([&](auto I) {
+    constexpr int i = decltype(I)::value;
+    if constexpr (SH && OP != 0) f[i] += R(weight<L, i>());
+  });
+  R sm = 0, mx = 0, my = 0, mz = 0;
+  static_for<0, L::Q>([&](auto I) {
+    constexpr int i = decltype(I)::value;
+    constexpr int cx = L::cx[i], cy = L::cy[i], cz = L::cz[i];
+    sm += f[i];
+    if constexpr (cx != 0) mx += cx > 0 ? f[i] : -f[i];
+    if constexpr (cy != 0) my += cy > 0 ? f[i] : -f[i];
+    if constexpr (cz != 0) mz += cz > 0 ? f[i] : -f[i];
+  });
+  const R ir = R(1) / sm;
+  Macro<R> m;
+  m.dens = sm; m.rho = sm; m.ux = mx * ir; m.uy = my * ir; m.uz = mz * ir;
+  return m;
+}
+
 template <class L, int ST, int OP, int EQ, bool SH, bool FORCE>
 __global__ void __launch_bounds__(kNodeThreads)
 step_nodes(StepArgs a) {
@@ -337,7 +440,11 @@ step_nodes(StepArgs a) {
   if (k >= nint) return;
   const int xi = (int)(k % g.nx), yi = (int)((k / g.nx) % g.ny), zi = (int)(k / ((long long)g.nx * g.ny));
   const int x = xi + g.hx, y = yi + g.hy, z = zi + g.hz;
-  if (a.flags && a.flags[((long long)z * g.sy + y) * g.sx + x] != 0) return;
+  const long long pn = ((long long)z * g.sy + y) * g.sx + x;
+  const unsigned fl = a.flags ? a.flags[pn] : 0u;
+  // Solid and Excluded skip (bounce-back is the identity on this storage);
+  // specular nodes run when their normals / masks are present
+  if (fl != 0 && !(a.spec && (fl == kSpecWall || fl == kSpecNode))) return;
   NodeNb<L> nb;
   node_neighbours<L>(g, x, y, z, nb);
   E* A = reinterpret_cast<E*>(a.f);
@@ -350,8 +457,14 @@ step_nodes(StepArgs a) {
     f[i] = to_real(A[slot<Q>(g, x, y, z, i + P)]);
     f[i + 1] = to_real(A[slot<Q>(g, m[0], m[1], m[2], i + 1 - P)]);
   }
-  const CollideParams<R> prm{(R)a.omega, (R)a.omega2, (R)a.fx, (R)a.fy, (R)a.fz};
-  const Macro<R> mc = collide<L, OP, EQ, SH, FORCE>(f, prm);
+  Macro<R> mc;
+  if (fl == kSpecWall) {
+    spec_wall_permute<L>(f, spec_axis(a.spec[pn]));
+  } else {
+    if (fl == kSpecNode) spec_node_mirror<L>(f, a.spec[pn]);
+    const CollideParams<R> prm{(R)a.omega, (R)a.omega2, (R)a.fx, (R)a.fy, (R)a.fz};
+    mc = collide<L, OP, EQ, SH, FORCE>(f, prm);
+  }
   A[slot<Q>(g, x, y, z, 0)] = from_real<E>(f[0]);
 #pragma unroll
   for (int i = 1; i < Q; i += 2) {
@@ -359,7 +472,7 @@ step_nodes(StepArgs a) {
     A[slot<Q>(g, m[0], m[1], m[2], i + 1 - P)] = from_real<E>(f[i]);
     A[slot<Q>(g, x, y, z, i + P)] = from_real<E>(f[i + 1]);
   }
-  if (a.rho) {
+  if (a.rho && fl != kSpecWall) {
     reinterpret_cast<R*>(a.rho)[k] = mc.rho;
     reinterpret_cast<R*>(a.ux)[k] = mc.ux;
     reinterpret_cast<R*>(a.uy)[k] = mc.uy;
@@ -489,7 +602,7 @@ __global__ void seed_kernel(SeedArgs a) {
   const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= g.n_padded) return;
   const int x = (int)(n % g.sx), y = (int)((n / g.sx) % g.sy), z = (int)(n / ((long long)g.sx * g.sy));
-  const bool fluid = a.flags[n] == 0;
+  const bool fluid = a.flags[n] == 0 || a.flags[n] == kSpecNode;  // SpecNode seeds as fluid
   R rho = (R)a.rho0, ux = 0, uy = 0, uz = 0;
   if (a.mode == 0) {
     if (fluid) { ux = (R)a.ux0; uy = (R)a.uy0; uz = (R)a.uz0; }
@@ -565,7 +678,10 @@ __global__ void macro_kernel(StepArgs a) {
   R* ux = reinterpret_cast<R*>(a.ux);
   R* uy = reinterpret_cast<R*>(a.uy);
   R* uz = reinterpret_cast<R*>(a.uz);
-  if (a.flags && a.flags[((long long)z * g.sy + y) * g.sx + x] != 0) {
+  const long long pn = ((long long)z * g.sy + y) * g.sx + x;
+  const unsigned fl = a.flags ? a.flags[pn] : 0u;
+  const bool spec_node = fl == kSpecNode && a.spec;
+  if (fl != 0 && !spec_node) {
     rho[k] = ux[k] = uy[k] = uz[k] = R(0);
     return;
   }
@@ -575,8 +691,14 @@ __global__ void macro_kernel(StepArgs a) {
   R f[Q];
 #pragma unroll
   for (int i = 0; i < Q; ++i) f[i] = to_real(A[load_slot<L>(g, nb, a.parity, i)]);
-  const CollideParams<R> prm{(R)a.omega, (R)a.omega2, (R)a.fx, (R)a.fy, (R)a.fz};
-  const Macro<R> m = macroscopic<L, OP, SH, FORCE>(f, prm);
+  Macro<R> m;
+  if (spec_node) {
+    spec_node_mirror<L>(f, a.spec[pn]);
+    m = spec_node_moments<L, OP, SH>(f);
+  } else {
+    const CollideParams<R> prm{(R)a.omega, (R)a.omega2, (R)a.fx, (R)a.fy, (R)a.fz};
+    m = macroscopic<L, OP, SH, FORCE>(f, prm);
+  }
   rho[k] = m.rho; ux[k] = m.ux; uy[k] = m.uy; uz[k] = m.uz;
 }
 
@@ -615,12 +737,16 @@ reduce_kernel(StepArgs a, double* partials) {
   for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < nint; k += stride) {
     const int xi = (int)(k % g.nx), yi = (int)((k / g.nx) % g.ny), zi = (int)(k / ((long long)g.nx * g.ny));
     const int x = xi + g.hx, y = yi + g.hy, z = zi + g.hz;
-    if (a.flags && a.flags[((long long)z * g.sy + y) * g.sx + x] != 0) continue;
+    const long long pn = ((long long)z * g.sy + y) * g.sx + x;
+    const unsigned fl = a.flags ? a.flags[pn] : 0u;
+    const bool spec_node = fl == kSpecNode && a.spec;
+    if (fl != 0 && !spec_node) continue;
     NodeNb<L> nb;
     node_neighbours<L>(g, x, y, z, nb);
     R f[Q];
 #pragma unroll
     for (int i = 0; i < Q; ++i) f[i] = to_real(A[load_slot<L>(g, nb, a.parity, i)]);
+    if (spec_node) spec_node_mirror<L>(f, a.spec[pn]);  // reduce, FluidSolver.hpp:1221-1222
     const Macro<R> m = macroscopic<L, OP, SH, FORCE>(f, prm);
     const double r = (double)m.rho, u = (double)m.ux, v = (double)m.uy, w = (double)m.uz;
     acc[0] += r;

@@ -11,7 +11,8 @@
 //     StoreF64); by default it follows Real, or -DLBM_B200_STORAGE_F16 /
 //     _BF16 selects 16-bit storage for every solver;
 //   * the policies must be ones the device runs: D2Q9 / D3Q27; BGK, TRT,
-//     MomentCollision; NoForcing or Guo; Fluid, Solid and Excluded cells.
+//     MomentCollision; NoForcing or Guo; Fluid, Solid and Excluded cells
+//     and the free-slip SpecWall / SpecNode cells.
 //     Anything else fails to compile (static_assert) or is rejected at
 //     set_geometry.
 #pragma once
@@ -23,6 +24,8 @@
 #include <vector>
 
 #include "boundary/Flags.hpp"
+#include "boundary/Regularized.hpp"
+#include "boundary/Specular.hpp"
 #include "collision/BGK.hpp"
 #include "collision/MomentCollision.hpp"
 #include "collision/TRT.hpp"
@@ -118,6 +121,33 @@ class FluidSolver {
     m3lb_facade::check(m3lb_set_flags(h_, a.data()), "set_geometry");
   }
 
+  // set_specular_walls (:193-218): fn(x, y, z) -> NormalCode; NrmNone leaves
+  // the node, an axis code marks it a free-slip ghost (SpecWall).  A code
+  // above NrmZm ends the program with the reference's message, as there.
+  template <class Fn>
+  void set_specular_walls(Fn fn) {
+    std::vector<std::uint8_t> a(std::size_t(dom_.n_interior()));
+    for (Index z = 0; z < dom_.nz; ++z)
+      for (Index y = 0; y < dom_.ny; ++y)
+        for (Index x = 0; x < dom_.nx; ++x)
+          a[(std::size_t(z) * dom_.ny + y) * dom_.nx + x] = std::uint8_t(fn(x, y, z));
+    m3lb_facade::check(m3lb_set_specular_walls(h_, a.data()), "set_specular_walls");
+    mark(a, SpecWall);
+  }
+
+  // set_specular_nodes (:236-268): fn(x, y, z) -> SpecFace mask; SpecNone
+  // leaves the node, any valid mask marks it an on-node free-slip node.
+  template <class Fn>
+  void set_specular_nodes(Fn fn) {
+    std::vector<std::uint8_t> a(std::size_t(dom_.n_interior()));
+    for (Index z = 0; z < dom_.nz; ++z)
+      for (Index y = 0; y < dom_.ny; ++y)
+        for (Index x = 0; x < dom_.nx; ++x)
+          a[(std::size_t(z) * dom_.ny + y) * dom_.nx + x] = std::uint8_t(fn(x, y, z));
+    m3lb_facade::check(m3lb_set_specular_nodes(h_, a.data()), "set_specular_nodes");
+    mark(a, SpecNode);
+  }
+
   // initialize (:553-561)
   void initialize(Real rho0, Real ux0 = 0, Real uy0 = 0, Real uz0 = 0) {
     push_params();
@@ -134,7 +164,7 @@ class FluidSolver {
       for (Index y = 0; y < dom_.ny; ++y)
         for (Index x = 0; x < dom_.nx; ++x) {
           const Index n = dom_.id(x, y, z);
-          if (flags_(n) != Fluid) continue;
+          if (flags_(n) != Fluid && flags_(n) != SpecNode) continue;
           const FlowState s = fn(n);
           const std::size_t k = (std::size_t(z) * dom_.ny + y) * dom_.nx + x;
           r[k] = s.rho; u[k] = s.ux; v[k] = s.uy; w[k] = s.uz;
@@ -211,6 +241,13 @@ class FluidSolver {
   }
 
  private:
+  // host copy of the flags after a specular setter marked the nonzero entries
+  void mark(const std::vector<std::uint8_t>& a, CellType type) {
+    for (Index z = 0; z < dom_.nz; ++z)
+      for (Index y = 0; y < dom_.ny; ++y)
+        for (Index x = 0; x < dom_.nx; ++x)
+          if (a[(std::size_t(z) * dom_.ny + y) * dom_.nx + x]) flags_(dom_.id(x, y, z)) = type;
+  }
   void push_params() {
     double w1 = 1, w2 = -1;
     coll_.device_rates(w1, w2);

@@ -96,6 +96,28 @@ class CellType(enum.IntEnum):
     SpecNode = 5
 
 
+class NormalCode(enum.IntEnum):
+    """Outward wall normals (Regularized.hpp:97-102), as set_specular_walls takes them."""
+    NrmNone = 0
+    NrmXp = 1
+    NrmXm = 2
+    NrmYp = 3
+    NrmYm = 4
+    NrmZp = 5
+    NrmZm = 6
+
+
+class SpecFace(enum.IntFlag):
+    """Face bits of an on-node specular mask (Specular.hpp:226-234)."""
+    SpecNone = 0
+    SpecXp = 0x01
+    SpecXm = 0x02
+    SpecYp = 0x04
+    SpecYm = 0x08
+    SpecZp = 0x10
+    SpecZm = 0x20
+
+
 # ---------------------------------------------------------------- policies
 class RawPopulations:
     name, shifted = "raw", False
@@ -331,6 +353,31 @@ class FluidSolver:
         fl = np.ascontiguousarray(fl, dtype=np.uint8).reshape(d.nz, d.ny, d.nx)
         capi.check(capi.lib().m3lb_set_flags(self._h, _ptr(fl)))
         self._flags = fl.copy()
+
+    def _per_node(self, fn_or_array):
+        d = self.dom
+        if callable(fn_or_array):
+            z, y, x = np.meshgrid(np.arange(d.nz), np.arange(d.ny), np.arange(d.nx), indexing="ij")
+            a = np.vectorize(lambda p, q, r: int(fn_or_array(p, q, r)), otypes=[np.uint8])(x, y, z)
+        else:
+            a = np.asarray(fn_or_array)
+        return np.ascontiguousarray(a, dtype=np.uint8).reshape(d.nz, d.ny, d.nx)
+
+    def set_specular_walls(self, fn_or_codes):
+        """Free-slip ghost walls (FluidSolver.hpp:193-218): fn(x, y, z) ->
+        NormalCode over interior coordinates, or the codes as an (nz, ny, nx)
+        array; NrmNone leaves a node as it is.  Call after set_geometry."""
+        codes = self._per_node(fn_or_codes)
+        capi.check(capi.lib().m3lb_set_specular_walls(self._h, _ptr(codes)))
+        self._flags = np.where(codes != 0, np.uint8(CellType.SpecWall), self._flags).astype(np.uint8)
+
+    def set_specular_nodes(self, fn_or_masks):
+        """On-node free-slip walls (FluidSolver.hpp:236-268): fn(x, y, z) ->
+        SpecFace mask, or the masks as an (nz, ny, nx) array; SpecNone leaves
+        a node as it is.  Call after set_geometry."""
+        masks = self._per_node(fn_or_masks)
+        capi.check(capi.lib().m3lb_set_specular_nodes(self._h, _ptr(masks)))
+        self._flags = np.where(masks != 0, np.uint8(CellType.SpecNode), self._flags).astype(np.uint8)
 
     def initialize(self, rho0=1.0, ux0=0.0, uy0=0.0, uz0=0.0):
         self._push_params()

@@ -38,6 +38,8 @@ def _bind(lib, prefix):
         "create": (_vp, [C.c_int] * 6 + [C.c_int] * 6 + [C.c_double] * 5),
         "destroy": (None, [_vp]),
         "set_geometry": (None, [_vp, _u8p]),
+        "set_specular_walls": (C.c_int, [_vp, _u8p]),
+        "set_specular_nodes": (C.c_int, [_vp, _u8p]),
         "initialize": (None, [_vp] + [C.c_double] * 4),
         "initialize_field": (None, [_vp] + [_dp] * 4),
         "step": (None, [_vp, C.c_int, C.c_int]),
@@ -149,6 +151,20 @@ class CpuSolver:
     def set_geometry(self, flags):
         fl = np.ascontiguousarray(flags, dtype=np.uint8).reshape(self.shape)
         self._f["set_geometry"](self._h, fl.ctypes.data_as(_u8p))
+
+    def set_specular_walls(self, codes):
+        """Normal code per interior node (0 none, 1..6 = +x -x +y -y +z -z);
+        FluidSolver.hpp:193-218.  Raises ValueError on a rejected code."""
+        a = np.ascontiguousarray(codes, dtype=np.uint8).reshape(self.shape)
+        if self._f["set_specular_walls"](self._h, a.ctypes.data_as(_u8p)) != 0:
+            raise ValueError("set_specular_walls: normal code outside 0..6")
+
+    def set_specular_nodes(self, masks):
+        """Face mask per interior node (bit 2a outward +a, bit 2a+1 outward
+        -a); FluidSolver.hpp:236-268.  Raises ValueError on a rejected mask."""
+        a = np.ascontiguousarray(masks, dtype=np.uint8).reshape(self.shape)
+        if self._f["set_specular_nodes"](self._h, a.ctypes.data_as(_u8p)) != 0:
+            raise ValueError("set_specular_nodes: mask outside 0x3F or with both faces of an axis")
 
     def initialize(self, rho0=1.0, ux=0.0, uy=0.0, uz=0.0):
         self._f["initialize"](self._h, rho0, ux, uy, uz)

@@ -31,7 +31,30 @@ static void build_dir_tables(void) {
   for (int i = 0; i < 9; ++i) D2Q9_DIR[D2Q9_CX[i] + 1][D2Q9_CY[i] + 1] = i;
   for (int i = 0; i < 27; ++i) D3Q27_DIR[D3Q27_CX[i] + 1][D3Q27_CY[i] + 1][D3Q27_CZ[i] + 1] = i;
 }
-__attribute__((constructor)) static void lbmo_init(void) { build_dir_tables(); }
+
+/* Mirror tables m[axis][i]: the direction whose velocity is c_i with
+ * component `axis` negated, i itself when there is none
+ * (src/boundary/Specular.hpp:104-118). */
+static int D2Q9_MIR[3][9];
+static int D3Q27_MIR[3][27];
+static void build_mirror_tables(void) {
+  for (int a = 0; a < 3; ++a) {
+    for (int i = 0; i < 9; ++i) {
+      int c[3] = {D2Q9_CX[i], D2Q9_CY[i], 0};
+      c[a] = -c[a];
+      D2Q9_MIR[a][i] = (c[2] == 0) ? D2Q9_DIR[c[0] + 1][c[1] + 1] : i;
+    }
+    for (int i = 0; i < 27; ++i) {
+      int c[3] = {D3Q27_CX[i], D3Q27_CY[i], D3Q27_CZ[i]};
+      c[a] = -c[a];
+      D3Q27_MIR[a][i] = D3Q27_DIR[c[0] + 1][c[1] + 1][c[2] + 1];
+    }
+  }
+}
+__attribute__((constructor)) static void lbmo_init(void) {
+  build_dir_tables();
+  build_mirror_tables();
+}
 
 /* float -> bfloat16 -> float, round to nearest even (NaN kept quiet). */
 static inline float lbmo_bf16_round(float v) {

@@ -19,7 +19,16 @@
  *
  * Codes: lattice 9 (D2Q9) / 27 (D3Q27); op 0 none (pure streaming), 1 BGK,
  * 2 TRT, 3 MRT, 4 central moments; eq 0 second order, 1 product form (BGK and
- * TRT only); flags per interior node: 0 fluid, 1 solid, 2 excluded.
+ * TRT only); flags per interior node: 0 fluid, 1 solid, 2 excluded, 4 specular
+ * ghost wall (SpecWall), 5 on-node specular wall (SpecNode).
+ *
+ * set_specular_walls takes one normal code per interior node (0 none, 1..6 =
+ * +x,-x,+y,-y,+z,-z outward normal) and marks the coded nodes SpecWall;
+ * set_specular_nodes takes one face mask per interior node (bit 2a: outward
+ * +axis a, bit 2a+1: outward -axis a) and marks the masked nodes SpecNode.
+ * Both return 0, or -1 without changing anything when a value is one the
+ * reference rejects (FluidSolver.hpp:193-268: a code above 6, a mask above
+ * 0x3F or with both faces of one axis).
  */
 #ifndef LBM_ORACLE_H
 #define LBM_ORACLE_H
@@ -31,6 +40,8 @@
                   double omega2, double fx, double fy, double fz);                   \
   void P##destroy(void* h);                                                          \
   void P##set_geometry(void* h, const uint8_t* flags);                               \
+  int P##set_specular_walls(void* h, const uint8_t* normal_codes);                   \
+  int P##set_specular_nodes(void* h, const uint8_t* face_masks);                     \
   void P##initialize(void* h, double rho, double ux, double uy, double uz);          \
   void P##initialize_field(void* h, const double* rho, const double* ux,             \
                            const double* uy, const double* uz);                      \

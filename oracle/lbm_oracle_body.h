@@ -19,6 +19,8 @@ typedef struct {
   R omega, omega2, fx, fy, fz;
   R* f;          /* populations, node-major: f[n*Q + q] (host LayoutRight) */
   uint8_t* flags;
+  uint8_t* spec_nrm;   /* SpecWall normal code per padded node */
+  uint8_t* spec_faces; /* SpecNode face mask per padded node */
   R *rho, *ux, *uy, *uz; /* stored macroscopic fields (StoreMacro) */
 } S(solver);
 
@@ -109,6 +111,34 @@ static inline void S(scatter1)(S(solver)* s, int par, long long n, const long lo
   else          { if (i & 1) A(n, i + 1) = v; else A(nb[i - 1], i - 1) = v; }
 }
 #undef A
+
+/* ---- Specular walls: src/boundary/Specular.hpp ---- */
+static inline int S(mir)(const S(solver)* s, int a, int i) {
+  return s->Q == 9 ? D2Q9_MIR[a][i] : D3Q27_MIR[a][i];
+}
+static inline int S(mirror_axis)(uint8_t code) {            /* :124-128 */
+  return (code == 1 || code == 2) ? 0 : ((code == 3 || code == 4) ? 1 : 2);
+}
+static inline int S(face_sign)(uint8_t faces, int a) {      /* :238-243 */
+  if (faces & (1u << (2 * a))) return 1;
+  if (faces & (1u << (2 * a + 1))) return -1;
+  return 0;
+}
+/* mirror_unknowns_faces (:263-278): every direction pointing into the domain
+ * across a masked face takes the value of its image, composed over the
+ * masked axes it crosses. */
+static void S(mirror_faces)(const S(solver)* s, R* f, uint8_t faces) {
+  R h[27];
+  for (int i = 0; i < s->Q; ++i) h[i] = f[i];
+  for (int i = 0; i < s->Q; ++i) {
+    int j = i, unknown = 0;
+    for (int a = 0; a < 3; ++a) {
+      const int sg = S(face_sign)(faces, a);
+      if (sg != 0 && S(c)(s, i, a) * sg < 0) { j = S(mir)(s, a, j); unknown = 1; }
+    }
+    if (unknown) f[i] = h[j];
+  }
+}
 
 /* ---- Equilibria: src/equilibrium/Equilibrium.hpp:28-124 ---- */
 static inline R S(phi)(const S(solver)* s, int i, R ux, R uy, R uz) {
@@ -403,6 +433,8 @@ void* F(create)(int lattice, int op, int eq, int shifted, int forcing, int quant
   s->fx = (R)fx; s->fy = (R)fy; s->fz = (R)fz;
   s->f = (R*)calloc((size_t)s->n_padded * s->Q, sizeof(R));
   s->flags = (uint8_t*)calloc((size_t)s->n_padded, 1);
+  s->spec_nrm = (uint8_t*)calloc((size_t)s->n_padded, 1);
+  s->spec_faces = (uint8_t*)calloc((size_t)s->n_padded, 1);
   s->rho = (R*)calloc((size_t)s->n_padded, sizeof(R));
   s->ux = (R*)calloc((size_t)s->n_padded, sizeof(R));
   s->uy = (R*)calloc((size_t)s->n_padded, sizeof(R));
@@ -417,7 +449,7 @@ void* F(create)(int lattice, int op, int eq, int shifted, int forcing, int quant
 void F(destroy)(void* h) {
   S(solver)* s = (S(solver)*)h;
   if (!s) return;
-  free(s->f); free(s->flags); free(s->rho); free(s->ux); free(s->uy); free(s->uz);
+  free(s->f); free(s->flags); free(s->spec_nrm); free(s->spec_faces); free(s->rho); free(s->ux); free(s->uy); free(s->uz);
   free(s);
 }
 void F(set_geometry)(void* h, const uint8_t* fl) {           /* :74-82 */
@@ -428,6 +460,46 @@ void F(set_geometry)(void* h, const uint8_t* fl) {           /* :74-82 */
         s->flags[S(idp)(s, x + s->hx, y + s->hy, z + s->hz)] =
             fl[((size_t)z * s->ny + y) * s->nx + x];
 }
+/* set_specular_walls (:193-218): interior normal codes, 0 = leave the node. */
+int F(set_specular_walls)(void* h, const uint8_t* codes) {
+  S(solver)* s = (S(solver)*)h;
+  const size_t nint = (size_t)s->nx * s->ny * s->nz;
+  for (size_t k = 0; k < nint; ++k)
+    if (codes[k] > 6) return -1;
+  memset(s->spec_nrm, 0, (size_t)s->n_padded);
+  for (int z = 0; z < s->nz; ++z)
+    for (int y = 0; y < s->ny; ++y)
+      for (int x = 0; x < s->nx; ++x) {
+        const uint8_t c = codes[((size_t)z * s->ny + y) * s->nx + x];
+        if (c == 0) continue;
+        const long long n = S(idp)(s, x + s->hx, y + s->hy, z + s->hz);
+        s->spec_nrm[n] = c;
+        s->flags[n] = 4;
+      }
+  return 0;
+}
+/* set_specular_nodes (:236-268): interior face masks, 0 = leave the node. */
+int F(set_specular_nodes)(void* h, const uint8_t* masks) {
+  S(solver)* s = (S(solver)*)h;
+  const size_t nint = (size_t)s->nx * s->ny * s->nz;
+  for (size_t k = 0; k < nint; ++k) {
+    const unsigned m = masks[k];
+    if (m > 0x3F) return -1;
+    for (int a = 0; a < 3; ++a)
+      if ((m & (1u << (2 * a))) && (m & (1u << (2 * a + 1)))) return -1;
+  }
+  memset(s->spec_faces, 0, (size_t)s->n_padded);
+  for (int z = 0; z < s->nz; ++z)
+    for (int y = 0; y < s->ny; ++y)
+      for (int x = 0; x < s->nx; ++x) {
+        const uint8_t m = masks[((size_t)z * s->ny + y) * s->nx + x];
+        if (m == 0) continue;
+        const long long n = S(idp)(s, x + s->hx, y + s->hy, z + s->hz);
+        s->spec_faces[n] = m;
+        s->flags[n] = 5;
+      }
+  return 0;
+}
 /* seed_populations -> scatter<P> (:634-637, 1231-1241), sequential node order. */
 static void S(scatter_fn)(S(solver)* s, const double* rho, const double* ux, const double* uy,
                           const double* uz, R rho0, R ux0, R uy0, R uz0, int field) {
@@ -435,7 +507,7 @@ static void S(scatter_fn)(S(solver)* s, const double* rho, const double* ux, con
   long long nb[27];
   for (long long n = 0; n < s->n_padded; ++n) {
     S(neighbours)(s, n, nb);
-    const int fluid = s->flags[n] == 0;
+    const int fluid = s->flags[n] == 0 || s->flags[n] == 5;  /* SpecNode seeds as fluid */
     R r = rho0, a = ux0, b = uy0, c = uz0;
     if (field) {                                             /* initialize_field :568-579 */
       r = (R)1; a = b = c = (R)0;
@@ -462,18 +534,28 @@ void F(initialize_field)(void* h, const double* rho, const double* ux, const dou
   s->t = 0;
   S(scatter_fn)(s, rho, ux, uy, uz, 0, 0, 0, 0, 1);
 }
-/* step -> run_step<P, StoreMacro> (:582-591, 712-1038), fluid branch only. */
+/* step -> run_step<P, StoreMacro> (:582-591, 712-1038): fluid, SpecWall
+ * (:745-757) and SpecNode (:791) branches. */
 void F(step)(void* h, int nsteps, int store_macro) {
   S(solver)* s = (S(solver)*)h;
   for (int t = 0; t < nsteps; ++t) {
     const int par = (int)(s->t % 2);
 #pragma omp parallel for schedule(static)
     for (long long n = 0; n < s->n_padded; ++n) {
-      if (s->flags[n] != 0) continue;                        /* Excluded / Solid skipped */
+      const uint8_t fl = s->flags[n];
+      if (fl != 0 && fl != 4 && fl != 5) continue;           /* Excluded / Solid skipped */
       long long nb[27];
       R f[27];
       S(neighbours)(s, n, nb);
       S(load_all)(s, par, n, nb, f);
+      if (fl == 4) {                                         /* ghost mirror, no collision */
+        const int ax = S(mirror_axis)(s->spec_nrm[n]);
+        R g[27];
+        for (int i = 0; i < s->Q; ++i) g[i] = f[S(mir)(s, ax, i)];
+        S(store_all)(s, par, n, nb, g);
+        continue;
+      }
+      if (fl == 5) S(mirror_faces)(s, f, s->spec_faces[n]);
       const S(macro_t) m = S(macroscopic)(s, f);
       if (s->op == 1) S(collide_bgk)(s, f, m);
       else if (s->op == 2) S(collide_trt)(s, f, m);
@@ -502,11 +584,27 @@ void F(macro)(void* h, double* rho, double* ux, double* uy, double* uz) {
   S(solver)* s = (S(solver)*)h;
   const int par = (int)(s->t % 2);
   for (long long n = 0; n < s->n_padded; ++n) {
-    if (s->flags[n] != 0) { s->rho[n] = s->ux[n] = s->uy[n] = s->uz[n] = (R)0; continue; }
+    const uint8_t fl = s->flags[n];
+    if (fl != 0 && fl != 5) { s->rho[n] = s->ux[n] = s->uy[n] = s->uz[n] = (R)0; continue; }
     long long nb[27];
     R f[27];
     S(neighbours)(s, n, nb);
     S(load_all)(s, par, n, nb, f);
+    if (fl == 5) {                                           /* :1061-1080, raw moments */
+      S(mirror_faces)(s, f, s->spec_faces[n]);
+      if (s->shifted && s->op != 0)                          /* no-collision runs raw */
+        for (int i = 0; i < s->Q; ++i) f[i] += S(w)(s, i);
+      R sm = 0, mx = 0, my = 0, mz = 0;
+      for (int i = 0; i < s->Q; ++i) {
+        sm += f[i];
+        mx += f[i] * (R)S(c)(s, i, 0);
+        my += f[i] * (R)S(c)(s, i, 1);
+        mz += f[i] * (R)S(c)(s, i, 2);
+      }
+      const R ir = (R)1 / sm;
+      s->rho[n] = sm; s->ux[n] = mx * ir; s->uy[n] = my * ir; s->uz[n] = mz * ir;
+      continue;
+    }
     const S(macro_t) m = S(macroscopic)(s, f);
     s->rho[n] = S(density)(s, m.dens);
     s->ux[n] = m.ux; s->uy[n] = m.uy; s->uz[n] = m.uz;
@@ -521,11 +619,12 @@ static double S(reduce)(S(solver)* s, int axis) {
   const int par = (int)(s->t % 2);
   R sum = 0;
   for (long long n = 0; n < s->n_padded; ++n) {
-    if (s->flags[n] != 0) continue;
+    if (s->flags[n] != 0 && s->flags[n] != 5) continue;
     long long nb[27];
     R f[27];
     S(neighbours)(s, n, nb);
     for (int i = 0; i < s->Q; ++i) f[i] = S(load1)(s, par, n, nb, i);
+    if (s->flags[n] == 5) S(mirror_faces)(s, f, s->spec_faces[n]);   /* :1221-1222 */
     const S(macro_t) m = S(macroscopic)(s, f);
     const R r = S(density)(s, m.dens);
     sum += (axis < 0) ? r : r * (axis == 0 ? m.ux : (axis == 1 ? m.uy : m.uz));

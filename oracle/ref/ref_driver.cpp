@@ -81,6 +81,25 @@ void* ref_create(int lattice, int streaming, int op, int eq, int shifted, int fo
 }
 void ref_destroy(void* h) { delete static_cast<refdrv::Base*>(h); }
 void ref_set_geometry(void* h, const std::uint8_t* f) { static_cast<refdrv::Base*>(h)->set_geometry(f); }
+// The reference aborts on a value it rejects; these check first and return -1
+// instead, so a caller's mistake cannot end the process.
+static long long ref_interior(void* h) { return static_cast<refdrv::Base*>(h)->n_interior(); }
+int ref_set_specular_walls(void* h, const std::uint8_t* codes) {
+  for (long long k = 0; k < ref_interior(h); ++k)
+    if (codes[k] > NrmZm) return -1;
+  static_cast<refdrv::Base*>(h)->set_specular_walls(codes);
+  return 0;
+}
+int ref_set_specular_nodes(void* h, const std::uint8_t* masks) {
+  for (long long k = 0; k < ref_interior(h); ++k) {
+    const unsigned m = masks[k];
+    if (m > 0x3F) return -1;
+    for (int a = 0; a < 3; ++a)
+      if ((m & (1u << (2 * a))) && (m & (1u << (2 * a + 1)))) return -1;
+  }
+  static_cast<refdrv::Base*>(h)->set_specular_nodes(masks);
+  return 0;
+}
 void ref_initialize(void* h, double r, double a, double b, double c) {
   static_cast<refdrv::Base*>(h)->initialize(r, a, b, c);
 }

@@ -10,6 +10,8 @@
 // Every entry point maps onto one public member of the reference solver:
 //   ref_create            FluidSolver(Domain, Collision)      FluidSolver.hpp:42
 //   ref_set_geometry      set_geometry(fn(x,y,z) -> CellType)  FluidSolver.hpp:74-82
+//   ref_set_specular_walls set_specular_walls(fn -> NormalCode) FluidSolver.hpp:193-218
+//   ref_set_specular_nodes set_specular_nodes(fn -> SpecFace)   FluidSolver.hpp:236-268
 //   ref_initialize        initialize(rho0, ux, uy, uz)         FluidSolver.hpp:553-561
 //   ref_initialize_field  initialize_field(fn(n) -> FlowState) FluidSolver.hpp:568-579
 //   ref_step              step(store_macroscopic)              FluidSolver.hpp:582-591
@@ -58,6 +60,8 @@ struct Params {
 struct Base {
   virtual ~Base() = default;
   virtual void set_geometry(const std::uint8_t* flags) = 0;
+  virtual void set_specular_walls(const std::uint8_t* codes) = 0;
+  virtual void set_specular_nodes(const std::uint8_t* masks) = 0;
   virtual void initialize(double rho, double ux, double uy, double uz) = 0;
   virtual void initialize_field(const double* rho, const double* ux, const double* uy,
                                 const double* uz) = 0;
@@ -70,6 +74,7 @@ struct Base {
   virtual void seed(const double* in) = 0;
   virtual double slot_sum() = 0;
   virtual long long n_padded() const = 0;
+  virtual long long n_interior() const = 0;
   virtual long long timestep() const = 0;
 };
 
@@ -106,6 +111,18 @@ struct Impl final : Base {
     const Domain dd = d;
     s.set_geometry([&](Index x, Index y, Index z) -> CellType {
       return CellType(flags[(std::size_t(z) * dd.ny + y) * dd.nx + x]);
+    });
+  }
+  void set_specular_walls(const std::uint8_t* codes) override {
+    const Domain dd = d;
+    s.set_specular_walls([&](Index x, Index y, Index z) -> std::uint8_t {
+      return codes[(std::size_t(z) * dd.ny + y) * dd.nx + x];
+    });
+  }
+  void set_specular_nodes(const std::uint8_t* masks) override {
+    const Domain dd = d;
+    s.set_specular_nodes([&](Index x, Index y, Index z) -> std::uint8_t {
+      return masks[(std::size_t(z) * dd.ny + y) * dd.nx + x];
     });
   }
   void initialize(double rho, double ux, double uy, double uz) override {
@@ -166,6 +183,7 @@ struct Impl final : Base {
     }
   }
   long long n_padded() const override { return d.n_padded; }
+  long long n_interior() const override { return (long long)d.nx * d.ny * d.nz; }
   long long timestep() const override { return (long long)s.timestep(); }
 };
 

@@ -77,6 +77,74 @@ def run(backend, case, seed, quant=None):
     return out
 
 
+# Free-slip walls (FluidSolver.hpp:193-268).  name -> (lattice, op, eq,
+# shifted, forcing, shape, kind, omega, omega2, steps, precision); `kind`
+# picks the geometry of spec_geometry() and, with it, the periodic axes.
+SPEC_CASES = {
+    "d2q9_bgk_guo_specwall_f64": (9, "bgk", 0, 1, 1, (10, 9, 1), "wall", 1.25, -1.0, 20, "f64"),
+    "d3q27_cm_specnode_f64": (27, "cm", 0, 1, 0, (8, 7, 6), "node", 1.6, -1.0, 9, "f64"),
+    "d3q27_trt_guo_specmixed_f32": (27, "trt", 0, 1, 1, (8, 7, 5), "mixed", 1.4, 1.1, 9, "f32"),
+    "d2q9_mrt_raw_specnode_f32": (9, "mrt", 0, 0, 0, (9, 8, 1), "node", 1.3, 1.5, 15, "f32"),
+}
+SPEC_PERIODIC = {"wall": (True, False, True), "node": (False, False, False),
+                 "mixed": (False, False, True)}
+
+
+def spec_geometry(lat, shape, kind):
+    """(flags, normal codes, face masks) over the interior, each (nz, ny, nx).
+
+    wall : solid row y = 0, SpecWall row y = ny-1 with normal +y (the
+           half-channel of the reference's validation/specular.cpp);
+    node : solid row y = 0, SpecNode on the x faces and (3-D) the z faces,
+           so the box edges carry two-face masks;
+    mixed: solid row y = 0, SpecWall columns on the x faces, SpecNode on the
+           top row between them."""
+    nx, ny, nz = shape
+    fl = np.zeros((nz, ny, nx), np.uint8)
+    codes = np.zeros_like(fl)
+    masks = np.zeros_like(fl)
+    fl[:, 0, :] = 1
+    if kind == "wall":
+        codes[:, -1, :] = 3
+    elif kind == "node":
+        masks[:, 1:, 0] |= 0x02
+        masks[:, 1:, -1] |= 0x01
+        if lat == 27:
+            masks[0, 1:, :] |= 0x20
+            masks[-1, 1:, :] |= 0x10
+    elif kind == "mixed":
+        codes[:, 1:, 0] = 2
+        codes[:, 1:, -1] = 1
+        masks[:, -1, 1:-1] = 0x04
+    else:
+        raise ValueError(kind)
+    return fl, codes, masks
+
+
+def run_spec(backend, case, seed, quant=None):
+    lat, op, eq, sh, fo, shape, kind, om, om2, steps, prec = case
+    nx, ny, nz = shape
+    per = SPEC_PERIODIC[kind]
+    F = (2e-5, -1e-5, 3e-6 if lat == 27 else 0.0) if fo else (0.0, 0.0, 0.0)
+    s = O.CpuSolver(backend, lattice=lat, op=op, eq=eq, shifted=sh, forcing=fo, nx=nx, ny=ny,
+                    nz=nz, px=per[0], py=per[1], pz=per[2], omega=om, omega2=om2, fx=F[0],
+                    fy=F[1], fz=F[2], precision=prec, quant=quant)
+    fl, codes, masks = spec_geometry(lat, shape, kind)
+    s.set_geometry(fl)
+    if codes.any():
+        s.set_specular_walls(codes)
+    if masks.any():
+        s.set_specular_nodes(masks)
+    s.initialize_field(*initial_field(shape, seed))
+    p0 = s.gather()
+    s.step(steps, store_macro=True)
+    out = {"pops0": p0, "pops": s.gather(), "stored": np.stack(s.stored_macro()),
+           "macro": np.stack(s.macro()), "mass": s.total_mass(),
+           "mom": np.array([s.total_momentum(a) for a in range(3)]), "slots": s.slot_sum()}
+    s.close()
+    return out
+
+
 def main():
     if not O.ref_available("f64"):
         raise SystemExit("reference build missing: make -C oracle ref")
@@ -85,6 +153,10 @@ def main():
     for k, (name, case) in enumerate(CASES.items()):
         r = run("ref", case, seed=100 + k)
         np.savez_compressed(HERE / f"{name}.npz", case=np.array(repr(case)), seed=100 + k, **r)
+        print(name, "mass", r["mass"])
+    for k, (name, case) in enumerate(SPEC_CASES.items()):
+        r = run_spec("ref", case, seed=200 + k)
+        np.savez_compressed(HERE / f"{name}.npz", case=np.array(repr(case)), seed=200 + k, **r)
         print(name, "mass", r["mass"])
 
 

@@ -55,6 +55,16 @@ class Case:
         self.gpu.set_geometry(flags)
         self.cpu.set_geometry(flags)
 
+    def specular(self, codes=None, masks=None):
+        """Free-slip walls on both sides: normal codes (SpecWall) and face
+        masks (SpecNode) per interior node, (nz, ny, nx)."""
+        if codes is not None and np.any(codes):
+            self.gpu.set_specular_walls(codes)
+            self.cpu.set_specular_walls(codes)
+        if masks is not None and np.any(masks):
+            self.gpu.set_specular_nodes(masks)
+            self.cpu.set_specular_nodes(masks)
+
     def init_random(self, seed=0, amp=0.03):
         rng = np.random.default_rng(seed)
         rho = 1 + 0.01 * rng.standard_normal(self.shape)

@@ -15,6 +15,7 @@ import shutil
 import subprocess
 from pathlib import Path
 
+import numpy as np
 import pytest
 
 ROOT = Path(__file__).resolve().parent.parent
@@ -104,3 +105,68 @@ def test_reference_example_runs_on_device(cuda_device, tmp_path):
     assert r.returncode == 0, r.stdout + r.stderr
     assert "DIVERGED" not in r.stdout
     assert out.exists() and len(out.read_text().splitlines()) == 49
+
+
+# ------------------------------------------------ free-slip wall validations
+# The reference's validation/specular.cpp, specular_node.cpp and
+# specwall_unsteady.cpp, built unmodified against the facade (`*_b200`, run on
+# the device) and against the host Kokkos stand-in (`*_cpu`, the reference's
+# own run): each must pass its own checks on the device and print the same
+# figures as the reference.
+REF_DIR = ROOT / "oracle" / "_ref"
+_NUM = r"[-+]?\d+\.\d+(?:e[-+]\d+)?"
+
+
+def _validation(name, *args):
+    exe = REF_DIR / name
+    if not exe.exists():
+        pytest.skip(f"{name} not built (make -C oracle facade-drivers ref-validation)")
+    env = dict(os.environ, OMP_NUM_THREADS=str(min(8, os.cpu_count() or 1)))
+    r = subprocess.run([str(exe), *args], capture_output=True, text=True, timeout=900, env=env)
+    return r.returncode, r.stdout
+
+
+def _figures(text, key):
+    return [[float(v) for v in re.findall(_NUM, ln)] for ln in text.splitlines() if key in ln]
+
+
+@pytest.mark.gpu
+def test_reference_specular_validation_on_device(cuda_device):
+    """Half channel closed by the ghost mirror = lower half of the full
+    channel to round-off, planes at 0.5 / H + 0.5, mass conserved
+    (validation/specular.cpp:103-160), for D2Q9 at tau 0.8 and 1.2 and D3Q27."""
+    rc, out = _validation("specular_b200")
+    assert rc == 0 and out.rstrip().endswith("PASS"), out
+    rc_ref, ref = _validation("specular_cpu")
+    assert rc_ref == 0
+    for key in ("no-slip plane", "symmetry plane", "u_max"):
+        for a, b in zip(_figures(out, key), _figures(ref, key), strict=True):
+            np.testing.assert_allclose(a, b, rtol=1e-9, atol=1e-15, err_msg=key)
+
+
+@pytest.mark.gpu
+def test_reference_specular_node_validation_on_device(cuda_device):
+    """On-node mirror: half box = periodic box to 1e-12 in 2-D, quarter box
+    with two-face edges in 3-D (validation/specular_node.cpp:284-368)."""
+    rc, out = _validation("specular_node_b200")
+    assert rc == 0 and out.rstrip().endswith("PASS"), out
+    assert out.count(" ok") == 6
+    rc_ref, ref = _validation("specular_node_cpu")
+    assert rc_ref == 0
+    # the control (halfway mirror on the same box) differs by the same amount
+    a, b = _figures(out, "CONTROL")[0], _figures(ref, "CONTROL")[0]
+    np.testing.assert_allclose(a, b, rtol=1e-9)
+
+
+@pytest.mark.gpu
+def test_reference_specwall_unsteady_on_device(cuda_device):
+    """The ghost mirror's first-order error for unsteady modes: the device
+    prints the reference's figures (validation/specwall_unsteady.cpp:79-91)."""
+    rc, out = _validation("specwall_unsteady_b200")
+    assert rc == 0, out
+    rc_ref, ref = _validation("specwall_unsteady_cpu")
+    assert rc_ref == 0
+    got, want = _figures(out, "SpecWall half box"), _figures(ref, "SpecWall half box")
+    assert len(got) == len(want) == 6
+    for a, b in zip(got, want):
+        np.testing.assert_allclose(a, b, rtol=5e-3)

@@ -189,3 +189,80 @@ def test_poiseuille_magic_parameter_is_exact(op, tau, lam):
     """README.md:240-276: at the magic parameter the halfway wall sits exactly
     midway; the discrete solution is the parabola to round-off (~1e-14)."""
     assert poiseuille(op, tau, lam=lam) < 1e-11
+
+
+# ------------------------------------------------------------ free-slip walls
+@pytest.mark.parametrize("name", list(G.SPEC_CASES))
+def test_oracle_reproduces_specular_golden(name):
+    """SpecWall / SpecNode fixtures made by the reference build."""
+    d = np.load(GOLDEN / f"{name}.npz")
+    r = G.run_spec("oracle", G.SPEC_CASES[name], seed=int(d["seed"]))
+    for k in ("pops0", "pops", "stored", "macro"):
+        np.testing.assert_array_equal(r[k], d[k], err_msg=k)
+    assert r["mass"] == float(d["mass"])
+    np.testing.assert_array_equal(r["mom"], d["mom"])
+    assert r["slots"] == float(d["slots"])
+
+
+@needs_ref
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+@pytest.mark.parametrize("kind", ["wall", "node", "mixed"])
+def test_oracle_specular_bit_identical_to_reference(prec, kind):
+    """Every operator, both storage conventions, with and without force, on
+    both lattices: ghost mirror, on-node mirror with edges, and the two mixed."""
+    O.set_ref_threads(1, prec)
+    ops = [("none", 0, -1.0), ("bgk", 0, -1.0), ("bgk", 1, -1.0), ("trt", 0, 1.1),
+           ("mrt", 0, 1.5), ("cm", 0, -1.0)]
+    for lat, (op, eq, om2), shifted, forcing in itertools.product(
+            [9, 27], ops, [1, 0], [0, 1]):
+        shape = (7, 6, 1) if lat == 9 else (6, 5, 5)
+        case = (lat, op, eq, shifted, forcing, shape, kind, 1.3, om2, 6, prec)
+        a = G.run_spec("oracle", case, seed=7)
+        b = G.run_spec("ref", case, seed=7)
+        for k in a:
+            np.testing.assert_array_equal(a[k], b[k], err_msg=f"{case} {k}")
+
+
+def test_oracle_specular_setters_reject_what_the_reference_rejects():
+    kw = dict(lattice=27, op="bgk", nx=4, ny=4, nz=4, px=False, py=False, pz=False,
+              precision="f64")
+    s = O.CpuSolver("oracle", **kw)
+    s.initialize(1.0, 0.02, 0.0, 0.0)
+    base = s.gather()
+    codes = np.zeros((4, 4, 4), np.uint8)
+    codes[1, 2, 3] = 7                       # corner code: not an axis normal
+    with pytest.raises(ValueError):
+        s.set_specular_walls(codes)
+    for bad in (0x40, 0x03, 0x0C, 0x30):     # stray bit, both faces of x / y / z
+        m = np.zeros((4, 4, 4), np.uint8)
+        m[0, 0, 0] = 0x01
+        m[2, 1, 0] = bad
+        with pytest.raises(ValueError):
+            s.set_specular_nodes(m)
+    # nothing was marked: the run equals a plain one
+    s.step(3)
+    t = O.CpuSolver("oracle", **kw)
+    t.initialize(1.0, 0.02, 0.0, 0.0)
+    t.step(3)
+    np.testing.assert_array_equal(s.gather(), t.gather())
+    assert not np.array_equal(base, t.gather())
+    s.close()
+    t.close()
+
+
+def test_oracle_specular_wall_conserves_mass():
+    """A ghost mirror permutes populations, so a box closed by SpecWall and
+    bounce-back conserves mass to round-off (validation/specular.cpp:33-38)."""
+    case = (27, "bgk", 0, 1, 1, (6, 8, 5), "wall", 1.2, -1.0, 0, "f64")
+    lat, op, eq, sh, fo, shape, kind, om, om2, _, prec = case
+    nx, ny, nz = shape
+    s = O.CpuSolver("oracle", lattice=27, op="bgk", shifted=1, forcing=1, nx=nx, ny=ny, nz=nz,
+                    px=True, py=False, pz=True, omega=1.2, fx=1e-5, precision="f64")
+    fl, codes, _ = G.spec_geometry(lat, shape, kind)
+    s.set_geometry(fl)
+    s.set_specular_walls(codes)
+    s.initialize(1.0)
+    m0 = s.total_mass()
+    s.step(200)
+    assert abs(s.total_mass() - m0) / m0 < 1e-13
+    s.close()
