@@ -98,9 +98,8 @@ int m3lb_set_params(m3lb_solver* h, double omega, double omega2, double fx, doub
 
 /* set_geometry(fn(x, y, z) -> CellType) (:74-82), the result of fn given as
  * an array over interior nodes: 0 Fluid, 1 Solid, 2 Excluded.  Resets every
- * interior flag, specular ones included; RegWall (3) is not offered and the
- * specular types (4, 5) are set by the two calls below (M3LB_ERR_UNSUPPORTED
- * for any value above 2). */
+ * interior flag, wall ones included; the wall types (3, 4, 5) are set by the
+ * calls below (M3LB_ERR_UNSUPPORTED for any value above 2). */
 int m3lb_set_flags(m3lb_solver* h, const uint8_t* flags);
 
 /* Normal codes of set_specular_walls (src/boundary/Regularized.hpp:97-102):
@@ -138,6 +137,47 @@ int m3lb_set_specular_walls(m3lb_solver* h, const uint8_t* normal_codes);
  * M3LB_ERR_INVALID and nothing changes.  While any specular node exists the
  * step runs in the one-node kernel.  Call after m3lb_set_flags. */
 int m3lb_set_specular_nodes(m3lb_solver* h, const uint8_t* face_masks);
+
+/* Normal codes of set_regularized_walls beyond the six axis walls
+ * (src/boundary/Regularized.hpp:97-105). */
+#define M3LB_NRM_CORNER 7   /* two or more walls meet: extrapolated density */
+#define M3LB_NRM_OUT_XP 8   /* pressure outlet on +x: imposed rho, closure u_n */
+#define M3LB_NRM_OUT_FREE 9 /* arbitrary-face outflow: donor rescaled to a density */
+#define M3LB_NRM_OUT_EQ 10  /* equilibrium outlet on +x */
+
+/* set_regularized_walls(fn(x, y, z) -> WallSpec) (FluidSolver.hpp:372-552):
+ * per interior node a normal code (0 leaves the node; 1..6 velocity walls
+ * with that outward normal; 7..10 above) and, in `states`, four doubles per
+ * node (ux, uy, uz, rho: the imposed velocity, and the density the outlet
+ * codes impose), or NULL for (0, 0, 0, 1).  The coded nodes become RegWall:
+ * on-node walls whose populations are rebuilt from (rho, u, Pi^(1)) each
+ * step before they collide (Latt et al. 2008, Regularized.hpp:1-40).
+ * Codes above 10, and an outlet (8, 10) without the upstream node(s) inside
+ * the domain (x < 1, or x < 2 at outflow order 2), are rejected with
+ * M3LB_ERR_INVALID and nothing changes.  Call after m3lb_set_flags. */
+int m3lb_set_regularized_walls(m3lb_solver* h, const uint8_t* normal_codes, const double* states);
+/* set_wall_velocity_scale (:294-303): every wall velocity as given times
+ * `scale` (absolute, not cumulative); densities untouched. */
+int m3lb_set_wall_velocity_scale(m3lb_solver* h, double scale);
+/* set_wall_density (:328-333): the density every wall state imposes. */
+int m3lb_set_wall_density(m3lb_solver* h, double rho);
+/* set_wall_velocity_field (:353-368): a wall velocity per interior node
+ * (three doubles, x fastest), replacing the states' velocities; then
+ * set_wall_velocity_field_scale scales it (absolute). */
+int m3lb_set_wall_velocity_field(m3lb_solver* h, const double* u3);
+int m3lb_set_wall_velocity_field_scale(m3lb_solver* h, double scale);
+/* set_fd_corners (:272): corner stress from finite-difference velocity
+ * gradients (default on) or from the corner's own populations. */
+int m3lb_set_fd_corners(m3lb_solver* h, int on);
+/* set_force_correction (:1311): the Guo corrections of the reconstruction
+ * (default on; they act under BGK, the one operator whose force the wall
+ * sees in the reference). */
+int m3lb_set_force_correction(m3lb_solver* h, int on);
+/* set_outflow_order (:1324): tangential extrapolation order at pressure
+ * outlets, 1 (default) or 2. */
+int m3lb_set_outflow_order(m3lb_solver* h, int order);
+/* set_outflow_density (:1330): target density of arbitrary-face outflows. */
+int m3lb_set_outflow_density(m3lb_solver* h, double rho);
 
 /* initialize(rho0, ux, uy, uz) (:553-561): equilibrium on fluid nodes, rest
  * equilibrium at rho0 elsewhere; resets the time step to 0. */

@@ -25,8 +25,9 @@ FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", 
 
 SLICES = [(lat, st) for lat in ("D2Q9", "D3Q27") for st in ("F32", "F16", "BF16", "F64")]
 HEADERS = ["lbm_common.cuh", "lbm_collide.cuh", "lbm_kernels.cuh", "lbm_stream.cuh", "lbm_rows.cuh",
+           "lbm_bound.cuh",
            "lbm_launch.h",
-           "lbm_host.h"]
+           "lbm_host.h", "lbm_walls.h"]
 
 
 def nvcc() -> str:
@@ -45,6 +46,7 @@ def _units():
     units.append((CSRC / "lbm_capi.cu", BUILD / "capi.o", []))
     units.append((CSRC / "lbm_noalloc.cu", BUILD / "noalloc.o", []))
     units.append((CSRC / "lbm_serve.cu", BUILD / "serve.o", []))
+    units.append((CSRC / "lbm_walls.cu", BUILD / "walls.o", []))
     return units
 
 
@@ -62,7 +64,7 @@ def up_to_date() -> bool:
         return False
     t = LIB.stat().st_mtime
     srcs = [CSRC / "lbm_inst.cu", CSRC / "lbm_capi.cu", CSRC / "lbm_noalloc.cu",
-            CSRC / "lbm_serve.cu", CSRC / "lbm_host.h",
+            CSRC / "lbm_serve.cu", CSRC / "lbm_walls.cu", CSRC / "lbm_host.h",
             *[CSRC / h for h in HEADERS],
             PKG.parent / "include" / "m3lb.h"]
     return all(p.stat().st_mtime <= t for p in srcs if p.exists())

@@ -78,6 +78,15 @@ SIGNATURES = {
     "m3lb_set_flags": (_i, [_vp, _vp]),
     "m3lb_set_specular_walls": (_i, [_vp, _vp]),
     "m3lb_set_specular_nodes": (_i, [_vp, _vp]),
+    "m3lb_set_regularized_walls": (_i, [_vp, _vp, _vp]),
+    "m3lb_set_wall_velocity_scale": (_i, [_vp, _d]),
+    "m3lb_set_wall_density": (_i, [_vp, _d]),
+    "m3lb_set_wall_velocity_field": (_i, [_vp, _vp]),
+    "m3lb_set_wall_velocity_field_scale": (_i, [_vp, _d]),
+    "m3lb_set_fd_corners": (_i, [_vp, _i]),
+    "m3lb_set_force_correction": (_i, [_vp, _i]),
+    "m3lb_set_outflow_order": (_i, [_vp, _i]),
+    "m3lb_set_outflow_density": (_i, [_vp, _d]),
     "m3lb_init_eq": (_i, [_vp] + [_d] * 4),
     "m3lb_init_field_f32": (_i, [_vp] + [_vp] * 4),
     "m3lb_init_field_f64": (_i, [_vp] + [_vp] * 4),

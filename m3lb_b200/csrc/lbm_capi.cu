@@ -11,6 +11,7 @@
 
 #include "../../include/m3lb.h"
 #include "lbm_host.h"
+#include "lbm_walls.h"
 
 using namespace m3lb;
 
@@ -120,12 +121,8 @@ struct m3lb_solver {
   uint8_t* flags = nullptr;          // per padded node
   std::vector<uint8_t> flags_host;   // per padded node
   bool has_geometry = false;
-  // specular walls (FluidSolver.hpp:193-268): per padded node the SpecWall
-  // normal code and the SpecNode face mask, and on the device one byte per
-  // node holding whichever the node's flag selects
-  std::vector<uint8_t> spec_nrm_host, spec_faces_host;
-  uint8_t* spec = nullptr;
-  bool has_spec = false;
+  // wall nodes (regularised and free-slip) and their device list
+  WallSet walls;
   void* macro[4] = {nullptr, nullptr, nullptr, nullptr};  // interior, arithmetic type
   void* staging = nullptr;           // init_field uploads (4 interior arrays)
   double* partials = nullptr;        // reduction scratch
@@ -145,7 +142,7 @@ struct m3lb_solver {
     a.g = g;
     a.f = f;
     a.flags = has_geometry ? flags : nullptr;
-    a.spec = has_spec ? spec : nullptr;
+    a.spec = walls.count ? walls.spec : nullptr;
     a.parity = (int)(t & 1);
     a.omega = omega; a.omega2 = omega2;
     a.fx = forcing ? fx : 0; a.fy = forcing ? fy : 0; a.fz = forcing ? fz : 0;
@@ -156,8 +153,7 @@ struct m3lb_solver {
   // one-node kernel runs everything.
   bool chunk_ok() const { return g.px && g.hx == 0 && (g.nx % 2) == 0; }
   int step_kernel() const {
-    // specular nodes run in the one-node kernel
-    if (node_kernel || has_spec || !chunk_ok() || kernel == M3LB_KERNEL_NODES) return kKernelNodes;
+    if (node_kernel || !chunk_ok() || kernel == M3LB_KERNEL_NODES) return kKernelNodes;
     // the streamed kernel addresses rows with 32-bit element counts
     const bool rows32 = (long long)g.nch * Q * 64 < (1LL << 31);
     // the row kernel: whole rows of at most 8 full chunks
@@ -265,7 +261,7 @@ int m3lb_destroy(m3lb_solver* h) {
   if (h->stream) cudaStreamSynchronize(h->stream);
   cudaFree(h->f);
   cudaFree(h->flags);
-  cudaFree(h->spec);
+  h->walls.release();
   for (void* p : h->macro) cudaFree(p);
   cudaFree(h->staging);
   cudaFree(h->partials);
@@ -282,39 +278,24 @@ int m3lb_set_params(m3lb_solver* h, double omega, double omega2, double fx, doub
 
 }  // extern "C"
 
-// Upload the host flags and, where specular nodes exist, their per-node
-// normal / mask byte; recompute which kernels the geometry allows.
+// Upload the host flags and rebuild the wall-node list.
 static int upload_geometry(m3lb_solver* h) {
   const Geo& g = h->g;
-  bool any = false, spec = false;
+  bool any = false;
   for (int z = 0; z < g.nz; ++z)
     for (int y = 0; y < g.ny; ++y)
-      for (int x = 0; x < g.nx; ++x) {
-        const uint8_t v = h->flags_host[((size_t)(z + g.hz) * g.sy + (y + g.hy)) * g.sx + (x + g.hx)];
-        any |= v != 0;
-        spec |= v == kSpecWall || v == kSpecNode;
-      }
+      for (int x = 0; x < g.nx; ++x)
+        any |= h->flags_host[((size_t)(z + g.hz) * g.sy + (y + g.hy)) * g.sx + (x + g.hx)] != 0;
   DeviceGuard dg(h->device);
   CUDA_TRY(cudaMemcpyAsync(h->flags, h->flags_host.data(), (size_t)g.n_padded,
                            cudaMemcpyHostToDevice, h->stream));
-  std::vector<uint8_t> sp;
-  if (spec) {
-    if (!h->spec && cudaMalloc((void**)&h->spec, (size_t)g.n_padded) != cudaSuccess) {
-      h->spec = nullptr;
-      return fail(M3LB_ERR_MEMORY, "specular: cannot allocate %lld bytes", g.n_padded);
-    }
-    sp.assign((size_t)g.n_padded, 0);
-    for (size_t n = 0; n < sp.size(); ++n) {
-      const uint8_t v = h->flags_host[n];
-      if (v == kSpecWall && !h->spec_nrm_host.empty()) sp[n] = h->spec_nrm_host[n];
-      if (v == kSpecNode && !h->spec_faces_host.empty()) sp[n] = h->spec_faces_host[n];
-    }
-    CUDA_TRY(cudaMemcpyAsync(h->spec, sp.data(), sp.size(), cudaMemcpyHostToDevice, h->stream));
-  }
   CUDA_TRY(cudaStreamSynchronize(h->stream));
   h->has_geometry = any;
-  h->has_spec = spec;
-  return M3LB_OK;
+  return h->walls.build(g, h->lattice, h->op, h->storage, h->flags_host, h->stream);
+}
+static int rebuild_walls(m3lb_solver* h) {
+  DeviceGuard dg(h->device);
+  return h->walls.build(h->g, h->lattice, h->op, h->storage, h->flags_host, h->stream);
 }
 
 extern "C" {
@@ -351,14 +332,14 @@ int m3lb_set_specular_walls(m3lb_solver* h, const uint8_t* codes) {
                       "set_specular_walls: normal code %u at (%d,%d,%d) is not an axis normal; "
                       "specular reflection is defined for codes 1..6 only", c, x, y, z);
       }
-  h->spec_nrm_host.assign((size_t)g.n_padded, 0);
+  h->walls.spec_nrm.assign((size_t)g.n_padded, 0);
   for (int z = 0; z < g.nz; ++z)
     for (int y = 0; y < g.ny; ++y)
       for (int x = 0; x < g.nx; ++x) {
         const uint8_t c = codes[((size_t)z * g.ny + y) * g.nx + x];
         if (!c) continue;
         const size_t n = ((size_t)(z + g.hz) * g.sy + (y + g.hy)) * g.sx + (x + g.hx);
-        h->spec_nrm_host[n] = c;
+        h->walls.spec_nrm[n] = c;
         h->flags_host[n] = kSpecWall;
       }
   return upload_geometry(h);
@@ -381,19 +362,108 @@ int m3lb_set_specular_nodes(m3lb_solver* h, const uint8_t* masks) {
                         "set_specular_nodes: mask %u at (%d,%d,%d) carries both faces of axis %d; "
                         "an on-node mirror needs one plane per axis", m, x, y, z, a);
       }
-  h->spec_faces_host.assign((size_t)g.n_padded, 0);
+  h->walls.spec_faces.assign((size_t)g.n_padded, 0);
   for (int z = 0; z < g.nz; ++z)
     for (int y = 0; y < g.ny; ++y)
       for (int x = 0; x < g.nx; ++x) {
         const uint8_t m = masks[((size_t)z * g.ny + y) * g.nx + x];
         if (!m) continue;
         const size_t n = ((size_t)(z + g.hz) * g.sy + (y + g.hy)) * g.sx + (x + g.hx);
-        h->spec_faces_host[n] = m;
+        h->walls.spec_faces[n] = m;
         h->flags_host[n] = kSpecNode;
       }
   return upload_geometry(h);
 }
 
+int m3lb_set_regularized_walls(m3lb_solver* h, const uint8_t* codes, const double* states) {
+  if (!h || !codes) return fail(M3LB_ERR_INVALID, "set_regularized_walls: null argument");
+  const int rc = h->walls.set_regularized(h->g, h->lattice, h->flags_host, codes, states);
+  if (rc) return rc;
+  return upload_geometry(h);
+}
+int m3lb_set_wall_velocity_scale(m3lb_solver* h, double scale) {
+  if (!h) return fail(M3LB_ERR_INVALID, "set_wall_velocity_scale: null handle");
+  h->walls.scale = scale;
+  return M3LB_OK;
+}
+int m3lb_set_wall_density(m3lb_solver* h, double rho) {
+  if (!h) return fail(M3LB_ERR_INVALID, "set_wall_density: null handle");
+  for (auto& kv : h->walls.reg) kv.second.u[3] = rho;
+  return rebuild_walls(h);
+}
+int m3lb_set_wall_velocity_field(m3lb_solver* h, const double* u3) {
+  if (!h || !u3) return fail(M3LB_ERR_INVALID, "set_wall_velocity_field: null argument");
+  h->walls.field.assign(u3, u3 + 3 * (size_t)h->n_interior());
+  h->walls.field_on = true;
+  h->walls.field_scale = 1;
+  return rebuild_walls(h);
+}
+int m3lb_set_wall_velocity_field_scale(m3lb_solver* h, double scale) {
+  if (!h) return fail(M3LB_ERR_INVALID, "set_wall_velocity_field_scale: null handle");
+  h->walls.field_scale = scale;
+  return M3LB_OK;
+}
+int m3lb_set_fd_corners(m3lb_solver* h, int on) {
+  if (!h) return fail(M3LB_ERR_INVALID, "set_fd_corners: null handle");
+  h->walls.fd_corners = on != 0;
+  return rebuild_walls(h);
+}
+int m3lb_set_force_correction(m3lb_solver* h, int on) {
+  if (!h) return fail(M3LB_ERR_INVALID, "set_force_correction: null handle");
+  h->walls.force_bc = on != 0;
+  return M3LB_OK;
+}
+int m3lb_set_outflow_order(m3lb_solver* h, int order) {
+  if (!h) return fail(M3LB_ERR_INVALID, "set_outflow_order: null handle");
+  for (const auto& kv : h->walls.reg) {
+    if (kv.second.code != kNrmOutXp || h->flags_host[kv.first] != kRegWall) continue;
+    const int x = (int)(kv.first % h->g.sx) - h->g.hx;
+    if (x < (order >= 2 ? 2 : 1))
+      return fail(M3LB_ERR_INVALID, "set_outflow_order: the pressure outlet node at x = %d has no "
+                  "second upstream node inside the domain", x);
+  }
+  h->walls.out_order = order;
+  return rebuild_walls(h);
+}
+int m3lb_set_outflow_density(m3lb_solver* h, double rho) {
+  if (!h) return fail(M3LB_ERR_INVALID, "set_outflow_density: null handle");
+  h->walls.out_rho = rho;
+  return M3LB_OK;
+}
+
+}  // extern "C"
+
+// The boundary pass around one bulk step (lbm_bound.cuh): snapshots of the
+// nodes read before their update and the corner densities ahead of the bulk
+// kernel; the wall nodes, level by level, after it.
+static int bound_before(m3lb_solver* h, const StepArgs& a, int* n) {
+  const WallSet& w = h->walls;
+  if (!w.count) return M3LB_OK;
+  const BoundArgs b = w.args(0, w.count);
+  const bool sh = h->shifted != 0, fo = h->forcing != 0;
+  if (w.nsnap) {
+    CUDA_TRY(h->L->bound(a, b, kBndSnapshot, h->op, h->eq, sh, fo, h->stream));
+    *n += 1;
+  }
+  if (w.corners) {
+    CUDA_TRY(h->L->bound(a, b, kBndCornerRho, h->op, h->eq, sh, fo, h->stream));
+    *n += 2;
+  }
+  return M3LB_OK;
+}
+static int bound_after(m3lb_solver* h, const StepArgs& a, int* n) {
+  const WallSet& w = h->walls;
+  int begin = 0;
+  for (int end : w.level_end) {
+    CUDA_TRY(h->L->bound(a, w.args(begin, end), kBndUpdate, h->op, h->eq, h->shifted != 0,
+                         h->forcing != 0, h->stream));
+    *n += 1;
+    begin = end;
+  }
+  return M3LB_OK;
+}
+
+extern "C" {
 static int seed(m3lb_solver* h, SeedArgs& a) {
   a.g = h->g;
   a.f = h->f;
@@ -482,7 +552,11 @@ int m3lb_step(m3lb_solver* h, int nsteps, int store_macro) {
       a.rho = h->macro[0]; a.ux = h->macro[1]; a.uy = h->macro[2]; a.uz = h->macro[3];
     }
     int n = 0;
+    int rc = bound_before(h, a, &n);
+    if (rc) return rc;
     CUDA_TRY(h->L->step(a, h->op, h->eq, h->shifted != 0, h->forcing != 0, kernel, h->stream, &n));
+    rc = bound_after(h, a, &n);
+    if (rc) return rc;
     h->launches += n;
     ++h->t;
   }
@@ -497,6 +571,11 @@ int m3lb_macro_device(m3lb_solver* h, void** rho, void** ux, void** uy, void** u
   a.rho = h->macro[0]; a.ux = h->macro[1]; a.uy = h->macro[2]; a.uz = h->macro[3];
   CUDA_TRY(h->L->macro(a, h->op, h->shifted != 0, h->forcing != 0, h->stream));
   h->launches += 1;
+  if (h->walls.count) {  // the state RegWall nodes report
+    CUDA_TRY(h->L->bound(a, h->walls.args(0, h->walls.count), kBndMacro, h->op, h->eq,
+                         h->shifted != 0, h->forcing != 0, h->stream));
+    h->launches += 1;
+  }
   if (rho) *rho = h->macro[0];
   if (ux) *ux = h->macro[1];
   if (uy) *uy = h->macro[2];

@@ -186,8 +186,9 @@ __host__ __device__ __forceinline__ int shift_coord(int v, int h, int n, int s, 
 }
 
 // Cell types (src/boundary/Flags.hpp:20-32): 0 Fluid, 1 Solid, 2 Excluded,
-// 4 SpecWall (free-slip ghost), 5 SpecNode (on-node free slip).
-constexpr uint8_t kSpecWall = 4, kSpecNode = 5;
+// 3 RegWall (regularised on-node wall), 4 SpecWall (free-slip ghost),
+// 5 SpecNode (on-node free slip).
+constexpr uint8_t kRegWall = 3, kSpecWall = 4, kSpecNode = 5;
 
 // Parameters of one step launch, passed by value.
 struct StepArgs {
@@ -195,7 +196,7 @@ struct StepArgs {
   void* f;                 // populations
   const uint8_t* flags;    // per padded node (0 fluid); nullptr: all interior fluid
   const uint8_t* spec;     // per padded node: SpecWall normal code / SpecNode face mask;
-                           // nullptr: no specular nodes (flags 4 and 5 then act as solid)
+                           // nullptr: no wall nodes (flags 3, 4 and 5 then act as solid)
   void* rho;               // macroscopic outputs, per padded node, or nullptr
   void* ux;
   void* uy;
@@ -204,6 +205,45 @@ struct StepArgs {
   double omega, omega2;    // BGK/TRT/MRT/CM rates (TRT: omega_p, omega_m; moments: omega, bulk)
   double fx, fy, fz;       // uniform Guo body force
   int* err;                // device status word: a kernel whose bounded wait ran out sets it
+};
+
+// ------------------------------------------------------------- wall nodes
+// Regularised-wall normal codes beyond the six axis walls
+// (src/boundary/Regularized.hpp:97-105) and the compact list of wall nodes
+// the boundary pass updates (lbm_bound.cuh).
+enum : uint8_t { kNrmCorner = 7, kNrmOutXp = 8, kNrmOutFree = 9, kNrmOutEq = 10 };
+constexpr int kBndRefs = 6;
+constexpr int kBndThreads = 128;
+
+// One wall node of the list.
+struct BNode {
+  long long n;                 // padded index
+  long long ref[kBndRefs];     // nodes this one reads (padded index), -1 unused:
+                               //   outflow donor / upstream 1, 2; corner stencil 2a, 2a+1
+  int ref_wall[kBndRefs];      // list position when the read is a wall node's state velocity
+  int snap[kBndRefs];          // snapshot slot when the read precedes the node's update, else -1
+  int c1, c2;                  // corner: list positions of the extrapolation nodes, -1 none
+  uint32_t unk;                // RegWall: directions whose source is outside the fluid
+  uint8_t type;                // kRegWall / kSpecWall / kSpecNode
+  uint8_t code;                // RegWall normal code, SpecWall normal code, SpecNode face mask
+  uint8_t onrm;                // NrmOutFree: outward normal of the donor axis
+  int8_t fd_dir[3];            // corner stencil per axis: +1 / -1 one-sided, 0 centred, 2 unused
+  double u[4];                 // wall state as given: ux, uy, uz, rho
+  double un[3];                // per-node wall velocity field
+};
+
+struct BoundArgs {
+  const BNode* nodes;
+  int begin, end;              // list positions of this launch
+  void* wall_rho;              // arithmetic type, one per list node (corner densities)
+  void* snap;                  // arithmetic type, Q per snapshot slot
+  double scale;                // set_wall_velocity_scale
+  double field_scale;          // set_wall_velocity_field_scale
+  int field_on;                // per-node wall velocity field in use
+  int fd_corners;              // corner stress from velocity gradients
+  int force_bc;                // Guo corrections of the reconstruction
+  int out_order;               // tangential extrapolation order at NrmOutXp
+  double out_rho;              // NrmOutFree target density
 };
 
 // Scatter (Access::scatter, EsotericPull.hpp:104-111): write, for node n and

@@ -6,6 +6,7 @@
 
 #include "lbm_stream.cuh"
 #include "lbm_rows.cuh"
+#include "lbm_bound.cuh"
 #include "lbm_launch.h"
 
 #ifndef M3LB_LAT
@@ -241,7 +242,51 @@ cudaError_t reduce(const StepArgs& a, int op, bool sh, bool force, double* parti
   return cudaErrorInvalidValue;
 }
 
-const Launchers kTable = {step, seed, gather, macro, reduce};
+template <int OP, int EQ, bool SH, bool FORCE>
+cudaError_t bound_t(const StepArgs& a, const BoundArgs& b, int phase, cudaStream_t s) {
+  using R = typename StoreT<ST>::real;
+  constexpr bool USH = SH && OP != 0;
+  const long long n = b.end - b.begin;
+  if (n <= 0) return cudaSuccess;
+  const unsigned grid = blocks_for(n, kBndThreads);
+  switch (phase) {
+    case kBndSnapshot: bnd_snapshot<L, ST><<<grid, kBndThreads, 0, s>>>(a, b); break;
+    case kBndCornerRho: {
+      bnd_wall_rho<L, ST, USH><<<grid, kBndThreads, 0, s>>>(a, b);
+      cudaError_t e = cudaGetLastError();
+      if (e != cudaSuccess) return e;
+      bnd_corner_rho<R><<<grid, kBndThreads, 0, s>>>(b);
+      break;
+    }
+    case kBndUpdate: bnd_step<L, ST, OP, EQ, SH, FORCE><<<grid, kBndThreads, 0, s>>>(a, b); break;
+    case kBndMacro: bnd_macro<L, ST, USH><<<grid, kBndThreads, 0, s>>>(a, b); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+template <int OP, int EQ, bool SH>
+cudaError_t bound_f(const StepArgs& a, const BoundArgs& b, int phase, bool force, cudaStream_t s) {
+  return force ? bound_t<OP, EQ, SH, true>(a, b, phase, s) : bound_t<OP, EQ, SH, false>(a, b, phase, s);
+}
+template <int OP, int EQ>
+cudaError_t bound_s(const StepArgs& a, const BoundArgs& b, int phase, bool sh, bool force,
+                    cudaStream_t s) {
+  if (sh) return bound_f<OP, EQ, true>(a, b, phase, force, s);
+  if constexpr (kRawOK) return bound_f<OP, EQ, false>(a, b, phase, force, s);
+  return cudaErrorInvalidValue;
+}
+cudaError_t bound(const StepArgs& a, const BoundArgs& b, int phase, int op, int eq, bool sh,
+                  bool force, cudaStream_t s) {
+  switch (op) {
+    case 0: return bound_t<0, 0, true, false>(a, b, phase, s);
+    case 1: return eq ? bound_s<1, 1>(a, b, phase, sh, force, s) : bound_s<1, 0>(a, b, phase, sh, force, s);
+    case 2: return eq ? bound_s<2, 1>(a, b, phase, sh, force, s) : bound_s<2, 0>(a, b, phase, sh, force, s);
+    case 3: return bound_s<3, 0>(a, b, phase, sh, force, s);
+    case 4: return bound_s<4, 0>(a, b, phase, sh, force, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+const Launchers kTable = {step, seed, gather, macro, reduce, bound};
 
 }  // namespace
 

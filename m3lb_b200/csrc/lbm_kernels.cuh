@@ -241,6 +241,9 @@ __device__ __forceinline__ void pairs_unit(const StepArgs& a, long long warp, in
     m = collide<L, OP, EQ, SH, FORCE>(f, prm);
 #pragma unroll
     for (int q = 0; q < Q; ++q) w[q] = WO::pack(f[q]);
+  } else {  // pure streaming reports rest: rho 1, u 0 (the no-collision mock)
+    m.dens = m.rho = bc<V>(1);
+    m.ux = m.uy = m.uz = bc<V>(0);
   }
 
   // ---- solid / excluded nodes write back what they read (the identity)
@@ -272,7 +275,7 @@ __device__ __forceinline__ void pairs_unit(const StepArgs& a, long long warp, in
     c.template store_pair<i>(w[i], w[i + 1]);
   });
 
-  if constexpr (OP != 0) {
+  {
     if (a.rho && c.active) {
       using R = S;
       const size_t kk = ((size_t)zi * g.ny + yi) * g.nx + x0;
@@ -440,11 +443,9 @@ step_nodes(StepArgs a) {
   if (k >= nint) return;
   const int xi = (int)(k % g.nx), yi = (int)((k / g.nx) % g.ny), zi = (int)(k / ((long long)g.nx * g.ny));
   const int x = xi + g.hx, y = yi + g.hy, z = zi + g.hz;
-  const long long pn = ((long long)z * g.sy + y) * g.sx + x;
-  const unsigned fl = a.flags ? a.flags[pn] : 0u;
   // Solid and Excluded skip (bounce-back is the identity on this storage);
-  // specular nodes run when their normals / masks are present
-  if (fl != 0 && !(a.spec && (fl == kSpecWall || fl == kSpecNode))) return;
+  // wall nodes are left to the boundary pass
+  if (a.flags && a.flags[((long long)z * g.sy + y) * g.sx + x] != 0) return;
   NodeNb<L> nb;
   node_neighbours<L>(g, x, y, z, nb);
   E* A = reinterpret_cast<E*>(a.f);
@@ -457,14 +458,8 @@ step_nodes(StepArgs a) {
     f[i] = to_real(A[slot<Q>(g, x, y, z, i + P)]);
     f[i + 1] = to_real(A[slot<Q>(g, m[0], m[1], m[2], i + 1 - P)]);
   }
-  Macro<R> mc;
-  if (fl == kSpecWall) {
-    spec_wall_permute<L>(f, spec_axis(a.spec[pn]));
-  } else {
-    if (fl == kSpecNode) spec_node_mirror<L>(f, a.spec[pn]);
-    const CollideParams<R> prm{(R)a.omega, (R)a.omega2, (R)a.fx, (R)a.fy, (R)a.fz};
-    mc = collide<L, OP, EQ, SH, FORCE>(f, prm);
-  }
+  const CollideParams<R> prm{(R)a.omega, (R)a.omega2, (R)a.fx, (R)a.fy, (R)a.fz};
+  const Macro<R> mc = collide<L, OP, EQ, SH, FORCE>(f, prm);
   A[slot<Q>(g, x, y, z, 0)] = from_real<E>(f[0]);
 #pragma unroll
   for (int i = 1; i < Q; i += 2) {
@@ -472,7 +467,7 @@ step_nodes(StepArgs a) {
     A[slot<Q>(g, m[0], m[1], m[2], i + 1 - P)] = from_real<E>(f[i]);
     A[slot<Q>(g, x, y, z, i + P)] = from_real<E>(f[i + 1]);
   }
-  if (a.rho && fl != kSpecWall) {
+  if (a.rho) {
     reinterpret_cast<R*>(a.rho)[k] = mc.rho;
     reinterpret_cast<R*>(a.ux)[k] = mc.ux;
     reinterpret_cast<R*>(a.uy)[k] = mc.uy;
@@ -602,7 +597,8 @@ __global__ void seed_kernel(SeedArgs a) {
   const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= g.n_padded) return;
   const int x = (int)(n % g.sx), y = (int)((n / g.sx) % g.sy), z = (int)(n / ((long long)g.sx * g.sy));
-  const bool fluid = a.flags[n] == 0 || a.flags[n] == kSpecNode;  // SpecNode seeds as fluid
+  // RegWall and SpecNode are fluid nodes and seed as such (FluidSolver.hpp:553-579)
+  const bool fluid = a.flags[n] == 0 || a.flags[n] == kRegWall || a.flags[n] == kSpecNode;
   R rho = (R)a.rho0, ux = 0, uy = 0, uz = 0;
   if (a.mode == 0) {
     if (fluid) { ux = (R)a.ux0; uy = (R)a.uy0; uz = (R)a.uz0; }
@@ -740,7 +736,8 @@ reduce_kernel(StepArgs a, double* partials) {
     const long long pn = ((long long)z * g.sy + y) * g.sx + x;
     const unsigned fl = a.flags ? a.flags[pn] : 0u;
     const bool spec_node = fl == kSpecNode && a.spec;
-    if (fl != 0 && !spec_node) continue;
+    // fluid-like: Fluid, RegWall and SpecNode (FluidSolver.hpp:1215)
+    if (fl != 0 && !spec_node && !(fl == kRegWall && a.spec)) continue;
     NodeNb<L> nb;
     node_neighbours<L>(g, x, y, z, nb);
     R f[Q];

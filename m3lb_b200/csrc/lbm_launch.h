@@ -25,7 +25,12 @@ struct Launchers {
   cudaError_t (*macro)(const StepArgs& a, int op, bool sh, bool force, cudaStream_t s);
   cudaError_t (*reduce)(const StepArgs& a, int op, bool sh, bool force, double* partials,
                         int nblocks, double* out, cudaStream_t s);
+  // boundary pass over the wall-node list b.begin..b.end (lbm_bound.cuh)
+  cudaError_t (*bound)(const StepArgs& a, const BoundArgs& b, int phase, int op, int eq, bool sh,
+                       bool force, cudaStream_t s);
 };
+// phases of the boundary pass
+enum BoundPhase { kBndSnapshot = 0, kBndCornerRho = 1, kBndUpdate = 2, kBndMacro = 3 };
 
 #define M3LB_DECLARE_LAUNCHERS(NAME) const Launchers* NAME();
 M3LB_DECLARE_LAUNCHERS(launchers_D2Q9_F32)

@@ -383,6 +383,9 @@ step_rows(StepArgs a, const __grid_constant__ RowMaps<L> maps) {
       m = collide<L, OP, EQ, SH, FORCE>(f, prm);
 #pragma unroll
       for (int q = 0; q < Q; ++q) w[q] = WO::pack(f[q]);
+    } else {  // pure streaming reports rest: rho 1, u 0 (the no-collision mock)
+      m.dens = m.rho = bc<V>(1);
+      m.ux = m.uy = m.uz = bc<V>(0);
     }
 
     // ---- write back in place: f_{i+1}' to the own slot, f_i' to the
@@ -423,7 +426,7 @@ step_rows(StepArgs a, const __grid_constant__ RowMaps<L> maps) {
       }
     });
 
-    if constexpr (OP != 0) {
+    {
       if (a.rho) {
         using R = S;
         const size_t kk = ((size_t)cur.zi * g.ny + cur.yi) * g.nx + x0;

@@ -384,6 +384,9 @@ step_stream(StepArgs a) {
       m = collide<L, OP, EQ, SH, FORCE>(f, prm);
 #pragma unroll
       for (int q = 0; q < Q; ++q) w[q] = WO::pack(f[q]);
+    } else {  // pure streaming reports rest: rho 1, u 0 (the no-collision mock)
+      m.dens = m.rho = bc<V>(1);
+      m.ux = m.uy = m.uz = bc<V>(0);
     }
     ChunkPtrs<L, ST> cp;
     cp.set(g, Al, P, cur);
@@ -450,7 +453,7 @@ step_stream(StepArgs a) {
       }
     });
 
-    if constexpr (OP != 0) {
+    {
       if (a.rho && lx.active) {
         using R = S;
         const size_t kk = ((size_t)cur.zi * g.ny + cur.yi) * g.nx + lx.x0;

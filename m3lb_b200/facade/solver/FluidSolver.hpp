@@ -12,7 +12,7 @@
 //     _BF16 selects 16-bit storage for every solver;
 //   * the policies must be ones the device runs: D2Q9 / D3Q27; BGK, TRT,
 //     MomentCollision; NoForcing or Guo; Fluid, Solid and Excluded cells
-//     and the free-slip SpecWall / SpecNode cells.
+//     and the wall cells RegWall, SpecWall and SpecNode.
 //     Anything else fails to compile (static_assert) or is rejected at
 //     set_geometry.
 #pragma once
@@ -73,6 +73,14 @@ class FluidSolver {
  public:
   using Lattice = L;
   static constexpr int Q = L::Q;
+
+  // One regularised wall node (:97-103): outward normal code, imposed
+  // velocity, and the density the outlet codes impose.
+  struct WallSpec {
+    std::uint8_t normal = NrmNone;
+    Real ux = 0, uy = 0, uz = 0;
+    Real rho = Real(1);
+  };
 
   static_assert(DeviceLattice<L>::code != 0, "the B200 path runs D2Q9 and D3Q27");
   static_assert(facade::IsDeviceStreaming<Streaming>::value,
@@ -135,6 +143,75 @@ class FluidSolver {
     mark(a, SpecWall);
   }
 
+  // set_regularized_walls (:372-552): fn(x, y, z) -> WallSpec; NrmNone leaves
+  // the node, any other code marks it a regularised on-node wall.
+  template <class Fn>
+  void set_regularized_walls(Fn fn) {
+    const std::size_t ni = std::size_t(dom_.n_interior());
+    std::vector<std::uint8_t> codes(ni, 0);
+    std::vector<double> st(4 * ni, 0.0);
+    for (Index z = 0; z < dom_.nz; ++z)
+      for (Index y = 0; y < dom_.ny; ++y)
+        for (Index x = 0; x < dom_.nx; ++x) {
+          const std::size_t k = (std::size_t(z) * dom_.ny + y) * dom_.nx + x;
+          const WallSpec w = fn(x, y, z);
+          codes[k] = w.normal;
+          st[4 * k] = w.ux; st[4 * k + 1] = w.uy; st[4 * k + 2] = w.uz; st[4 * k + 3] = w.rho;
+        }
+    m3lb_facade::check(m3lb_set_regularized_walls(h_, codes.data(), st.data()),
+                       "set_regularized_walls");
+    mark(codes, RegWall);
+    // distinct wall states, as the reference's deduplicated table counts them
+    std::vector<std::array<Real, 4>> table;
+    for (std::size_t k = 0; k < ni; ++k) {
+      if (!codes[k]) continue;
+      const std::array<Real, 4> v{Real(st[4 * k]), Real(st[4 * k + 1]), Real(st[4 * k + 2]),
+                                  Real(st[4 * k + 3])};
+      bool seen = false;
+      for (const auto& t : table) seen = seen || t == v;
+      if (!seen) table.push_back(v);
+    }
+    n_wall_states_ = table.empty() ? 1 : table.size();
+  }
+  std::size_t n_wall_states() const { return n_wall_states_; }
+  void set_wall_velocity_scale(Real sc) {
+    m3lb_facade::check(m3lb_set_wall_velocity_scale(h_, sc), "set_wall_velocity_scale");
+  }
+  void set_wall_density(Real r) { m3lb_facade::check(m3lb_set_wall_density(h_, r), "set_wall_density"); }
+  // fn(x, y, z) -> std::array<Real, 3>, lattice units, interior coordinates
+  template <class Fn>
+  void set_wall_velocity_field(Fn fn) {
+    std::vector<double> u(3 * std::size_t(dom_.n_interior()));
+    for (Index z = 0; z < dom_.nz; ++z)
+      for (Index y = 0; y < dom_.ny; ++y)
+        for (Index x = 0; x < dom_.nx; ++x) {
+          const std::size_t k = (std::size_t(z) * dom_.ny + y) * dom_.nx + x;
+          const auto v = fn(x, y, z);
+          u[3 * k] = v[0]; u[3 * k + 1] = v[1]; u[3 * k + 2] = v[2];
+        }
+    m3lb_facade::check(m3lb_set_wall_velocity_field(h_, u.data()), "set_wall_velocity_field");
+  }
+  void set_wall_velocity_field_scale(Real s) {
+    m3lb_facade::check(m3lb_set_wall_velocity_field_scale(h_, s), "set_wall_velocity_field_scale");
+  }
+  void set_fd_corners(bool on) { m3lb_facade::check(m3lb_set_fd_corners(h_, on), "set_fd_corners"); }
+  void set_force_correction(bool on) {
+    m3lb_facade::check(m3lb_set_force_correction(h_, on), "set_force_correction");
+  }
+  void set_outflow_order(int k) {
+    m3lb_facade::check(m3lb_set_outflow_order(h_, k), "set_outflow_order");
+  }
+  void set_outflow_density(Real r) {
+    out_rho_ = r;
+    m3lb_facade::check(m3lb_set_outflow_density(h_, r), "set_outflow_density");
+  }
+  Real outflow_density() const { return out_rho_; }
+  Index wall_count() const {
+    Index n = 0;
+    for (Index k = 0; k < dom_.n_padded; ++k) n += flags_(k) == RegWall;
+    return n;
+  }
+
   // set_specular_nodes (:236-268): fn(x, y, z) -> SpecFace mask; SpecNone
   // leaves the node, any valid mask marks it an on-node free-slip node.
   template <class Fn>
@@ -164,7 +241,7 @@ class FluidSolver {
       for (Index y = 0; y < dom_.ny; ++y)
         for (Index x = 0; x < dom_.nx; ++x) {
           const Index n = dom_.id(x, y, z);
-          if (flags_(n) != Fluid && flags_(n) != SpecNode) continue;
+          if (flags_(n) != Fluid && flags_(n) != RegWall && flags_(n) != SpecNode) continue;
           const FlowState s = fn(n);
           const std::size_t k = (std::size_t(z) * dom_.ny + y) * dom_.nx + x;
           r[k] = s.rho; u[k] = s.ux; v[k] = s.uy; w[k] = s.uz;
@@ -293,6 +370,8 @@ class FluidSolver {
   Collision coll_;
   Streaming pop_{};
   m3lb_solver* h_ = nullptr;
+  Real out_rho_ = Real(1);
+  std::size_t n_wall_states_ = 0;
   View1D<std::uint8_t> flags_;
   View1D<Real> rho_, ux_, uy_, uz_;
   mutable bool fields_stale_ = false;

@@ -107,6 +107,25 @@ class NormalCode(enum.IntEnum):
     NrmZm = 6
 
 
+class WallCode(enum.IntEnum):
+    """Regularised-wall codes beyond the axis normals (Regularized.hpp:97-105)."""
+    NrmCorner = 7
+    NrmOutXp = 8
+    NrmOutFree = 9
+    NrmOutEq = 10
+
+
+@dataclass
+class WallSpec:
+    """One regularised wall node (FluidSolver.hpp:97-103): outward normal code,
+    imposed velocity, and the density the outlet codes impose."""
+    normal: int = 0
+    ux: float = 0.0
+    uy: float = 0.0
+    uz: float = 0.0
+    rho: float = 1.0
+
+
 class SpecFace(enum.IntFlag):
     """Face bits of an on-node specular mask (Specular.hpp:226-234)."""
     SpecNone = 0
@@ -378,6 +397,64 @@ class FluidSolver:
         masks = self._per_node(fn_or_masks)
         capi.check(capi.lib().m3lb_set_specular_nodes(self._h, _ptr(masks)))
         self._flags = np.where(masks != 0, np.uint8(CellType.SpecNode), self._flags).astype(np.uint8)
+
+    def set_regularized_walls(self, fn_or_codes, states=None):
+        """Regularised on-node walls (FluidSolver.hpp:372-552): fn(x, y, z) ->
+        WallSpec over interior coordinates, or the normal codes as an
+        (nz, ny, nx) array with `states` (nz, ny, nx, 4) = (ux, uy, uz, rho)
+        or None for (0, 0, 0, 1).  Call after set_geometry."""
+        d = self.dom
+        if callable(fn_or_codes):
+            codes = np.zeros((d.nz, d.ny, d.nx), np.uint8)
+            st = np.zeros((d.nz, d.ny, d.nx, 4))
+            st[..., 3] = 1.0
+            for z in range(d.nz):
+                for y in range(d.ny):
+                    for x in range(d.nx):
+                        w = fn_or_codes(x, y, z)
+                        if int(w.normal) == 0:
+                            continue
+                        codes[z, y, x] = int(w.normal)
+                        st[z, y, x] = (w.ux, w.uy, w.uz, w.rho)
+        else:
+            codes = self._per_node(fn_or_codes)
+            st = None if states is None else np.broadcast_to(states, (d.nz, d.ny, d.nx, 4))
+        st_arr = None if st is None else np.ascontiguousarray(st, dtype=np.float64)
+        capi.check(capi.lib().m3lb_set_regularized_walls(
+            self._h, _ptr(codes), _ptr(st_arr) if st_arr is not None else None))
+        self._flags = np.where(codes != 0, np.uint8(CellType.RegWall), self._flags).astype(np.uint8)
+
+    def set_wall_velocity_scale(self, sc):
+        capi.check(capi.lib().m3lb_set_wall_velocity_scale(self._h, float(sc)))
+
+    def set_wall_density(self, r):
+        capi.check(capi.lib().m3lb_set_wall_density(self._h, float(r)))
+
+    def set_wall_velocity_field(self, fn_or_array):
+        """fn(x, y, z) -> (ux, uy, uz), or an (nz, ny, nx, 3) array."""
+        d = self.dom
+        if callable(fn_or_array):
+            u = np.array([[[fn_or_array(x, y, z) for x in range(d.nx)] for y in range(d.ny)]
+                          for z in range(d.nz)], dtype=np.float64)
+        else:
+            u = np.asarray(fn_or_array, dtype=np.float64)
+        u = np.ascontiguousarray(np.broadcast_to(u, (d.nz, d.ny, d.nx, 3)))
+        capi.check(capi.lib().m3lb_set_wall_velocity_field(self._h, _ptr(u)))
+
+    def set_wall_velocity_field_scale(self, sc):
+        capi.check(capi.lib().m3lb_set_wall_velocity_field_scale(self._h, float(sc)))
+
+    def set_fd_corners(self, on):
+        capi.check(capi.lib().m3lb_set_fd_corners(self._h, int(bool(on))))
+
+    def set_force_correction(self, on):
+        capi.check(capi.lib().m3lb_set_force_correction(self._h, int(bool(on))))
+
+    def set_outflow_order(self, k):
+        capi.check(capi.lib().m3lb_set_outflow_order(self._h, int(k)))
+
+    def set_outflow_density(self, r):
+        capi.check(capi.lib().m3lb_set_outflow_density(self._h, float(r)))
 
     def initialize(self, rho0=1.0, ux0=0.0, uy0=0.0, uz0=0.0):
         self._push_params()

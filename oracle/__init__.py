@@ -40,6 +40,15 @@ def _bind(lib, prefix):
         "set_geometry": (None, [_vp, _u8p]),
         "set_specular_walls": (C.c_int, [_vp, _u8p]),
         "set_specular_nodes": (C.c_int, [_vp, _u8p]),
+        "set_regularized_walls": (C.c_int, [_vp, _u8p, _dp]),
+        "set_wall_velocity_scale": (None, [_vp, C.c_double]),
+        "set_wall_density": (None, [_vp, C.c_double]),
+        "set_wall_velocity_field": (None, [_vp, _dp]),
+        "set_wall_velocity_field_scale": (None, [_vp, C.c_double]),
+        "set_fd_corners": (None, [_vp, C.c_int]),
+        "set_force_correction": (None, [_vp, C.c_int]),
+        "set_outflow_order": (C.c_int, [_vp, C.c_int]),
+        "set_outflow_density": (None, [_vp, C.c_double]),
         "initialize": (None, [_vp] + [C.c_double] * 4),
         "initialize_field": (None, [_vp] + [_dp] * 4),
         "step": (None, [_vp, C.c_int, C.c_int]),
@@ -165,6 +174,45 @@ class CpuSolver:
         a = np.ascontiguousarray(masks, dtype=np.uint8).reshape(self.shape)
         if self._f["set_specular_nodes"](self._h, a.ctypes.data_as(_u8p)) != 0:
             raise ValueError("set_specular_nodes: mask outside 0x3F or with both faces of an axis")
+
+    def set_regularized_walls(self, codes, spec=None):
+        """Normal code per interior node (0 none, 1..6 axis walls, 7 corner,
+        8 pressure outlet, 9 free outflow, 10 equilibrium outlet) and the
+        state (ux, uy, uz, rho) per node, shaped (nz, ny, nx, 4), or None for
+        (0, 0, 0, 1); FluidSolver.hpp:372-552."""
+        a = np.ascontiguousarray(codes, dtype=np.uint8).reshape(self.shape)
+        sp = None
+        if spec is not None:
+            sp = np.ascontiguousarray(np.broadcast_to(spec, self.shape + (4,)), dtype=np.float64)
+        if self._f["set_regularized_walls"](self._h, a.ctypes.data_as(_u8p),
+                                             _ptr(sp) if sp is not None else None) != 0:
+            raise ValueError("set_regularized_walls: rejected normal code or outlet position")
+
+    def set_wall_velocity_scale(self, sc):
+        self._f["set_wall_velocity_scale"](self._h, float(sc))
+
+    def set_wall_density(self, r):
+        self._f["set_wall_density"](self._h, float(r))
+
+    def set_wall_velocity_field(self, u3):
+        a = np.ascontiguousarray(np.broadcast_to(u3, self.shape + (3,)), dtype=np.float64)
+        self._f["set_wall_velocity_field"](self._h, _ptr(a))
+
+    def set_wall_velocity_field_scale(self, sc):
+        self._f["set_wall_velocity_field_scale"](self._h, float(sc))
+
+    def set_fd_corners(self, on):
+        self._f["set_fd_corners"](self._h, int(bool(on)))
+
+    def set_force_correction(self, on):
+        self._f["set_force_correction"](self._h, int(bool(on)))
+
+    def set_outflow_order(self, k):
+        if self._f["set_outflow_order"](self._h, int(k)) != 0:
+            raise ValueError("set_outflow_order: a pressure outlet lacks the upstream nodes")
+
+    def set_outflow_density(self, r):
+        self._f["set_outflow_density"](self._h, float(r))
 
     def initialize(self, rho0=1.0, ux=0.0, uy=0.0, uz=0.0):
         self._f["initialize"](self._h, rho0, ux, uy, uz)

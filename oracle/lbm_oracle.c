@@ -56,6 +56,9 @@ __attribute__((constructor)) static void lbmo_init(void) {
   build_mirror_tables();
 }
 
+/* Normal codes beyond the six axis walls (src/boundary/Regularized.hpp:97-105). */
+enum { NRM_CORNER = 7, NRM_OUTXP = 8, NRM_OUTFREE = 9, NRM_OUTEQ = 10 };
+
 /* float -> bfloat16 -> float, round to nearest even (NaN kept quiet). */
 static inline float lbmo_bf16_round(float v) {
   uint32_t u;

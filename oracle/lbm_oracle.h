@@ -29,6 +29,12 @@
  * Both return 0, or -1 without changing anything when a value is one the
  * reference rejects (FluidSolver.hpp:193-268: a code above 6, a mask above
  * 0x3F or with both faces of one axis).
+ *
+ * set_regularized_walls takes a normal code per interior node (0 none, 1..6
+ * axis velocity walls, 7 corner, 8 pressure outlet +x, 9 arbitrary-face
+ * outflow, 10 equilibrium outlet +x) and, per node, (ux, uy, uz, rho) or
+ * NULL; it marks the coded nodes RegWall (3).  The other wall setters follow
+ * FluidSolver.hpp:272-370, 1311-1330.
  */
 #ifndef LBM_ORACLE_H
 #define LBM_ORACLE_H
@@ -42,6 +48,15 @@
   void P##set_geometry(void* h, const uint8_t* flags);                               \
   int P##set_specular_walls(void* h, const uint8_t* normal_codes);                   \
   int P##set_specular_nodes(void* h, const uint8_t* face_masks);                     \
+  int P##set_regularized_walls(void* h, const uint8_t* codes, const double* spec);   \
+  void P##set_wall_velocity_scale(void* h, double sc);                               \
+  void P##set_wall_density(void* h, double r);                                       \
+  void P##set_wall_velocity_field(void* h, const double* u3);                        \
+  void P##set_wall_velocity_field_scale(void* h, double sc);                         \
+  void P##set_fd_corners(void* h, int on);                                           \
+  void P##set_force_correction(void* h, int on);                                     \
+  int P##set_outflow_order(void* h, int k);                                          \
+  void P##set_outflow_density(void* h, double r);                                    \
   void P##initialize(void* h, double rho, double ux, double uy, double uz);          \
   void P##initialize_field(void* h, const double* rho, const double* ux,             \
                            const double* uy, const double* uz);                      \

@@ -21,6 +21,14 @@ typedef struct {
   uint8_t* flags;
   uint8_t* spec_nrm;   /* SpecWall normal code per padded node */
   uint8_t* spec_faces; /* SpecNode face mask per padded node */
+  /* regularised walls (FluidSolver.hpp:97-103, 272-552, 1266-1290), per
+   * padded node; the state table is kept per node (u0 = as given) */
+  uint8_t *bc_nrm, *bc_ext, *bc_onrm;
+  uint32_t* bc_unk;
+  long long* bc_don;
+  R *bc_rho, *wall_u0, *wall_un;  /* u0: 4 per node (ux, uy, uz, rho) */
+  R wall_scale, wall_un_scale, outflow_rho;
+  int wall_un_on, has_corners, fd_corners, force_bc, out_order, has_walls;
   R *rho, *ux, *uy, *uz; /* stored macroscopic fields (StoreMacro) */
 } S(solver);
 
@@ -111,6 +119,13 @@ static inline void S(scatter1)(S(solver)* s, int par, long long n, const long lo
   else          { if (i & 1) A(n, i + 1) = v; else A(nb[i - 1], i - 1) = v; }
 }
 #undef A
+static inline void S(load_node)(const S(solver)* s, int par, long long n, R* g, int unshift) {
+  long long nb[27];
+  S(neighbours)(s, n, nb);
+  S(load_all)(s, par, n, nb, g);
+  if (unshift)
+    for (int i = 0; i < s->Q; ++i) g[i] += S(w)(s, i);
+}
 
 /* ---- Specular walls: src/boundary/Specular.hpp ---- */
 static inline int S(mir)(const S(solver)* s, int a, int i) {
@@ -141,9 +156,9 @@ static void S(mirror_faces)(const S(solver)* s, R* f, uint8_t faces) {
 }
 
 /* ---- Equilibria: src/equilibrium/Equilibrium.hpp:28-124 ---- */
-static inline R S(phi)(const S(solver)* s, int i, R ux, R uy, R uz) {
+static inline R S(phi_e)(const S(solver)* s, int eqc, int i, R ux, R uy, R uz) {
   const R cx = (R)S(c)(s, i, 0), cy = (R)S(c)(s, i, 1), cz = (R)S(c)(s, i, 2);
-  if (s->eq == 0) {                                          /* SecondOrderPhi :49-60 */
+  if (eqc == 0) {                                          /* SecondOrderPhi :49-60 */
     const R ics2 = (R)3 / (R)1;
     const R cu = cx * ux + cy * uy + cz * uz;
     const R uu = ux * ux + uy * uy + uz * uz;
@@ -169,6 +184,9 @@ static inline R S(phi)(const S(solver)* s, int i, R ux, R uy, R uz) {
     chi[a] = (c3[a] == 0) ? (R)1 - (R)1.5 * u3[a] * u3[a]
                           : (R)1 + (R)3 * u3[a] * ((R)c3[a] + u3[a]);
   return chi[0] * chi[1] * chi[2] - (R)1;
+}
+static inline R S(phi)(const S(solver)* s, int i, R ux, R uy, R uz) {
+  return S(phi_e)(s, s->eq, i, ux, uy, uz);
 }
 static inline R S(eq)(const S(solver)* s, int i, R rho, R ux, R uy, R uz) {
   return S(w)(s, i) * rho * ((R)1 + S(phi)(s, i, ux, uy, uz)); /* :34-37 */
@@ -415,6 +433,119 @@ static R S(seed_value)(const S(solver)* s, int i, R rho, R ux, R uy, R uz) {
   return f[i];
 }
 
+/* ---- Regularised walls: src/boundary/Regularized.hpp ---- */
+static void S(normal_of)(uint8_t code, int n[3]) {          /* :153-166 */
+  n[0] = n[1] = n[2] = 0;
+  if (code >= 1 && code <= 6) n[(code - 1) / 2] = (code & 1) ? 1 : -1;
+  else if (code == NRM_OUTXP) n[0] = 1;
+}
+/* The equilibrium the wall rebuilds against (EquilibriumOf, :47-57): the
+ * operator's own for BGK/TRT, the product form for the moment operators,
+ * second order for the no-collision mock. */
+static inline int S(bc_eq)(const S(solver)* s) { return s->op >= 3 ? 1 : (s->op == 0 ? 0 : s->eq); }
+static inline R S(bc_feq)(const S(solver)* s, int i, R rho, R ux, R uy, R uz) {
+  return S(w)(s, i) * rho * ((R)1 + S(phi_e)(s, S(bc_eq)(s), i, ux, uy, uz));
+}
+static inline int S(unshift)(const S(solver)* s) { return s->shifted && s->op != 0; }
+static R S(bc_density)(const S(solver)* s, const R* f, const int nrm[3], const R* u) { /* :178-190 */
+  R out = 0, tang = 0;
+  for (int i = 0; i < s->Q; ++i) {
+    const int cn = S(c)(s, i, 0) * nrm[0] + S(c)(s, i, 1) * nrm[1] + S(c)(s, i, 2) * nrm[2];
+    if (cn > 0) out += f[i];
+    else if (cn == 0) tang += f[i];
+  }
+  const R uperp = u[0] * (R)nrm[0] + u[1] * (R)nrm[1] + u[2] * (R)nrm[2];
+  return ((R)2 * out + tang) / ((R)1 + uperp);
+}
+static R S(bc_normal_velocity)(const S(solver)* s, const R* f, const int nrm[3], R rho) { /* :196-206 */
+  R out = 0, tang = 0;
+  for (int i = 0; i < s->Q; ++i) {
+    const int cn = S(c)(s, i, 0) * nrm[0] + S(c)(s, i, 1) * nrm[1] + S(c)(s, i, 2) * nrm[2];
+    if (cn > 0) out += f[i];
+    else if (cn == 0) tang += f[i];
+  }
+  return ((R)2 * out + tang) / rho - (R)1;
+}
+/* Q_i : Pi with the off-diagonal terms twice (:226-231, 314-318). */
+static inline R S(q_pi)(const S(solver)* s, int i, const R* Pi) {
+  const R cs2v = (R)1 / (R)3;
+  const R cx = (R)S(c)(s, i, 0), cy = (R)S(c)(s, i, 1), cz = (R)S(c)(s, i, 2);
+  const int d3 = s->D == 3;
+  return (cx * cx - cs2v) * Pi[0] + (cy * cy - cs2v) * Pi[1] +
+         (d3 ? (cz * cz - cs2v) * Pi[2] : (R)0) +
+         (R)2 * (cx * cy * Pi[3] + (d3 ? (cx * cz * Pi[4] + cy * cz * Pi[5]) : (R)0));
+}
+static void S(bc_apply_with_stress)(const S(solver)* s, R* f, R rho, const R* u, const R* Pi) { /* :219-236 */
+  const R cs2v = (R)1 / (R)3, cs4v = cs2v * cs2v;
+  for (int i = 0; i < s->Q; ++i)
+    f[i] = S(bc_feq)(s, i, rho, u[0], u[1], u[2]) + S(w)(s, i) / ((R)2 * cs4v) * S(q_pi)(s, i, Pi);
+}
+static void S(bc_stress_from_gradient)(R rho, R omega, R g[3][3], R* Pi) { /* :240-250 */
+  const R cs2v = (R)1 / (R)3;
+  const R k = -(R)2 * cs2v * rho / omega;
+  Pi[0] = k * g[0][0];
+  Pi[1] = k * g[1][1];
+  Pi[2] = k * g[2][2];
+  Pi[3] = k * (R)0.5 * (g[0][1] + g[1][0]);
+  Pi[4] = k * (R)0.5 * (g[0][2] + g[2][0]);
+  Pi[5] = k * (R)0.5 * (g[1][2] + g[2][1]);
+}
+static inline int S(opp)(int i) { return i == 0 ? 0 : ((i & 1) ? i + 1 : i - 1); }
+/* Eqs. (44)-(45) with the forced corrections (:262-328). */
+static void S(bc_apply)(const S(solver)* s, R* f, R rho, const R* u, uint32_t unknown, const R* Fv) {
+  const R cs2v = (R)1 / (R)3, cs4v = cs2v * cs2v;
+  R feq[27];
+  for (int i = 0; i < s->Q; ++i) feq[i] = S(bc_feq)(s, i, rho, u[0], u[1], u[2]);
+  const R hodd = (R)0.5 / cs2v;
+  for (int i = 0; i < s->Q; ++i) {
+    if (!(unknown & (1u << i))) continue;
+    const R cF = Fv ? ((R)S(c)(s, i, 0) * Fv[0] + (R)S(c)(s, i, 1) * Fv[1] +
+                       (R)S(c)(s, i, 2) * Fv[2]) : (R)0;
+    const R odd = S(w)(s, i) * hodd * cF;
+    const int o = S(opp)(i);
+    f[i] = (unknown & (1u << o)) ? feq[i] - odd : feq[i] + (f[o] - feq[o]) - (R)2 * odd;
+  }
+  R Pi[6] = {0, 0, 0, 0, 0, 0};
+  for (int i = 0; i < s->Q; ++i) {
+    const R d = f[i] - feq[i];
+    const R cx = (R)S(c)(s, i, 0), cy = (R)S(c)(s, i, 1), cz = (R)S(c)(s, i, 2);
+    Pi[0] += d * cx * cx; Pi[1] += d * cy * cy; Pi[2] += d * cz * cz;
+    Pi[3] += d * cx * cy; Pi[4] += d * cx * cz; Pi[5] += d * cy * cz;
+  }
+  for (int i = 0; i < s->Q; ++i) {
+    const R cx = (R)S(c)(s, i, 0), cy = (R)S(c)(s, i, 1), cz = (R)S(c)(s, i, 2);
+    const R cF = Fv ? (cx * Fv[0] + cy * Fv[1] + cz * Fv[2]) : (R)0;
+    f[i] = feq[i] - S(w)(s, i) * hodd * cF + S(w)(s, i) / ((R)2 * cs4v) * S(q_pi)(s, i, Pi);
+  }
+}
+/* Interior coordinates -> padded index, unwrapped (Domain::id). */
+static inline long long S(idi)(const S(solver)* s, long long x, long long y, long long z) {
+  return ((z + s->hz) * s->sy + (y + s->hy)) * s->sx + (x + s->hx);
+}
+/* Wall velocity of a node: the per-node field when set, else its state. */
+static inline void S(wall_vel)(const S(solver)* s, long long n, R* uw) {
+  for (int a = 0; a < 3; ++a)
+    uw[a] = s->wall_un_on ? s->wall_un_scale * s->wall_un[n * 3 + a]
+                          : s->wall_u0[n * 4 + a] * s->wall_scale;
+}
+static inline void S(load_node)(const S(solver)* s, int par, long long n, R* g, int unshift);
+/* Velocity at the k-th upstream node of an outflow face (:896-912). */
+static void S(up_vel)(const S(solver)* s, int par, long long n, int k, R* v) {
+  int px, py, pz;
+  S(coords)(s, n, &px, &py, &pz);
+  const long long m = S(idi)(s, px - s->hx - k, py - s->hy, pz - s->hz);
+  R g[27];
+  S(load_node)(s, par, m, g, S(unshift)(s));
+  R sm = 0;
+  v[0] = v[1] = v[2] = 0;
+  for (int i = 0; i < s->Q; ++i) {
+    sm += g[i];
+    for (int a = 0; a < 3; ++a) v[a] += g[i] * (R)S(c)(s, i, a);
+  }
+  const R ir = (R)1 / sm;
+  for (int a = 0; a < 3; ++a) v[a] *= ir;
+}
+
 /* ---- FluidSolver: src/solver/FluidSolver.hpp ---- */
 void* F(create)(int lattice, int op, int eq, int shifted, int forcing, int quant, int nx, int ny,
                 int nz, int px, int py, int pz, double omega, double omega2, double fx, double fy,
@@ -435,6 +566,17 @@ void* F(create)(int lattice, int op, int eq, int shifted, int forcing, int quant
   s->flags = (uint8_t*)calloc((size_t)s->n_padded, 1);
   s->spec_nrm = (uint8_t*)calloc((size_t)s->n_padded, 1);
   s->spec_faces = (uint8_t*)calloc((size_t)s->n_padded, 1);
+  s->bc_nrm = (uint8_t*)calloc((size_t)s->n_padded, 1);
+  s->bc_ext = (uint8_t*)calloc((size_t)s->n_padded, 1);
+  s->bc_onrm = (uint8_t*)calloc((size_t)s->n_padded, 1);
+  s->bc_unk = (uint32_t*)calloc((size_t)s->n_padded, sizeof(uint32_t));
+  s->bc_don = (long long*)calloc((size_t)s->n_padded, sizeof(long long));
+  s->bc_rho = (R*)calloc((size_t)s->n_padded, sizeof(R));
+  s->wall_u0 = (R*)calloc((size_t)s->n_padded * 4, sizeof(R));
+  s->wall_un = (R*)calloc((size_t)s->n_padded * 3, sizeof(R));
+  s->wall_scale = (R)1; s->wall_un_scale = (R)1; s->outflow_rho = (R)1;
+  s->fd_corners = op != 0;   /* has_shear_omega: every operator but the no-collision mock */
+  s->force_bc = 1; s->out_order = 1;
   s->rho = (R*)calloc((size_t)s->n_padded, sizeof(R));
   s->ux = (R*)calloc((size_t)s->n_padded, sizeof(R));
   s->uy = (R*)calloc((size_t)s->n_padded, sizeof(R));
@@ -449,7 +591,9 @@ void* F(create)(int lattice, int op, int eq, int shifted, int forcing, int quant
 void F(destroy)(void* h) {
   S(solver)* s = (S(solver)*)h;
   if (!s) return;
-  free(s->f); free(s->flags); free(s->spec_nrm); free(s->spec_faces); free(s->rho); free(s->ux); free(s->uy); free(s->uz);
+  free(s->f); free(s->flags); free(s->spec_nrm); free(s->spec_faces);
+  free(s->bc_nrm); free(s->bc_ext); free(s->bc_onrm); free(s->bc_unk); free(s->bc_don);
+  free(s->bc_rho); free(s->wall_u0); free(s->wall_un); free(s->rho); free(s->ux); free(s->uy); free(s->uz);
   free(s);
 }
 void F(set_geometry)(void* h, const uint8_t* fl) {           /* :74-82 */
@@ -500,6 +644,301 @@ int F(set_specular_nodes)(void* h, const uint8_t* masks) {
       }
   return 0;
 }
+/* set_regularized_walls (:372-552): normal code per interior node (0 none)
+ * and, per node, the state (ux, uy, uz, rho) or NULL for (0, 0, 0, 1).
+ * Returns -1 without changes for a code above NrmOutEq, or an NrmOutXp /
+ * NrmOutEq node whose upstream stencil leaves the interior (x < 1, or x < 2
+ * at outflow order 2). */
+int F(set_regularized_walls)(void* h, const uint8_t* codes, const double* spec) {
+  S(solver)* s = (S(solver)*)h;
+  for (int z = 0; z < s->nz; ++z)
+    for (int y = 0; y < s->ny; ++y)
+      for (int x = 0; x < s->nx; ++x) {
+        const uint8_t c = codes[((size_t)z * s->ny + y) * s->nx + x];
+        if (c > NRM_OUTEQ) return -1;
+        if ((c == NRM_OUTXP || c == NRM_OUTEQ) && x < (c == NRM_OUTXP ? s->out_order : 1))
+          return -1;
+      }
+  memset(s->bc_nrm, 0, (size_t)s->n_padded);
+  for (int z = 0; z < s->nz; ++z)
+    for (int y = 0; y < s->ny; ++y)
+      for (int x = 0; x < s->nx; ++x) {
+        const size_t k = ((size_t)z * s->ny + y) * s->nx + x;
+        if (!codes[k]) continue;
+        const long long n = S(idi)(s, x, y, z);
+        s->bc_nrm[n] = codes[k];
+        for (int a = 0; a < 4; ++a) s->wall_u0[n * 4 + a] = spec ? (R)spec[k * 4 + a] : (R)(a == 3);
+        s->flags[n] = 3;
+      }
+  /* corners: an axis direction whose next two nodes are straight walls */
+  static const int d6[6][3] = {{1,0,0},{-1,0,0},{0,1,0},{0,-1,0},{0,0,1},{0,0,-1}};
+  memset(s->bc_ext, 0, (size_t)s->n_padded);
+  s->has_corners = 0;
+  for (int z = 0; z < s->nz; ++z)
+    for (int y = 0; y < s->ny; ++y)
+      for (int x = 0; x < s->nx; ++x) {
+        const long long n = S(idi)(s, x, y, z);
+        if (s->bc_nrm[n] != NRM_CORNER) continue;
+        s->has_corners = 1;
+        for (int k = 0; k < (s->nz > 1 ? 6 : 4); ++k) {
+          const int x1 = x + d6[k][0], y1 = y + d6[k][1], z1 = z + d6[k][2];
+          const int x2 = x + 2 * d6[k][0], y2 = y + 2 * d6[k][1], z2 = z + 2 * d6[k][2];
+          if (x1 < 0 || y1 < 0 || z1 < 0 || x2 < 0 || y2 < 0 || z2 < 0) continue;
+          if (x1 >= s->nx || y1 >= s->ny || z1 >= s->nz) continue;
+          if (x2 >= s->nx || y2 >= s->ny || z2 >= s->nz) continue;
+          const uint8_t a = s->bc_nrm[S(idi)(s, x1, y1, z1)], b = s->bc_nrm[S(idi)(s, x2, y2, z2)];
+          if (a != 0 && a != NRM_CORNER && b != 0 && b != NRM_CORNER) {
+            s->bc_ext[n] = (uint8_t)(k + 1);
+            break;
+          }
+        }
+      }
+  /* unknown directions: the source node is outside the domain, Excluded or Solid */
+  memset(s->bc_unk, 0, (size_t)s->n_padded * sizeof(uint32_t));
+  const int nn[3] = {s->nx, s->ny, s->nz};
+  for (int z = 0; z < s->nz; ++z)
+    for (int y = 0; y < s->ny; ++y)
+      for (int x = 0; x < s->nx; ++x) {
+        const long long n = S(idi)(s, x, y, z);
+        if (!s->bc_nrm[n]) continue;
+        uint32_t m = 0;
+        for (int i = 0; i < s->Q; ++i) {
+          int src[3] = {x - S(c)(s, i, 0), y - S(c)(s, i, 1), z - S(c)(s, i, 2)};
+          int outside = 0;
+          for (int a = 0; a < 3; ++a) {
+            if (s->per[a]) src[a] = (src[a] + nn[a]) % nn[a];
+            else if (src[a] < 0 || src[a] >= nn[a]) outside = 1;
+          }
+          if (!outside) {
+            const uint8_t sf = s->flags[S(idi)(s, src[0], src[1], src[2])];
+            if (sf == 2 || sf == 1) outside = 1;
+          }
+          if (outside) m |= 1u << i;
+        }
+        s->bc_unk[n] = m;
+      }
+  /* outflow donors: the fluid neighbour opposite the axis step that leaves */
+  static const int dd[6][3] = {{-1,0,0},{1,0,0},{0,-1,0},{0,1,0},{0,0,-1},{0,0,1}};
+  static const uint8_t dcode[6] = {2, 1, 4, 3, 6, 5};
+  for (long long n = 0; n < s->n_padded; ++n) { s->bc_don[n] = n; s->bc_onrm[n] = 0; }
+  for (int z = 0; z < s->nz; ++z)
+    for (int y = 0; y < s->ny; ++y)
+      for (int x = 0; x < s->nx; ++x) {
+        const long long n = S(idi)(s, x, y, z);
+        if (s->bc_nrm[n] != NRM_OUTFREE) continue;
+        for (int k = 0; k < 6; ++k) {
+          const int qx = x + dd[k][0], qy = y + dd[k][1], qz = z + dd[k][2];
+          const int leaves = (qx < 0 || qx >= s->nx || qy < 0 || qy >= s->ny || qz < 0 ||
+                              qz >= s->nz) || s->flags[S(idi)(s, qx, qy, qz)] == 1;
+          if (!leaves) continue;
+          const int o = k ^ 1;
+          const int rx = x + dd[o][0], ry = y + dd[o][1], rz = z + dd[o][2];
+          if (rx < 0 || rx >= s->nx || ry < 0 || ry >= s->ny || rz < 0 || rz >= s->nz) continue;
+          const long long m = S(idi)(s, rx, ry, rz);
+          if (s->flags[m] != 0) continue;
+          s->bc_don[n] = m;
+          s->bc_onrm[n] = dcode[k];
+          break;
+        }
+      }
+  s->wall_scale = (R)1;
+  s->has_walls = 1;
+  return 0;
+}
+void F(set_wall_velocity_scale)(void* h, double sc) { ((S(solver)*)h)->wall_scale = (R)sc; } /* :294-303 */
+void F(set_wall_density)(void* h, double r) {                                  /* :328-333 */
+  S(solver)* s = (S(solver)*)h;
+  for (long long n = 0; n < s->n_padded; ++n) s->wall_u0[n * 4 + 3] = (R)r;
+}
+void F(set_wall_velocity_field)(void* h, const double* u3) {                     /* :353-368 */
+  S(solver)* s = (S(solver)*)h;
+  memset(s->wall_un, 0, (size_t)s->n_padded * 3 * sizeof(R));
+  for (int z = 0; z < s->nz; ++z)
+    for (int y = 0; y < s->ny; ++y)
+      for (int x = 0; x < s->nx; ++x) {
+        const size_t k = ((size_t)z * s->ny + y) * s->nx + x;
+        const long long n = S(idi)(s, x, y, z);
+        for (int a = 0; a < 3; ++a) s->wall_un[n * 3 + a] = (R)u3[k * 3 + a];
+      }
+  s->wall_un_on = 1;
+  s->wall_un_scale = (R)1;
+}
+void F(set_wall_velocity_field_scale)(void* h, double sc) { ((S(solver)*)h)->wall_un_scale = (R)sc; }
+void F(set_fd_corners)(void* h, int on) { ((S(solver)*)h)->fd_corners = on != 0; }
+void F(set_force_correction)(void* h, int on) { ((S(solver)*)h)->force_bc = on != 0; }
+int F(set_outflow_order)(void* h, int k) {                                       /* :1324 */
+  S(solver)* s = (S(solver)*)h;
+  for (int z = 0; z < s->nz; ++z)
+    for (int y = 0; y < s->ny; ++y)
+      for (int x = 0; x < (k >= 2 ? 2 : 1) && x < s->nx; ++x)
+        if (s->flags[S(idi)(s, x, y, z)] == 3 && s->bc_nrm[S(idi)(s, x, y, z)] == NRM_OUTXP) return -1;
+  s->out_order = k;
+  return 0;
+}
+void F(set_outflow_density)(void* h, double r) { ((S(solver)*)h)->outflow_rho = (R)r; }
+
+/* corner_density<P> (:664-712): closure density of every straight wall node,
+ * then the corners extrapolated from two of them, at the parity the sweep
+ * is about to read. */
+static void S(corner_density)(S(solver)* s, int par) {
+  static const int d6[6][3] = {{1,0,0},{-1,0,0},{0,1,0},{0,-1,0},{0,0,1},{0,0,-1}};
+  for (long long n = 0; n < s->n_padded; ++n) {
+    if (s->flags[n] != 3) continue;
+    const uint8_t code = s->bc_nrm[n];
+    if (code == NRM_CORNER || code == 0) continue;
+    R f[27], uw[3];
+    int nrm[3];
+    S(load_node)(s, par, n, f, S(unshift)(s));
+    S(normal_of)(code, nrm);
+    S(wall_vel)(s, n, uw);
+    s->bc_rho[n] = (code == NRM_OUTXP || code == NRM_OUTEQ) ? s->wall_u0[n * 4 + 3]
+                 : (code == NRM_OUTFREE) ? s->outflow_rho : S(bc_density)(s, f, nrm, uw);
+  }
+  for (long long n = 0; n < s->n_padded; ++n) {
+    if (s->flags[n] != 3 || s->bc_nrm[n] != NRM_CORNER) continue;
+    const int k = s->bc_ext[n];
+    if (k == 0) { s->bc_rho[n] = (R)1; continue; }
+    int px, py, pz;
+    S(coords)(s, n, &px, &py, &pz);
+    const int x = px - s->hx, y = py - s->hy, z = pz - s->hz;
+    const int* e = d6[k - 1];
+    const long long n1 = S(idi)(s, x + e[0], y + e[1], z + e[2]);
+    const long long n2 = S(idi)(s, x + 2 * e[0], y + 2 * e[1], z + 2 * e[2]);
+    s->bc_rho[n] = (R)2 * s->bc_rho[n1] - s->bc_rho[n2];
+  }
+}
+
+/* Velocity of a node for the corner stencil (:965-986): a wall node's
+ * imposed state velocity, else the moments of its populations. */
+static void S(vel_at)(const S(solver)* s, int par, long long m, R* out) {
+  if (s->flags[m] == 3) {
+    for (int a = 0; a < 3; ++a) out[a] = s->wall_u0[m * 4 + a] * s->wall_scale;
+    return;
+  }
+  long long nb[27];
+  R g2[27];
+  S(neighbours)(s, m, nb);
+  S(load_all)(s, par, m, nb, g2);
+  R sm = 0, mx = 0, my = 0, mz = 0;
+  for (int i = 0; i < s->Q; ++i) {
+    R v = g2[i];
+    if (S(unshift)(s)) v += S(w)(s, i);
+    sm += v;
+    mx += v * (R)S(c)(s, i, 0);
+    my += v * (R)S(c)(s, i, 1);
+    mz += v * (R)S(c)(s, i, 2);
+  }
+  const R ir = (R)1 / sm;
+  out[0] = mx * ir; out[1] = my * ir; out[2] = mz * ir;
+}
+
+/* The RegWall branch of run_step (:792-1021).  Returns 1 when the node is
+ * finished (outflow codes that overwrite the node), 0 when it goes on to
+ * collide like a fluid node. */
+static int S(regwall)(S(solver)* s, int par, long long n, const long long* nb, R* f) {
+  const int Q = s->Q;
+  const int unsh = S(unshift)(s);
+  if (unsh)
+    for (int i = 0; i < Q; ++i) f[i] += S(w)(s, i);
+  const uint8_t code = s->bc_nrm[n];
+  int nrm[3];
+  S(normal_of)(code, nrm);
+  R uw[3];
+  S(wall_vel)(s, n, uw);
+  /* has_forcing<Collision> (Regularized.hpp:81-86) looks for a ForcingPolicy
+   * member type, which of these operators only BGK declares (BGK.hpp:37):
+   * the wall sees the force under BGK alone. */
+  R Fv[3] = {0, 0, 0};
+  if (s->forcing && s->op == 1) { Fv[0] = s->fx; Fv[1] = s->fy; Fv[2] = s->fz; }
+  R ur[3] = {uw[0], uw[1], uw[2]};
+  R rw;
+  if (code == NRM_OUTFREE) {
+    R g[27];
+    S(load_node)(s, par, s->bc_don[n], g, unsh);
+    R sm = 0;
+    for (int i = 0; i < Q; ++i) sm += g[i];
+    if (sm > (R)0) {
+      const R sc = s->outflow_rho / sm;
+      for (int i = 0; i < Q; ++i) f[i] = g[i] * sc;
+    }
+    if (unsh)
+      for (int i = 0; i < Q; ++i) f[i] -= S(w)(s, i);
+    S(store_all)(s, par, n, nb, f);
+    return 1;
+  } else if (code == NRM_OUTEQ) {
+    const R rw2 = s->wall_u0[n * 4 + 3];
+    int px, py, pz;
+    S(coords)(s, n, &px, &py, &pz);
+    R g[27];
+    S(load_node)(s, par, S(idi)(s, px - s->hx - 1, py - s->hy, pz - s->hz), g, unsh);
+    R sm = 0, mu[3] = {0, 0, 0};
+    for (int i = 0; i < Q; ++i) {
+      sm += g[i];
+      for (int a = 0; a < 3; ++a) mu[a] += g[i] * (R)S(c)(s, i, a);
+    }
+    const R ir = (sm > (R)0) ? (R)1 / sm : (R)0;
+    for (int a = 0; a < 3; ++a) mu[a] *= ir;
+    for (int i = 0; i < Q; ++i) f[i] = S(bc_feq)(s, i, rw2, mu[0], mu[1], mu[2]);
+    if (unsh)
+      for (int i = 0; i < Q; ++i) f[i] -= S(w)(s, i);
+    S(store_all)(s, par, n, nb, f);
+    return 1;
+  } else if (code == NRM_OUTXP) {
+    rw = s->wall_u0[n * 4 + 3];
+    R ut[3];
+    S(up_vel)(s, par, n, 1, ut);
+    if (s->out_order >= 2) {
+      R v2[3];
+      S(up_vel)(s, par, n, 2, v2);
+      for (int a = 0; a < 3; ++a) ut[a] = (R)2 * ut[a] - v2[a];
+    }
+    const R un = S(bc_normal_velocity)(s, f, nrm, rw);
+    R utn = 0;
+    for (int a = 0; a < 3; ++a) utn += ut[a] * (R)nrm[a];
+    for (int a = 0; a < 3; ++a) ur[a] = ut[a] + (un - utn) * (R)nrm[a];
+  } else {
+    rw = (code == NRM_CORNER) ? s->bc_rho[n] : S(bc_density)(s, f, nrm, ur);
+  }
+  if (s->fd_corners && s->op != 0 && code == NRM_CORNER) {
+    int px, py, pz;
+    S(coords)(s, n, &px, &py, &pz);
+    const int ic[3] = {px - s->hx, py - s->hy, pz - s->hz};
+    const int nn[3] = {s->nx, s->ny, s->nz};
+    R grad[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    for (int a = 0; a < s->D; ++a) {
+      if (nn[a] < 3) continue;
+      int dir = 0;
+      if (!s->per[a]) {
+        if (ic[a] == 0) dir = 1;
+        else if (ic[a] == nn[a] - 1) dir = -1;
+      }
+      R u1[3], u2[3];
+      int c1[3] = {ic[0], ic[1], ic[2]}, c2[3] = {ic[0], ic[1], ic[2]};
+      if (dir != 0) {
+        c1[a] += dir; c2[a] += 2 * dir;
+        S(vel_at)(s, par, S(idi)(s, c1[0], c1[1], c1[2]), u1);
+        S(vel_at)(s, par, S(idi)(s, c2[0], c2[1], c2[2]), u2);
+        for (int b = 0; b < s->D; ++b)
+          grad[a][b] = (R)dir * ((R)(-1.5) * uw[b] + (R)2 * u1[b] - (R)0.5 * u2[b]);
+      } else {
+        c1[a] = (ic[a] + 1) % nn[a];
+        c2[a] = (ic[a] - 1 + nn[a]) % nn[a];
+        S(vel_at)(s, par, S(idi)(s, c1[0], c1[1], c1[2]), u1);
+        S(vel_at)(s, par, S(idi)(s, c2[0], c2[1], c2[2]), u2);
+        for (int b = 0; b < s->D; ++b) grad[a][b] = (R)0.5 * (u1[b] - u2[b]);
+      }
+    }
+    R Pi[6];
+    S(bc_stress_from_gradient)(rw, s->omega, grad, Pi);
+    S(bc_apply_with_stress)(s, f, rw, ur, Pi);
+  } else {
+    S(bc_apply)(s, f, rw, ur, s->bc_unk[n], s->force_bc ? Fv : 0);
+  }
+  if (unsh)
+    for (int i = 0; i < Q; ++i) f[i] -= S(w)(s, i);
+  return 0;
+}
+
 /* seed_populations -> scatter<P> (:634-637, 1231-1241), sequential node order. */
 static void S(scatter_fn)(S(solver)* s, const double* rho, const double* ux, const double* uy,
                           const double* uz, R rho0, R ux0, R uy0, R uz0, int field) {
@@ -507,7 +946,7 @@ static void S(scatter_fn)(S(solver)* s, const double* rho, const double* ux, con
   long long nb[27];
   for (long long n = 0; n < s->n_padded; ++n) {
     S(neighbours)(s, n, nb);
-    const int fluid = s->flags[n] == 0 || s->flags[n] == 5;  /* SpecNode seeds as fluid */
+    const int fluid = s->flags[n] == 0 || s->flags[n] == 3 || s->flags[n] == 5; /* :557, 575 */
     R r = rho0, a = ux0, b = uy0, c = uz0;
     if (field) {                                             /* initialize_field :568-579 */
       r = (R)1; a = b = c = (R)0;
@@ -540,14 +979,19 @@ void F(step)(void* h, int nsteps, int store_macro) {
   S(solver)* s = (S(solver)*)h;
   for (int t = 0; t < nsteps; ++t) {
     const int par = (int)(s->t % 2);
-#pragma omp parallel for schedule(static)
+    if (s->has_walls && s->has_corners) S(corner_density)(s, par);
+    /* Regularised walls may read neighbour nodes inside the in-place sweep,
+     * so with walls the sweep runs in index order, as the reference's
+     * one-thread build runs it. */
+#pragma omp parallel for schedule(static) if (!s->has_walls)
     for (long long n = 0; n < s->n_padded; ++n) {
       const uint8_t fl = s->flags[n];
-      if (fl != 0 && fl != 4 && fl != 5) continue;           /* Excluded / Solid skipped */
+      if (fl != 0 && fl != 3 && fl != 4 && fl != 5) continue; /* Excluded / Solid skipped */
       long long nb[27];
       R f[27];
       S(neighbours)(s, n, nb);
       S(load_all)(s, par, n, nb, f);
+      if (fl == 3 && S(regwall)(s, par, n, nb, f)) continue;
       if (fl == 4) {                                         /* ghost mirror, no collision */
         const int ax = S(mirror_axis)(s->spec_nrm[n]);
         R g[27];
@@ -585,11 +1029,69 @@ void F(macro)(void* h, double* rho, double* ux, double* uy, double* uz) {
   const int par = (int)(s->t % 2);
   for (long long n = 0; n < s->n_padded; ++n) {
     const uint8_t fl = s->flags[n];
-    if (fl != 0 && fl != 5) { s->rho[n] = s->ux[n] = s->uy[n] = s->uz[n] = (R)0; continue; }
+    if (fl != 0 && fl != 3 && fl != 5) { s->rho[n] = s->ux[n] = s->uy[n] = s->uz[n] = (R)0; continue; }
     long long nb[27];
     R f[27];
     S(neighbours)(s, n, nb);
     S(load_all)(s, par, n, nb, f);
+    if (fl == 3) {                                           /* :1085-1188, reported state */
+      if (S(unshift)(s))
+        for (int i = 0; i < s->Q; ++i) f[i] += S(w)(s, i);
+      const uint8_t code = s->bc_nrm[n];
+      int nrm[3];
+      S(normal_of)(code, nrm);
+      R uw[3];
+      S(wall_vel)(s, n, uw);
+      R rw;
+      if (code == NRM_OUTFREE) {
+        rw = s->outflow_rho;
+        int onr[3];
+        S(normal_of)(s->bc_onrm[n], onr);
+        R g[27];
+        S(load_node)(s, par, s->bc_don[n], g, S(unshift)(s));
+        R sm = 0, m4[3] = {0, 0, 0};
+        for (int i = 0; i < s->Q; ++i) {
+          sm += g[i];
+          for (int a = 0; a < 3; ++a) m4[a] += g[i] * (R)S(c)(s, i, a);
+        }
+        const R ir = (sm > (R)0) ? (R)1 / sm : (R)0;
+        const R un = S(bc_normal_velocity)(s, f, onr, rw);
+        R utn = 0;
+        for (int a = 0; a < 3; ++a) utn += m4[a] * ir * (R)onr[a];
+        for (int a = 0; a < 3; ++a) uw[a] = m4[a] * ir + (un - utn) * (R)onr[a];
+      } else if (code == NRM_OUTEQ) {
+        rw = s->wall_u0[n * 4 + 3];
+        int px, py, pz;
+        S(coords)(s, n, &px, &py, &pz);
+        R g[27];
+        S(load_node)(s, par, S(idi)(s, px - s->hx - 1, py - s->hy, pz - s->hz), g, S(unshift)(s));
+        R sm = 0, mu[3] = {0, 0, 0};
+        for (int i = 0; i < s->Q; ++i) {
+          sm += g[i];
+          for (int a = 0; a < 3; ++a) mu[a] += g[i] * (R)S(c)(s, i, a);
+        }
+        const R ir = (sm > (R)0) ? (R)1 / sm : (R)0;
+        for (int a = 0; a < 3; ++a) uw[a] = mu[a] * ir;
+      } else if (code == NRM_OUTXP) {
+        rw = s->wall_u0[n * 4 + 3];
+        R ut[3];
+        S(up_vel)(s, par, n, 1, ut);
+        if (s->out_order >= 2) {
+          R v2[3];
+          S(up_vel)(s, par, n, 2, v2);
+          for (int a = 0; a < 3; ++a) ut[a] = (R)2 * ut[a] - v2[a];
+        }
+        const R un = S(bc_normal_velocity)(s, f, nrm, rw);
+        R utn = 0;
+        for (int a = 0; a < 3; ++a) utn += ut[a] * (R)nrm[a];
+        for (int a = 0; a < 3; ++a) uw[a] = ut[a] + (un - utn) * (R)nrm[a];
+      } else {
+        rw = (code == NRM_CORNER) ? s->bc_rho[n] : S(bc_density)(s, f, nrm, uw);
+      }
+      s->rho[n] = rw;
+      s->ux[n] = uw[0]; s->uy[n] = uw[1]; s->uz[n] = uw[2];
+      continue;
+    }
     if (fl == 5) {                                           /* :1061-1080, raw moments */
       S(mirror_faces)(s, f, s->spec_faces[n]);
       if (s->shifted && s->op != 0)                          /* no-collision runs raw */
@@ -619,7 +1121,7 @@ static double S(reduce)(S(solver)* s, int axis) {
   const int par = (int)(s->t % 2);
   R sum = 0;
   for (long long n = 0; n < s->n_padded; ++n) {
-    if (s->flags[n] != 0 && s->flags[n] != 5) continue;
+    if (s->flags[n] != 0 && s->flags[n] != 3 && s->flags[n] != 5) continue;
     long long nb[27];
     R f[27];
     S(neighbours)(s, n, nb);

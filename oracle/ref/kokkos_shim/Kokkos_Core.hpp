@@ -41,6 +41,7 @@ struct HostSpace {
 struct OpenMP {
   using memory_space = HostSpace;
   using execution_space = OpenMP;
+  static const char* name() { return "OpenMP"; }
 };
 using DefaultExecutionSpace = OpenMP;
 using DefaultHostExecutionSpace = OpenMP;

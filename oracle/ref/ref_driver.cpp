@@ -90,6 +90,40 @@ int ref_set_specular_walls(void* h, const std::uint8_t* codes) {
   static_cast<refdrv::Base*>(h)->set_specular_walls(codes);
   return 0;
 }
+// Normal codes per interior node and (ux, uy, uz, rho) per node or NULL.
+// Rejected (-1, nothing changed), as the C ABI rejects them: a code above
+// NrmOutEq, and a pressure / equilibrium outlet whose upstream stencil leaves
+// the interior (x below the outflow order, resp. below 1).
+int ref_set_regularized_walls(void* h, const std::uint8_t* codes, const double* spec) {
+  auto* b = static_cast<refdrv::Base*>(h);
+  const long long n = ref_interior(h), nx = b->nx();
+  for (long long k = 0; k < n; ++k) {
+    const unsigned c = codes[k];
+    if (c > NrmOutEq) return -1;
+    if ((c == NrmOutXp || c == NrmOutEq) && k % nx < (c == NrmOutXp ? b->out_order : 1)) return -1;
+  }
+  b->wall_codes.assign(codes, codes + n);
+  b->set_regularized_walls(codes, spec);
+  return 0;
+}
+void ref_set_wall_velocity_scale(void* h, double sc) { static_cast<refdrv::Base*>(h)->set_wall_velocity_scale(sc); }
+void ref_set_wall_density(void* h, double r) { static_cast<refdrv::Base*>(h)->set_wall_density(r); }
+void ref_set_wall_velocity_field(void* h, const double* u3) { static_cast<refdrv::Base*>(h)->set_wall_velocity_field(u3); }
+void ref_set_wall_velocity_field_scale(void* h, double sc) {
+  static_cast<refdrv::Base*>(h)->set_wall_velocity_field_scale(sc);
+}
+void ref_set_fd_corners(void* h, int on) { static_cast<refdrv::Base*>(h)->set_fd_corners(on != 0); }
+void ref_set_force_correction(void* h, int on) { static_cast<refdrv::Base*>(h)->set_force_correction(on != 0); }
+int ref_set_outflow_order(void* h, int k) {
+  auto* b = static_cast<refdrv::Base*>(h);
+  const long long nx = b->nx();
+  for (std::size_t i = 0; i < b->wall_codes.size(); ++i)
+    if (b->wall_codes[i] == NrmOutXp && (long long)(i % nx) < (k >= 2 ? 2 : 1)) return -1;
+  b->out_order = k;
+  b->set_outflow_order(k);
+  return 0;
+}
+void ref_set_outflow_density(void* h, double r) { static_cast<refdrv::Base*>(h)->set_outflow_density(r); }
 int ref_set_specular_nodes(void* h, const std::uint8_t* masks) {
   for (long long k = 0; k < ref_interior(h); ++k) {
     const unsigned m = masks[k];

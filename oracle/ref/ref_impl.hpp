@@ -12,6 +12,9 @@
 //   ref_set_geometry      set_geometry(fn(x,y,z) -> CellType)  FluidSolver.hpp:74-82
 //   ref_set_specular_walls set_specular_walls(fn -> NormalCode) FluidSolver.hpp:193-218
 //   ref_set_specular_nodes set_specular_nodes(fn -> SpecFace)   FluidSolver.hpp:236-268
+//   ref_set_regularized_walls set_regularized_walls(fn -> WallSpec) FluidSolver.hpp:372-552
+//   ref_set_wall_* / ref_set_fd_corners / ref_set_force_correction / ref_set_outflow_*
+//                         the wall setters of FluidSolver.hpp:272-370, 1311-1330
 //   ref_initialize        initialize(rho0, ux, uy, uz)         FluidSolver.hpp:553-561
 //   ref_initialize_field  initialize_field(fn(n) -> FlowState) FluidSolver.hpp:568-579
 //   ref_step              step(store_macroscopic)              FluidSolver.hpp:582-591
@@ -33,6 +36,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <memory>
+#include <vector>
 
 using namespace lbm;
 
@@ -59,9 +63,24 @@ struct Params {
 
 struct Base {
   virtual ~Base() = default;
+  // the driver's own record of the wall codes and the outflow order, for the
+  // argument checks of ref_set_regularized_walls / ref_set_outflow_order
+  std::vector<std::uint8_t> wall_codes;
+  int out_order = 1;
   virtual void set_geometry(const std::uint8_t* flags) = 0;
   virtual void set_specular_walls(const std::uint8_t* codes) = 0;
   virtual void set_specular_nodes(const std::uint8_t* masks) = 0;
+  virtual void set_regularized_walls(const std::uint8_t* codes, const double* spec) = 0;
+  virtual void set_wall_velocity_scale(double sc) = 0;
+  virtual void set_wall_density(double r) = 0;
+  virtual void set_wall_velocity_field(const double* u3) = 0;
+  virtual void set_wall_velocity_field_scale(double sc) = 0;
+  virtual void set_fd_corners(bool on) = 0;
+  virtual void set_force_correction(bool on) = 0;
+  virtual void set_outflow_order(int k) = 0;
+  virtual void set_outflow_density(double r) = 0;
+  virtual long long nx() const = 0;
+  virtual long long ny() const = 0;
   virtual void initialize(double rho, double ux, double uy, double uz) = 0;
   virtual void initialize_field(const double* rho, const double* ux, const double* uy,
                                 const double* uz) = 0;
@@ -125,6 +144,38 @@ struct Impl final : Base {
       return masks[(std::size_t(z) * dd.ny + y) * dd.nx + x];
     });
   }
+  void set_regularized_walls(const std::uint8_t* codes, const double* spec) override {
+    const Domain dd = d;
+    using WS = typename FluidSolver<L, Strm, Coll>::WallSpec;
+    s.set_regularized_walls([&](Index x, Index y, Index z) -> WS {
+      const std::size_t k = (std::size_t(z) * dd.ny + y) * dd.nx + x;
+      WS w;
+      w.normal = codes[k];
+      if (spec) {
+        w.ux = Real(spec[4 * k]); w.uy = Real(spec[4 * k + 1]);
+        w.uz = Real(spec[4 * k + 2]); w.rho = Real(spec[4 * k + 3]);
+      }
+      return w;
+    });
+  }
+  void set_wall_velocity_scale(double sc) override { s.set_wall_velocity_scale(Real(sc)); }
+  void set_wall_density(double r) override { s.set_wall_density(Real(r)); }
+  void set_wall_velocity_field(const double* u3) override {
+    const Domain dd = d;
+    s.set_wall_velocity_field([&](Index x, Index y, Index z) -> std::array<Real, 3> {
+      const std::size_t k = (std::size_t(z) * dd.ny + y) * dd.nx + x;
+      return {Real(u3[3 * k]), Real(u3[3 * k + 1]), Real(u3[3 * k + 2])};
+    });
+  }
+  void set_wall_velocity_field_scale(double sc) override {
+    s.set_wall_velocity_field_scale(Real(sc));
+  }
+  void set_fd_corners(bool on) override { s.set_fd_corners(on); }
+  void set_force_correction(bool on) override { s.set_force_correction(on); }
+  void set_outflow_order(int k) override { s.set_outflow_order(k); }
+  void set_outflow_density(double r) override { s.set_outflow_density(Real(r)); }
+  long long nx() const override { return d.nx; }
+  long long ny() const override { return d.ny; }
   void initialize(double rho, double ux, double uy, double uz) override {
     s.initialize(Real(rho), Real(ux), Real(uy), Real(uz));
   }

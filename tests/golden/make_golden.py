@@ -121,6 +121,100 @@ def spec_geometry(lat, shape, kind):
     return fl, codes, masks
 
 
+# Regularised walls (FluidSolver.hpp:372-552, 792-1021).  name -> (lattice,
+# op, eq, shifted, forcing, shape, kind, omega, omega2, steps, precision).
+WALL_CASES = {
+    "d2q9_bgk_cavity_f64": (9, "bgk", 0, 1, 0, (10, 9, 1), "cavity", 1.3, -1.0, 25, "f64"),
+    "d3q27_cm_inout_guo_f64": (27, "cm", 0, 1, 1, (9, 7, 5), "inout", 1.5, -1.0, 12, "f64"),
+    "d3q27_trt_outfree_f32": (27, "trt", 0, 1, 1, (9, 6, 5), "outfree", 1.4, 1.1, 10, "f32"),
+    "d2q9_mrt_fdcorner_f32": (9, "mrt", 0, 0, 1, (10, 9, 1), "fdcorner", 1.2, 1.5, 15, "f32"),
+}
+WALL_PERIODIC = {"couette": (True, False, True), "cavity": (False, False, True),
+                 "inout": (False, False, True), "outeq": (False, False, True),
+                 "outfree": (False, False, True), "fdcorner": (True, False, True)}
+
+
+def wall_geometry(lat, shape, kind):
+    """(flags, normal codes, states (nz, ny, nx, 4)) over the interior.
+
+    couette : RegWall floor (u = 0) and lid (u = (0.02, 0.01, 0)), periodic x;
+    cavity  : a box of RegWall faces, lid u = (0.05, 0, 0), NrmCorner on the
+              corners (edges in 3-D, z periodic): corner densities and the
+              finite-difference corner stress;
+    inout   : solid floor and ceiling, velocity inlet at x = 0, pressure
+              outlet (NrmOutXp, rho 1.01) at x = nx-1;
+    outeq   : the same with the equilibrium outlet (NrmOutEq);
+    outfree : solid floor and ceiling, arbitrary-face outflow (NrmOutFree) on
+              both x faces, so one donor precedes its node in index order and
+              one follows it;
+    fdcorner: RegWall floor and lid, periodic x, with NrmCorner nodes inside
+              both rows, whose finite-difference stencil reads fluid nodes
+              above (later in index order) and below (earlier) them."""
+    nx, ny, nz = shape
+    fl = np.zeros((nz, ny, nx), np.uint8)
+    codes = np.zeros_like(fl)
+    st = np.zeros((nz, ny, nx, 4))
+    st[..., 3] = 1.0
+    if kind == "couette":
+        codes[:, 0, :] = 4
+        codes[:, -1, :] = 3
+        st[:, -1, :, 0] = 0.02
+        st[:, -1, :, 1] = 0.01
+    elif kind == "cavity":
+        codes[:, :, 0] = 2
+        codes[:, :, -1] = 1
+        codes[:, 0, :] = 4
+        codes[:, -1, :] = 3
+        st[:, -1, :, 0] = 0.05
+        for y in (0, ny - 1):
+            for x in (0, nx - 1):
+                codes[:, y, x] = 7
+                st[:, y, x, 0] = 0.0
+    elif kind in ("inout", "outeq"):
+        fl[:, 0, :] = 1
+        fl[:, -1, :] = 1
+        codes[:, 1:-1, 0] = 2
+        st[:, 1:-1, 0, 0] = 0.03
+        codes[:, 1:-1, -1] = 8 if kind == "inout" else 10
+        st[:, 1:-1, -1, 3] = 1.01
+    elif kind == "outfree":
+        fl[:, 0, :] = 1
+        fl[:, -1, :] = 1
+        codes[:, 1:-1, 0] = 9
+        codes[:, 1:-1, -1] = 9
+    elif kind == "fdcorner":
+        codes[:, 0, :] = 4
+        codes[:, -1, :] = 3
+        st[:, -1, :, 0] = 0.03
+        codes[:, 0, 3] = 7
+        codes[:, -1, nx - 3] = 7
+        st[:, -1, nx - 3, 0] = 0.03
+    else:
+        raise ValueError(kind)
+    return fl, codes, st
+
+
+def run_wall(backend, case, seed, quant=None):
+    lat, op, eq, sh, fo, shape, kind, om, om2, steps, prec = case
+    nx, ny, nz = shape
+    per = WALL_PERIODIC[kind]
+    F = (2e-5, -1e-5, 3e-6 if lat == 27 else 0.0) if fo else (0.0, 0.0, 0.0)
+    s = O.CpuSolver(backend, lattice=lat, op=op, eq=eq, shifted=sh, forcing=fo, nx=nx, ny=ny,
+                    nz=nz, px=per[0], py=per[1], pz=per[2], omega=om, omega2=om2, fx=F[0],
+                    fy=F[1], fz=F[2], precision=prec, quant=quant)
+    fl, codes, st = wall_geometry(lat, shape, kind)
+    s.set_geometry(fl)
+    s.set_regularized_walls(codes, st)
+    s.initialize_field(*initial_field(shape, seed))
+    p0 = s.gather()
+    s.step(steps, store_macro=True)
+    out = {"pops0": p0, "pops": s.gather(), "stored": np.stack(s.stored_macro()),
+           "macro": np.stack(s.macro()), "mass": s.total_mass(),
+           "mom": np.array([s.total_momentum(a) for a in range(3)]), "slots": s.slot_sum()}
+    s.close()
+    return out
+
+
 def run_spec(backend, case, seed, quant=None):
     lat, op, eq, sh, fo, shape, kind, om, om2, steps, prec = case
     nx, ny, nz = shape
@@ -157,6 +251,10 @@ def main():
     for k, (name, case) in enumerate(SPEC_CASES.items()):
         r = run_spec("ref", case, seed=200 + k)
         np.savez_compressed(HERE / f"{name}.npz", case=np.array(repr(case)), seed=200 + k, **r)
+        print(name, "mass", r["mass"])
+    for k, (name, case) in enumerate(WALL_CASES.items()):
+        r = run_wall("ref", case, seed=300 + k)
+        np.savez_compressed(HERE / f"{name}.npz", case=np.array(repr(case)), seed=300 + k, **r)
         print(name, "mass", r["mass"])
 
 

@@ -65,6 +65,17 @@ class Case:
             self.gpu.set_specular_nodes(masks)
             self.cpu.set_specular_nodes(masks)
 
+    def regularized(self, codes, states=None):
+        """Regularised walls on both sides (codes per interior node, states
+        (nz, ny, nx, 4) or None)."""
+        self.gpu.set_regularized_walls(codes, states)
+        self.cpu.set_regularized_walls(codes, states)
+
+    def both(self, name, *args):
+        """Call the same setter on the device solver and the oracle."""
+        getattr(self.gpu, name)(*args)
+        getattr(self.cpu, name)(*args)
+
     def init_random(self, seed=0, amp=0.03):
         rng = np.random.default_rng(seed)
         rho = 1 + 0.01 * rng.standard_normal(self.shape)

@@ -107,27 +107,34 @@ def test_reference_example_runs_on_device(cuda_device, tmp_path):
     assert out.exists() and len(out.read_text().splitlines()) == 49
 
 
-# ------------------------------------------------ free-slip wall validations
-# The reference's validation/specular.cpp, specular_node.cpp and
-# specwall_unsteady.cpp, built unmodified against the facade (`*_b200`, run on
-# the device) and against the host Kokkos stand-in (`*_cpu`, the reference's
-# own run): each must pass its own checks on the device and print the same
-# figures as the reference.
+# ------------------------------------------------------ wall validations
+# The reference's validation/specular.cpp, specular_node.cpp,
+# specwall_unsteady.cpp, regularized.cpp and cavity.cpp, built unmodified
+# against the facade (`*_b200`, run on the device): each must pass its own
+# checks there and print the figures the reference prints on the host
+# (tests/golden/validation/<name>.txt, made by make_validation_golden.py).
 REF_DIR = ROOT / "oracle" / "_ref"
+VGOLD = ROOT / "tests" / "golden" / "validation"
 _NUM = r"[-+]?\d+\.\d+(?:e[-+]\d+)?"
 
 
 def _validation(name, *args):
-    exe = REF_DIR / name
+    exe = REF_DIR / f"{name}_b200"
     if not exe.exists():
-        pytest.skip(f"{name} not built (make -C oracle facade-drivers ref-validation)")
-    env = dict(os.environ, OMP_NUM_THREADS=str(min(8, os.cpu_count() or 1)))
-    r = subprocess.run([str(exe), *args], capture_output=True, text=True, timeout=900, env=env)
-    return r.returncode, r.stdout
+        pytest.skip(f"{name}_b200 not built (make -C oracle facade-drivers)")
+    r = subprocess.run([str(exe), *args], capture_output=True, text=True, timeout=1200)
+    return r.returncode, r.stdout, (VGOLD / f"{name}.txt").read_text()
 
 
 def _figures(text, key):
     return [[float(v) for v in re.findall(_NUM, ln)] for ln in text.splitlines() if key in ln]
+
+
+def _same_figures(out, ref, key, rtol, atol=0.0):
+    got, want = _figures(out, key), _figures(ref, key)
+    assert len(got) == len(want) > 0, key
+    for a, b in zip(got, want):
+        np.testing.assert_allclose(a, b, rtol=rtol, atol=atol, err_msg=key)
 
 
 @pytest.mark.gpu
@@ -135,38 +142,65 @@ def test_reference_specular_validation_on_device(cuda_device):
     """Half channel closed by the ghost mirror = lower half of the full
     channel to round-off, planes at 0.5 / H + 0.5, mass conserved
     (validation/specular.cpp:103-160), for D2Q9 at tau 0.8 and 1.2 and D3Q27."""
-    rc, out = _validation("specular_b200")
+    rc, out, ref = _validation("specular")
     assert rc == 0 and out.rstrip().endswith("PASS"), out
-    rc_ref, ref = _validation("specular_cpu")
-    assert rc_ref == 0
-    for key in ("no-slip plane", "symmetry plane", "u_max"):
-        for a, b in zip(_figures(out, key), _figures(ref, key), strict=True):
-            np.testing.assert_allclose(a, b, rtol=1e-9, atol=1e-15, err_msg=key)
+    for key in ("no-slip plane", "symmetry plane"):
+        _same_figures(out, ref, key, rtol=1e-9)
+    _same_figures(out, ref, "u_max", rtol=1e-9, atol=1e-15)
 
 
 @pytest.mark.gpu
 def test_reference_specular_node_validation_on_device(cuda_device):
     """On-node mirror: half box = periodic box to 1e-12 in 2-D, quarter box
     with two-face edges in 3-D (validation/specular_node.cpp:284-368)."""
-    rc, out = _validation("specular_node_b200")
+    rc, out, ref = _validation("specular_node")
     assert rc == 0 and out.rstrip().endswith("PASS"), out
     assert out.count(" ok") == 6
-    rc_ref, ref = _validation("specular_node_cpu")
-    assert rc_ref == 0
     # the control (halfway mirror on the same box) differs by the same amount
-    a, b = _figures(out, "CONTROL")[0], _figures(ref, "CONTROL")[0]
-    np.testing.assert_allclose(a, b, rtol=1e-9)
+    _same_figures(out, ref, "CONTROL", rtol=1e-9)
 
 
 @pytest.mark.gpu
 def test_reference_specwall_unsteady_on_device(cuda_device):
     """The ghost mirror's first-order error for unsteady modes: the device
     prints the reference's figures (validation/specwall_unsteady.cpp:79-91)."""
-    rc, out = _validation("specwall_unsteady_b200")
+    rc, out, ref = _validation("specwall_unsteady")
     assert rc == 0, out
-    rc_ref, ref = _validation("specwall_unsteady_cpu")
-    assert rc_ref == 0
-    got, want = _figures(out, "SpecWall half box"), _figures(ref, "SpecWall half box")
+    _same_figures(out, ref, "SpecWall half box", rtol=5e-3)
+
+
+@pytest.mark.gpu
+def test_reference_regularized_validation_on_device(cuda_device):
+    """Regularised walls: Couette exact, the wall ON the node at every tau,
+    second-order Poiseuille on D2Q9 and D3Q27 (validation/regularized.cpp),
+    with the reference's error table to 1e-6."""
+    rc, out, ref = _validation("regularized")
+    assert rc == 0, out
+    # W, L2 error, order, wall position, steps: identical convergence tables
+    got = [ln.split() for ln in out.splitlines() if re.match(r"\s+(8|16|32)\s+\d\.\d+e", ln)]
+    want = [ln.split() for ln in ref.splitlines() if re.match(r"\s+(8|16|32)\s+\d\.\d+e", ln)]
     assert len(got) == len(want) == 6
     for a, b in zip(got, want):
-        np.testing.assert_allclose(a, b, rtol=5e-3)
+        assert a[0] == b[0]
+        np.testing.assert_allclose(float(a[1]), float(b[1]), rtol=1e-6)
+        # steps to steady state: the stopping test sits at round-off level
+        assert abs(int(a[-1]) - int(b[-1])) <= 0.05 * int(b[-1])
+    # the fitted wall planes: at 0 and W to round-off on both sides
+    got_planes = [ln.split() for ln in out.splitlines() if re.match(r"\s+\d\.\d\d\s+(8|16)\s", ln)]
+    assert len(got_planes) == 8
+    for row in got_planes:
+        assert abs(float(row[2])) < 1e-12 and abs(float(row[3]) - float(row[1])) < 1e-9
+
+
+@pytest.mark.gpu
+def test_reference_cavity_validation_on_device(cuda_device):
+    """Lid-driven cavity at Re = 100 with regularised walls and
+    finite-difference corners against Ghia et al.: the device's centreline
+    profiles equal the reference's (validation/cavity.cpp)."""
+    rc, out, ref = _validation("cavity")
+    assert rc == 0 and "DIVERGED" not in out, out
+    rows = lambda t: [ln.split() for ln in t.splitlines() if re.match(r"\s+0\.\d+\s+-?\d\.\d+\s+-?\d", ln)]
+    got, want = rows(out), rows(ref)
+    assert len(got) == len(want) > 10
+    for a, b in zip(got, want):
+        np.testing.assert_allclose([float(v) for v in a], [float(v) for v in b], atol=2e-5)

@@ -131,9 +131,9 @@ def test_setters_reject_what_the_reference_rejects(cuda_device):
     t.close()
 
 
-def test_specular_runs_one_node_kernel_whatever_the_option(cuda_device):
-    """A row-kernel request on a lattice with specular nodes still gives the
-    one-node result (the chunk kernels have no specular branch)."""
+def test_specular_same_under_every_bulk_kernel(cuda_device):
+    """Wall nodes are updated by the boundary pass, whatever bulk kernel runs
+    the fluid: the one-node, paired and row kernels give one result."""
     res = []
     for kernel in (capi.KERNEL_NODES, capi.KERNEL_ROWS, capi.KERNEL_PAIRS):
         c = _case(27, 4, 0, -1.0, "f16", True, False, "mixed", shape=(64, 6, 4))

@@ -266,3 +266,117 @@ def test_oracle_specular_wall_conserves_mass():
     s.step(200)
     assert abs(s.total_mass() - m0) / m0 < 1e-13
     s.close()
+
+
+# ------------------------------------------------------- regularised walls
+@pytest.mark.parametrize("name", list(G.WALL_CASES))
+def test_oracle_reproduces_wall_golden(name):
+    """RegWall fixtures (velocity walls, corners, outlets) made by the reference build."""
+    d = np.load(GOLDEN / f"{name}.npz")
+    r = G.run_wall("oracle", G.WALL_CASES[name], seed=int(d["seed"]))
+    for k in ("pops0", "pops", "stored", "macro"):
+        np.testing.assert_array_equal(r[k], d[k], err_msg=k)
+    assert r["mass"] == float(d["mass"])
+    np.testing.assert_array_equal(r["mom"], d["mom"])
+    assert r["slots"] == float(d["slots"])
+
+
+@needs_ref
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+@pytest.mark.parametrize("kind", list(G.WALL_PERIODIC))
+def test_oracle_walls_bit_identical_to_reference(prec, kind):
+    """Every operator, storage convention and force on both lattices, against
+    the reference run on one thread (its outflow and corner branches read
+    neighbour nodes inside the in-place sweep, so its result is defined by
+    the sweep order; one thread is index order)."""
+    O.set_ref_threads(1, prec)
+    ops = [("none", 0, -1.0), ("bgk", 0, -1.0), ("bgk", 1, -1.0), ("trt", 0, 1.1),
+           ("mrt", 0, 1.5), ("cm", 0, -1.0)]
+    for lat, (op, eq, om2), shifted, forcing in itertools.product([9, 27], ops, [1, 0], [0, 1]):
+        shape = (10, 9, 1) if lat == 9 else (8, 7, 5)
+        case = (lat, op, eq, shifted, forcing, shape, kind, 1.3, om2, 7, prec)
+        a = G.run_wall("oracle", case, seed=7)
+        b = G.run_wall("ref", case, seed=7)
+        for k in a:
+            np.testing.assert_array_equal(a[k], b[k], err_msg=f"{case} {k}")
+
+
+WALL_MODIFIERS = {
+    "scale": [("set_wall_velocity_scale", 0.5)],
+    "density": [("set_wall_density", 1.02)],
+    "field": [("set_wall_velocity_field", "field"), ("set_wall_velocity_field_scale", 0.7)],
+    "no_fd": [("set_fd_corners", False)],
+    "no_force_bc": [("set_force_correction", False)],
+    "order2": [("set_outflow_order", 2)],
+    "outflow_rho": [("set_outflow_density", 0.98)],
+}
+
+
+@needs_ref
+@pytest.mark.parametrize("mod", list(WALL_MODIFIERS))
+@pytest.mark.parametrize("kind", ["cavity", "inout", "outfree", "fdcorner"])
+def test_oracle_wall_setters_match_reference(mod, kind):
+    O.set_ref_threads(1, "f64")
+    lat, shape = 27, (8, 7, 5)
+    nx, ny, nz = shape
+    per = G.WALL_PERIODIC[kind]
+    out = []
+    for backend in ("oracle", "ref"):
+        s = O.CpuSolver(backend, lattice=lat, op="bgk", shifted=1, forcing=1, nx=nx, ny=ny, nz=nz,
+                        px=per[0], py=per[1], pz=per[2], omega=1.3, fx=2e-5, fy=-1e-5, fz=3e-6,
+                        precision="f64")
+        fl, codes, st = G.wall_geometry(lat, shape, kind)
+        s.set_geometry(fl)
+        s.set_regularized_walls(codes, st)
+        for fn, arg in WALL_MODIFIERS[mod]:
+            if arg == "field":
+                arg = 0.01 * np.random.default_rng(2).standard_normal((nz, ny, nx, 3))
+            getattr(s, fn)(arg)
+        s.initialize_field(*G.initial_field(shape, 9))
+        s.step(6, store_macro=True)
+        out.append((s.gather(), s.stored_macro(), s.macro(), s.total_mass()))
+        s.close()
+    (ga, sa, ma, mass_a), (gb, sb, mb, mass_b) = out
+    np.testing.assert_array_equal(ga, gb)
+    for x, y in zip(sa + ma, sb + mb):
+        np.testing.assert_array_equal(x, y)
+    assert mass_a == mass_b
+
+
+def test_oracle_wall_setters_reject():
+    s = O.CpuSolver("oracle", lattice=9, op="bgk", nx=8, ny=6, nz=1, px=False, py=False,
+                    precision="f64")
+    codes = np.zeros((1, 6, 8), np.uint8)
+    codes[0, 2, 3] = 11
+    with pytest.raises(ValueError):
+        s.set_regularized_walls(codes)
+    codes[0, 2, 3] = 0
+    codes[0, 2, 0] = 8
+    with pytest.raises(ValueError):
+        s.set_regularized_walls(codes)
+    codes[0, 2, 0] = 0
+    codes[0, 2, 1] = 8
+    s.set_regularized_walls(codes)
+    with pytest.raises(ValueError):
+        s.set_outflow_order(2)
+    s.close()
+
+
+def test_oracle_couette_between_regularized_walls_is_exact():
+    """Linear profiles carry no curvature slip (FluidSolver.hpp:1296-1303:
+    Couette exact to round-off at every tau)."""
+    ny, U = 10, 0.04
+    s = O.CpuSolver("oracle", lattice=9, op="bgk", nx=4, ny=ny, nz=1, px=True, py=False,
+                    omega=1.1, precision="f64")
+    codes = np.zeros((1, ny, 4), np.uint8)
+    st = np.zeros((1, ny, 4, 4))
+    st[..., 3] = 1.0
+    codes[0, 0, :] = 4
+    codes[0, -1, :] = 3
+    st[0, -1, :, 0] = U
+    s.set_regularized_walls(codes, st)
+    s.initialize(1.0)
+    s.step(6000)
+    ux = s.macro()[1][0, :, 0]
+    np.testing.assert_allclose(ux, U * np.arange(ny) / (ny - 1), rtol=0, atol=1e-10)
+    s.close()
