@@ -262,6 +262,63 @@ def gpu_arm(args, rank, world, dist):
         out["accuracy"] = accuracy_arm(args, dev, stream, omega)
     if rank == 0 and world == 1 and args.serve_requests > 0:
         out["serving"] = serving_arm(args)
+    if rank == 0 and world == 1 and args.walls_steps > 0:
+        out["walls"] = walls_arm(args, stream, omega)
+    return out
+
+
+def walls_arm(args, stream, omega):
+    """Cost of wall nodes on the headline lattice: the periodic box against
+    a channel (periodic x and z) closed by regularised velocity walls, a
+    resting floor at y = 0 and a lid moving at u0 at y = N-1, both driven
+    through the boundary-node pass after the bulk kernel; and the same
+    channel with free-slip ghost walls (SpecWall).  Same operator, storage
+    and kernel choice as the headline; CUDA events over args.walls_steps
+    steps each."""
+    import torch
+    from m3lb_b200 import capi
+    from m3lb_b200 import solver as S
+
+    n = args.size
+    out = {"workload": f"D3Q27 CM {n}^3 {args.storage}: periodic box vs channel walls at y = 0, {n - 1}",
+           "steps": args.walls_steps, "wall_nodes": 2 * n * n}
+
+    def timed(kind):
+        dom = S.Domain(n, n, n, True, kind == "periodic", True)
+        coll = S.CentralMoments(S.D3Q27, S.NoForcing(), S.ShiftedPopulations, omega=omega)
+        s = S.FluidSolver(dom, coll, storage=args.storage)
+        s.set_stream(stream)
+        s.set_option(capi.OPT_KERNEL, KERNELS[args.kernel])
+        codes = np.zeros((n, n, n), np.uint8)
+        if kind == "regwall":
+            st = np.zeros((n, n, n, 4))
+            st[..., 3] = 1.0
+            st[:, -1, :, 0] = U0
+            codes[:, 0, :] = 4
+            codes[:, -1, :] = 3
+            s.set_regularized_walls(codes, st)
+        elif kind == "specwall":
+            codes[:, 0, :] = 4
+            codes[:, -1, :] = 3
+            s.set_specular_walls(codes)
+        del codes
+        s.initialize(1.0)
+        s.steps(5)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        s.steps(args.walls_steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / args.walls_steps
+        launches = s.launch_count()
+        s.close()
+        return {"ms_per_step": ms, "glups": n ** 3 / ms / 1e6, "launches_total": launches}
+
+    for kind in ("periodic", "regwall", "specwall"):
+        out[kind] = timed(kind)
+    for kind in ("regwall", "specwall"):
+        out[kind]["vs_periodic"] = out["periodic"]["ms_per_step"] / out[kind]["ms_per_step"]
     return out
 
 
@@ -511,6 +568,8 @@ def main():
     ap.add_argument("--serve-budget-gb", type=int, default=4)
     ap.add_argument("--serve-resident", type=int, default=16)
     ap.add_argument("--serve-round", type=int, default=100)
+    ap.add_argument("--walls-steps", type=int, default=100,
+                    help="steps of each wall-cost measurement (0: skip it)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
