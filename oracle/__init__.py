@@ -33,6 +33,28 @@ _u8p = C.POINTER(C.c_uint8)
 _vp = C.c_void_p
 
 
+_SCALAR_SIG = {
+    "screate": (_vp, [C.c_int] * 8 + [C.c_double] * 3),
+    "sdestroy": (None, [_vp]),
+    "sset_geometry": (None, [_vp, _u8p]),
+    "sset_wall_values": (None, [_vp, _dp]),
+    "sset_specular_walls": (C.c_int, [_vp, _u8p]),
+    "sset_specular_nodes": (C.c_int, [_vp, _u8p]),
+    "sset_omega_field": (None, [_vp, _dp]),
+    "sset_velocity": (None, [_vp, _dp, _dp, _dp]),
+    "sfinalize_geometry": (None, [_vp]),
+    "sinitialize": (None, [_vp, C.c_double]),
+    "sinitialize_field": (None, [_vp, _dp]),
+    "sstep": (None, [_vp, C.c_int]),
+    "sadd_source": (None, [_vp, _dp]),
+    "scompute_field": (None, [_vp]),
+    "sfield": (None, [_vp, _dp]),
+    "stotal": (C.c_double, [_vp]),
+    "sn_padded": (C.c_longlong, [_vp]),
+    "stimestep": (C.c_longlong, [_vp]),
+}
+
+
 def _bind(lib, prefix):
     sig = {
         "create": (_vp, [C.c_int] * 6 + [C.c_int] * 6 + [C.c_double] * 5),
@@ -62,6 +84,11 @@ def _bind(lib, prefix):
         "n_padded": (C.c_longlong, [_vp]),
         "timestep": (C.c_longlong, [_vp]),
     }
+    sig["set_buoyancy"] = ((C.c_int if prefix == "ref_" else None),
+                           [_vp, _dp] + [C.c_double] * 6)
+    sig.update(_SCALAR_SIG)
+    if prefix != "ref_":  # the reference solver has no population readout
+        sig["sgather"] = (None, [_vp, _dp])
     fns = {}
     for name, (res, args) in sig.items():
         fn = getattr(lib, prefix + name)
@@ -214,6 +241,16 @@ class CpuSolver:
     def set_outflow_density(self, r):
         self._f["set_outflow_density"](self._h, float(r))
 
+    def set_buoyancy(self, T, g=(0.0, 1.0, 0.0), rho0=1.0, beta=1.0, T0=0.0):
+        """Boussinesq force F = f + g rho0 beta (T - T0) per node (BoussinesqGuo,
+        Forcing.hpp:93-127); T per interior node.  The reference build needs a
+        solver made with forcing=2 for this."""
+        a = np.ascontiguousarray(np.broadcast_to(T, self.shape), dtype=np.float64)
+        rc = self._f["set_buoyancy"](self._h, _ptr(a), *map(float, g), float(rho0), float(beta),
+                                     float(T0))
+        if rc is not None and rc != 0:
+            raise ValueError("set_buoyancy: this solver has no Boussinesq forcing")
+
     def initialize(self, rho0=1.0, ux=0.0, uy=0.0, uz=0.0):
         self._f["initialize"](self._h, rho0, ux, uy, uz)
 
@@ -257,6 +294,115 @@ class CpuSolver:
     @property
     def timestep(self):
         return int(self._f["timestep"](self._h))
+
+
+SOPS = {"bgk": 1, "trt": 2, "regularised": 3}
+
+
+class ScalarCpuSolver:
+    """One scalar (advection-diffusion) lattice on the CPU, the API of the
+    reference's ScalarSolver (src/solver/ScalarSolver.hpp): D2Q5 (lattice 5)
+    or D3Q7 (7), ScalarBGK / ScalarTRT / ScalarRegularised.  Interior arrays
+    are (nz, ny, nx); initialize_field takes one value per padded node."""
+
+    def __init__(self, backend="oracle", lattice=7, op="bgk", nx=8, ny=8, nz=8, px=True, py=True,
+                 pz=True, omega=1.0, T_ref=0.0, Lambda=0.25, precision="f64"):
+        self.backend, self.precision = backend, precision
+        self.Q = lattice
+        self.nx, self.ny, self.nz = nx, ny, nz
+        self.shape = (nz, ny, nx)
+        self.per = (bool(px), bool(py), bool(pz))
+        self._f = _lib(backend, precision)
+        opc = SOPS[op] if isinstance(op, str) else int(op)
+        h = self._f["screate"](lattice, opc, nx, ny, nz, int(px), int(py), int(pz), omega, T_ref,
+                               Lambda)
+        if not h:
+            raise ValueError("unsupported scalar configuration")
+        self._h = h
+        self.n_padded = int(self._f["sn_padded"](h))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._f["sdestroy"](self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _u8(self, a):
+        return np.ascontiguousarray(np.broadcast_to(a, self.shape), dtype=np.uint8)
+
+    def _f64(self, a, shape=None):
+        return np.ascontiguousarray(np.broadcast_to(a, shape or self.shape), dtype=np.float64)
+
+    def set_geometry(self, cells):
+        a = self._u8(cells)
+        self._f["sset_geometry"](self._h, a.ctypes.data_as(_u8p))
+
+    def set_wall_values(self, tw):
+        a = self._f64(tw)
+        self._f["sset_wall_values"](self._h, _ptr(a))
+
+    def set_specular_walls(self, codes):
+        a = self._u8(codes)
+        if self._f["sset_specular_walls"](self._h, a.ctypes.data_as(_u8p)) != 0:
+            raise ValueError("set_specular_walls: normal code outside 0..6")
+
+    def set_specular_nodes(self, masks):
+        a = self._u8(masks)
+        if self._f["sset_specular_nodes"](self._h, a.ctypes.data_as(_u8p)) != 0:
+            raise ValueError("set_specular_nodes: rejected mask")
+
+    def set_omega_field(self, om):
+        a = self._f64(om)
+        self._f["sset_omega_field"](self._h, _ptr(a))
+
+    def set_velocity(self, ux, uy=None, uz=None):
+        if ux is None:
+            self._f["sset_velocity"](self._h, None, None, None)
+            return
+        arrs = [self._f64(v) for v in (ux, uy, uz)]
+        self._f["sset_velocity"](self._h, *[_ptr(v) for v in arrs])
+
+    def finalize_geometry(self):
+        self._f["sfinalize_geometry"](self._h)
+
+    def initialize(self, T0):
+        self._f["sinitialize"](self._h, float(T0))
+
+    def initialize_field(self, T_padded):
+        a = self._f64(T_padded, (self.n_padded,))
+        self._f["sinitialize_field"](self._h, _ptr(a))
+
+    def step(self, n=1):
+        self._f["sstep"](self._h, int(n))
+
+    def add_source(self, dC):
+        a = self._f64(dC)
+        self._f["sadd_source"](self._h, _ptr(a))
+
+    def compute_field(self):
+        self._f["scompute_field"](self._h)
+
+    def field(self):
+        out = np.empty(self.shape, np.float64)
+        self._f["sfield"](self._h, _ptr(out))
+        return out
+
+    def total(self):
+        return float(self._f["stotal"](self._h))
+
+    def gather(self):
+        out = np.empty((self.n_padded, self.Q), np.float64)
+        self._f["sgather"](self._h, _ptr(out))
+        return out
+
+    @property
+    def timestep(self):
+        return int(self._f["stimestep"](self._h))
 
 
 def build(ref: bool = True, jobs: int | None = None) -> None:

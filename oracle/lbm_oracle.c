@@ -23,6 +23,16 @@ static const int D3Q27_CZ[27] = {0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, -1, -1, 1,
 static const int D3Q27_W[27] = {64, 16, 16, 16, 16, 16, 16, 4, 4, 4, 4, 4, 4, 4,
                                 4,  4,  4,  4,  4,  1,  1,  1, 1, 1, 1, 1, 1}; /* / 216 */
 
+/* The scalar lattices D2Q5 (w /6, cs2 1/3) and D3Q7 (w /8, cs2 1/4):
+ * rest, then the axis pairs (src/lattice/Lattices.hpp:51-70, 100-121). */
+static const int D2Q5_C[2][5] = {{0, 1, -1, 0, 0}, {0, 0, 0, 1, -1}};
+static const int D2Q5_W[5] = {2, 1, 1, 1, 1};
+static const int D3Q7_C[3][7] = {{0, 1, -1, 0, 0, 0, 0}, {0, 0, 0, 1, -1, 0, 0}, {0, 0, 0, 0, 0, 1, -1}};
+static const int D3Q7_W[7] = {2, 1, 1, 1, 1, 1, 1};
+/* Their axis mirrors: the partner of each axis pair about its own axis. */
+static const int D2Q5_MIR[3][5] = {{0, 2, 1, 3, 4}, {0, 1, 2, 4, 3}, {0, 1, 2, 3, 4}};
+static const int D3Q7_MIR[3][7] = {{0, 2, 1, 3, 4, 5, 6}, {0, 1, 2, 4, 3, 5, 6}, {0, 1, 2, 3, 4, 6, 5}};
+
 /* Direction index for component indices (velocity + 1), the product-basis
  * table pi() of src/collision/ProductBasis.hpp:118-131. */
 static int D2Q9_DIR[3][3];
@@ -58,6 +68,8 @@ __attribute__((constructor)) static void lbmo_init(void) {
 
 /* Normal codes beyond the six axis walls (src/boundary/Regularized.hpp:97-105). */
 enum { NRM_CORNER = 7, NRM_OUTXP = 8, NRM_OUTFREE = 9, NRM_OUTEQ = 10 };
+enum { SB_BULK = 0, SB_ADIABATIC = 1, SB_DIRICHLET = 2, SB_EXCLUDED = 3, SB_MOMENT = 4,
+       SB_OUTFLOW = 5, SB_SPECULAR = 6 };
 
 /* float -> bfloat16 -> float, round to nearest even (NaN kept quiet). */
 static inline float lbmo_bf16_round(float v) {
@@ -76,11 +88,13 @@ static inline float lbmo_bf16_round(float v) {
 #define R double
 #define P lbmo_f64_
 #include "lbm_oracle_body.h"
+#include "lbm_oracle_scalar.h"
 #undef R
 #undef P
 
 #define R float
 #define P lbmo_f32_
 #include "lbm_oracle_body.h"
+#include "lbm_oracle_scalar.h"
 #undef R
 #undef P

@@ -57,6 +57,8 @@
   void P##set_force_correction(void* h, int on);                                     \
   int P##set_outflow_order(void* h, int k);                                          \
   void P##set_outflow_density(void* h, double r);                                    \
+  void P##set_buoyancy(void* h, const double* T, double gx, double gy, double gz,    \
+                       double rho0, double beta, double T0);                         \
   void P##initialize(void* h, double rho, double ux, double uy, double uz);          \
   void P##initialize_field(void* h, const double* rho, const double* ux,             \
                            const double* uy, const double* uz);                      \
@@ -71,7 +73,37 @@
   long long P##n_padded(void* h);                                                    \
   long long P##timestep(void* h);
 
+/* The scalar (advection-diffusion) lattice: src/solver/ScalarSolver.hpp.
+ * lattice 5 (D2Q5) / 7 (D3Q7); op 1 ScalarBGK, 2 ScalarTRT, 3 ScalarRegularised;
+ * cells per interior node: 0 bulk, 1 adiabatic, 2 Dirichlet, 3 excluded,
+ * 4 moment (on-node Dirichlet), 5 outflow, 6 specular.  initialize_field
+ * takes one value per PADDED node, as the reference's fn(n) does. */
+#define LBMO_DECLARE_SCALAR(P)                                                       \
+  void* P##screate(int lattice, int op, int nx, int ny, int nz, int px, int py,      \
+                   int pz, double omega, double T_ref, double Lambda);               \
+  void P##sdestroy(void* h);                                                         \
+  void P##sset_geometry(void* h, const uint8_t* cells);                              \
+  void P##sset_wall_values(void* h, const double* tw);                               \
+  int P##sset_specular_walls(void* h, const uint8_t* codes);                         \
+  int P##sset_specular_nodes(void* h, const uint8_t* masks);                         \
+  void P##sset_omega_field(void* h, const double* omega);                            \
+  void P##sset_velocity(void* h, const double* ux, const double* uy,                 \
+                        const double* uz);                                           \
+  void P##sfinalize_geometry(void* h);                                               \
+  void P##sinitialize(void* h, double T0);                                           \
+  void P##sinitialize_field(void* h, const double* T_padded);                        \
+  void P##sstep(void* h, int n);                                                     \
+  void P##sadd_source(void* h, const double* dC);                                    \
+  void P##scompute_field(void* h);                                                   \
+  void P##sfield(void* h, double* T);                                                \
+  double P##stotal(void* h);                                                         \
+  void P##sgather(void* h, double* out);                                             \
+  long long P##sn_padded(void* h);                                                   \
+  long long P##stimestep(void* h);
+
 LBMO_DECLARE(lbmo_f64_)
 LBMO_DECLARE(lbmo_f32_)
+LBMO_DECLARE_SCALAR(lbmo_f64_)
+LBMO_DECLARE_SCALAR(lbmo_f32_)
 
 #endif

@@ -29,6 +29,11 @@ typedef struct {
   R *bc_rho, *wall_u0, *wall_un;  /* u0: 4 per node (ux, uy, uz, rho) */
   R wall_scale, wall_un_scale, outflow_rho;
   int wall_un_on, has_corners, fd_corners, force_bc, out_order, has_walls;
+  /* Boussinesq buoyancy (src/forcing/Forcing.hpp:93-127): per padded node
+   * F = f_uniform + g rho0 beta (T - T0) */
+  int buoyant;
+  R* temp;
+  R ufx, ufy, ufz, bgx, bgy, bgz, brho0, bbeta, bT0;
   R *rho, *ux, *uy, *uz; /* stored macroscopic fields (StoreMacro) */
 } S(solver);
 
@@ -562,6 +567,8 @@ void* F(create)(int lattice, int op, int eq, int shifted, int forcing, int quant
   s->n_padded = (long long)s->sx * s->sy * s->sz;
   s->omega = (R)omega; s->omega2 = (R)omega2;
   s->fx = (R)fx; s->fy = (R)fy; s->fz = (R)fz;
+  s->ufx = s->fx; s->ufy = s->fy; s->ufz = s->fz;
+  s->temp = (R*)calloc((size_t)s->n_padded, sizeof(R));
   s->f = (R*)calloc((size_t)s->n_padded * s->Q, sizeof(R));
   s->flags = (uint8_t*)calloc((size_t)s->n_padded, 1);
   s->spec_nrm = (uint8_t*)calloc((size_t)s->n_padded, 1);
@@ -593,7 +600,7 @@ void F(destroy)(void* h) {
   if (!s) return;
   free(s->f); free(s->flags); free(s->spec_nrm); free(s->spec_faces);
   free(s->bc_nrm); free(s->bc_ext); free(s->bc_onrm); free(s->bc_unk); free(s->bc_don);
-  free(s->bc_rho); free(s->wall_u0); free(s->wall_un); free(s->rho); free(s->ux); free(s->uy); free(s->uz);
+  free(s->bc_rho); free(s->wall_u0); free(s->wall_un); free(s->temp); free(s->rho); free(s->ux); free(s->uy); free(s->uz);
   free(s);
 }
 void F(set_geometry)(void* h, const uint8_t* fl) {           /* :74-82 */
@@ -776,6 +783,30 @@ int F(set_outflow_order)(void* h, int k) {                                      
   return 0;
 }
 void F(set_outflow_density)(void* h, double r) { ((S(solver)*)h)->outflow_rho = (R)r; }
+
+/* Boussinesq forcing (BoussinesqGuo, Forcing.hpp:93-127): T per interior
+ * node; NULL returns to the uniform force. */
+void F(set_buoyancy)(void* h, const double* T, double gx, double gy, double gz, double rho0,
+                     double beta, double T0) {
+  S(solver)* s = (S(solver)*)h;
+  s->buoyant = T != 0;
+  s->bgx = (R)gx; s->bgy = (R)gy; s->bgz = (R)gz;
+  s->brho0 = (R)rho0; s->bbeta = (R)beta; s->bT0 = (R)T0;
+  if (T)
+    for (int z = 0; z < s->nz; ++z)
+      for (int y = 0; y < s->ny; ++y)
+        for (int x = 0; x < s->nx; ++x)
+          s->temp[S(idi)(s, x, y, z)] = (R)T[((size_t)z * s->ny + y) * s->nx + x];
+  s->fx = s->ufx; s->fy = s->ufy; s->fz = s->ufz;
+}
+/* BoussinesqGuo::at(n): the force at node n (sets fx, fy, fz). */
+static inline void S(force_at)(S(solver)* s, long long n) {
+  if (!s->buoyant) return;
+  const R b = s->brho0 * s->bbeta * (s->temp[n] - s->bT0);
+  s->fx = s->ufx + s->bgx * b;
+  s->fy = s->ufy + s->bgy * b;
+  s->fz = s->ufz + s->bgz * b;
+}
 
 /* corner_density<P> (:664-712): closure density of every straight wall node,
  * then the corners extrapolated from two of them, at the parity the sweep
@@ -983,10 +1014,11 @@ void F(step)(void* h, int nsteps, int store_macro) {
     /* Regularised walls may read neighbour nodes inside the in-place sweep,
      * so with walls the sweep runs in index order, as the reference's
      * one-thread build runs it. */
-#pragma omp parallel for schedule(static) if (!s->has_walls)
+#pragma omp parallel for schedule(static) if (!s->has_walls && !s->buoyant)
     for (long long n = 0; n < s->n_padded; ++n) {
       const uint8_t fl = s->flags[n];
       if (fl != 0 && fl != 3 && fl != 4 && fl != 5) continue; /* Excluded / Solid skipped */
+      S(force_at)(s, n);
       long long nb[27];
       R f[27];
       S(neighbours)(s, n, nb);
@@ -1030,6 +1062,7 @@ void F(macro)(void* h, double* rho, double* ux, double* uy, double* uz) {
   for (long long n = 0; n < s->n_padded; ++n) {
     const uint8_t fl = s->flags[n];
     if (fl != 0 && fl != 3 && fl != 5) { s->rho[n] = s->ux[n] = s->uy[n] = s->uz[n] = (R)0; continue; }
+    S(force_at)(s, n);
     long long nb[27];
     R f[27];
     S(neighbours)(s, n, nb);
@@ -1122,6 +1155,7 @@ static double S(reduce)(S(solver)* s, int axis) {
   R sum = 0;
   for (long long n = 0; n < s->n_padded; ++n) {
     if (s->flags[n] != 0 && s->flags[n] != 3 && s->flags[n] != 5) continue;
+    S(force_at)(s, n);
     long long nb[27];
     R f[27];
     S(neighbours)(s, n, nb);

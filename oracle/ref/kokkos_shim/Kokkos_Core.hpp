@@ -16,6 +16,7 @@
 #include <cmath>
 #include <cstddef>
 #include <cstdint>
+#include <initializer_list>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -169,6 +170,43 @@ void parallel_reduce(const std::string&, const P& p, const F& f, R& result) {
 template <class P, class F, class R>
 void parallel_reduce(const P& p, const F& f, R& result) {
   parallel_reduce(std::string(), p, f, result);
+}
+
+// Two-dimensional ranges for reductions: rows (first index) split over
+// threads in static chunks, the second index fastest.
+template <unsigned N> struct Rank {};
+template <class RankT>
+struct MDRangePolicy {
+  std::int64_t b[2] = {0, 0}, e[2] = {0, 0};
+  MDRangePolicy(std::initializer_list<std::int64_t> lo, std::initializer_list<std::int64_t> hi) {
+    std::size_t k = 0;
+    for (auto v : lo) b[k++] = v;
+    k = 0;
+    for (auto v : hi) e[k++] = v;
+  }
+};
+template <class RankT, class F, class R>
+void parallel_reduce(const std::string&, const MDRangePolicy<RankT>& p, const F& f, R& result) {
+  int nt = 1;
+#ifdef _OPENMP
+  nt = omp_get_max_threads();
+#endif
+  std::vector<R> part(std::size_t(nt), R(0));
+#pragma omp parallel num_threads(nt)
+  {
+    int t = 0;
+#ifdef _OPENMP
+    t = omp_get_thread_num();
+#endif
+    R acc = R(0);
+#pragma omp for schedule(static)
+    for (std::int64_t i = p.b[0]; i < p.e[0]; ++i)
+      for (std::int64_t j = p.b[1]; j < p.e[1]; ++j) f(i, j, acc);
+    part[std::size_t(t)] = acc;
+  }
+  R s = R(0);
+  for (const R& v : part) s += v;
+  result = s;
 }
 
 inline void fence() {}

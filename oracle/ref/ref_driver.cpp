@@ -41,6 +41,10 @@ Base* make_D3Q27_TwoLattice_Guo_ShiftedPopulations(int, int, const Domain&, cons
 Base* make_D3Q27_TwoLattice_Guo_RawPopulations(int, int, const Domain&, const Params&);
 Base* make_D3Q27_TwoLattice_NoForcing_ShiftedPopulations(int, int, const Domain&, const Params&);
 Base* make_D3Q27_TwoLattice_NoForcing_RawPopulations(int, int, const Domain&, const Params&);
+Base* make_D2Q9_EsotericPull_BoussinesqGuo_ShiftedPopulations(int, int, const Domain&, const Params&);
+Base* make_D2Q9_EsotericPull_BoussinesqGuo_RawPopulations(int, int, const Domain&, const Params&);
+Base* make_D3Q27_EsotericPull_BoussinesqGuo_ShiftedPopulations(int, int, const Domain&, const Params&);
+Base* make_D3Q27_EsotericPull_BoussinesqGuo_RawPopulations(int, int, const Domain&, const Params&);
 
 static Base* make(int lattice, int streaming, int op, int eq, int shifted, int forcing,
                   const Domain& d, const Params& p) {
@@ -49,6 +53,15 @@ static Base* make(int lattice, int streaming, int op, int eq, int shifted, int f
                               : make_##LAT##_##STRM##_Guo_RawPopulations(op, eq, d, p);    \
   return shifted ? make_##LAT##_##STRM##_NoForcing_ShiftedPopulations(op, eq, d, p)        \
                  : make_##LAT##_##STRM##_NoForcing_RawPopulations(op, eq, d, p);
+  if (forcing == 2 && !streaming) {  // Boussinesq buoyancy (BoussinesqGuo)
+    if (lattice == 9)
+      return shifted ? make_D2Q9_EsotericPull_BoussinesqGuo_ShiftedPopulations(op, eq, d, p)
+                     : make_D2Q9_EsotericPull_BoussinesqGuo_RawPopulations(op, eq, d, p);
+    if (lattice == 27)
+      return shifted ? make_D3Q27_EsotericPull_BoussinesqGuo_ShiftedPopulations(op, eq, d, p)
+                     : make_D3Q27_EsotericPull_BoussinesqGuo_RawPopulations(op, eq, d, p);
+    return nullptr;
+  }
   if (lattice == 9) {
     if (streaming) { REF_PICK(D2Q9, TwoLattice) }
     REF_PICK(D2Q9, EsotericPull)
@@ -71,11 +84,12 @@ void ref_set_threads(int n) { omp_set_num_threads(n > 0 ? n : 1); }
 int ref_get_threads() { return omp_get_max_threads(); }
 
 // lattice: 9 (D2Q9) or 27 (D3Q27).  streaming: 0 EsotericPull, 1 TwoLattice.
+// forcing: 0 none, 1 uniform Guo, 2 BoussinesqGuo (Esoteric Pull only).
 void* ref_create(int lattice, int streaming, int op, int eq, int shifted, int forcing,
                  int nx, int ny, int nz, int px, int py, int pz, double omega,
                  double omega2, double fx, double fy, double fz) {
   const Domain d(nx, ny, nz, px != 0, py != 0, pz != 0);
-  refdrv::Params p{omega, omega2, fx, fy, fz};
+  refdrv::Params p{omega, omega2, fx, fy, fz, d.n_padded};
   if (op < 0 || op > 4) return nullptr;
   return refdrv::make(lattice, streaming, op, eq, shifted, forcing, d, p);
 }
@@ -124,6 +138,12 @@ int ref_set_outflow_order(void* h, int k) {
   return 0;
 }
 void ref_set_outflow_density(void* h, double r) { static_cast<refdrv::Base*>(h)->set_outflow_density(r); }
+// A solver made with forcing 2 (BoussinesqGuo): the temperature per interior
+// node and the buoyancy parameters; -1 for any other solver.
+int ref_set_buoyancy(void* h, const double* T, double gx, double gy, double gz, double rho0,
+                     double beta, double T0) {
+  return static_cast<refdrv::Base*>(h)->set_buoyancy(T, gx, gy, gz, rho0, beta, T0);
+}
 int ref_set_specular_nodes(void* h, const std::uint8_t* masks) {
   for (long long k = 0; k < ref_interior(h); ++k) {
     const unsigned m = masks[k];

@@ -59,7 +59,18 @@ struct NoCollision {
 
 struct Params {
   double omega = 1, omega2 = -1, fx = 0, fy = 0, fz = 0;
+  long long n_padded = 0;
 };
+
+// The forcing policy's parameters: the uniform Guo force, or the uniform part
+// of BoussinesqGuo with a temperature view of the lattice's size (zero until
+// ref_set_buoyancy fills it).
+inline void set_force(NoForcing&, const Params&) {}
+inline void set_force(Guo& g, const Params& p) { g = Guo{Real(p.fx), Real(p.fy), Real(p.fz)}; }
+inline void set_force(BoussinesqGuo& b, const Params& p) {
+  b.fx = Real(p.fx); b.fy = Real(p.fy); b.fz = Real(p.fz);
+  b.T = View1D<Real>("T", p.n_padded);
+}
 
 struct Base {
   virtual ~Base() = default;
@@ -79,6 +90,10 @@ struct Base {
   virtual void set_force_correction(bool on) = 0;
   virtual void set_outflow_order(int k) = 0;
   virtual void set_outflow_density(double r) = 0;
+  // BoussinesqGuo solvers only: T per interior node, buoyancy g rho0 beta (T - T0)
+  virtual int set_buoyancy(const double*, double, double, double, double, double, double) {
+    return -1;
+  }
   virtual long long nx() const = 0;
   virtual long long ny() const = 0;
   virtual void initialize(double rho, double ux, double uy, double uz) = 0;
@@ -102,19 +117,19 @@ template <class Coll> void apply_params(Coll& c, const Params& p);
 template <class L, class E, class F, class S>
 void apply_params(BGK<L, E, F, S>& c, const Params& p) {
   c.omega = Real(p.omega);
-  if constexpr (F::active) c.forcing = Guo{Real(p.fx), Real(p.fy), Real(p.fz)};
+  set_force(c.forcing, p);
 }
 template <class L, class E, class F, class S>
 void apply_params(TRT<L, E, F, S>& c, const Params& p) {
   c.omega_p = Real(p.omega);
   c.omega_m = Real(p.omega2);
-  if constexpr (F::active) c.forcing = Guo{Real(p.fx), Real(p.fy), Real(p.fz)};
+  set_force(c.forcing, p);
 }
 template <class L, class F, class S, bool C>
 void apply_params(MomentCollision<L, F, S, C>& c, const Params& p) {
   c.omega = Real(p.omega);
   c.omega_bulk = Real(p.omega2);
-  if constexpr (F::active) c.forcing = Guo{Real(p.fx), Real(p.fy), Real(p.fz)};
+  set_force(c.forcing, p);
 }
 template <class L>
 void apply_params(NoCollision<L>&, const Params&) {}
@@ -174,6 +189,21 @@ struct Impl final : Base {
   void set_force_correction(bool on) override { s.set_force_correction(on); }
   void set_outflow_order(int k) override { s.set_outflow_order(k); }
   void set_outflow_density(double r) override { s.set_outflow_density(Real(r)); }
+  int set_buoyancy(const double* T, double gx, double gy, double gz, double rho0, double beta,
+                   double T0) override {
+    if constexpr (requires(Coll& c) { c.forcing.T; c.forcing.beta; }) {
+      auto& f = s.collision().forcing;
+      f.gx = Real(gx); f.gy = Real(gy); f.gz = Real(gz);
+      f.rho0 = Real(rho0); f.beta = Real(beta); f.T0 = Real(T0);
+      for (Index z = 0; z < d.nz; ++z)
+        for (Index y = 0; y < d.ny; ++y)
+          for (Index x = 0; x < d.nx; ++x)
+            f.T(d.id(x, y, z)) = Real(T[(std::size_t(z) * d.ny + y) * d.nx + x]);
+      return 0;
+    } else {
+      return -1;
+    }
+  }
   long long nx() const override { return d.nx; }
   long long ny() const override { return d.ny; }
   void initialize(double rho, double ux, double uy, double uz) override {

@@ -239,6 +239,152 @@ def run_spec(backend, case, seed, quant=None):
     return out
 
 
+# Scalar lattice (src/solver/ScalarSolver.hpp).  name -> (lattice, op, shape,
+# kind, omega, steps, precision).
+SCALAR_CASES = {
+    "d3q7_bgk_walls_f64": (7, "bgk", (8, 7, 6), "walls", 1.3, 12, "f64"),
+    "d3q7_trt_outflow_f32": (7, "trt", (9, 6, 5), "outflow", 1.1, 10, "f32"),
+    "d2q5_regularised_moment_f64": (5, "regularised", (10, 9, 1), "moment", 1.5, 15, "f64"),
+    "d2q5_bgk_specular_f32": (5, "bgk", (10, 9, 1), "specular", 0.9, 15, "f32"),
+}
+SCALAR_PERIODIC = {"periodic": (True, True, True), "walls": (True, False, True),
+                   "moment": (True, False, True), "outflow": (False, True, True),
+                   "specular": (True, False, True)}
+
+
+def scalar_geometry(lattice, shape, kind):
+    """(cells, wall values, specular codes, specular masks) over the interior.
+
+    periodic: bulk everywhere;
+    walls   : Dirichlet floor (T = 1, anti-bounce-back) and adiabatic lid;
+    moment  : on-node Dirichlet (ScalarMoment) floor at T = 1 and lid at T = 0;
+    outflow : Dirichlet inlet column at x = 0, outflow column at x = nx-1;
+    specular: on-node mirror floor (set_specular_nodes) and lid
+              (set_specular_walls), a Dirichlet node in the middle."""
+    nx, ny, nz = shape
+    cells = np.zeros((nz, ny, nx), np.uint8)
+    tw = np.zeros((nz, ny, nx))
+    codes = np.zeros_like(cells)
+    masks = np.zeros_like(cells)
+    if kind == "walls":
+        cells[:, 0, :] = 2
+        tw[:, 0, :] = 1.0
+        cells[:, -1, :] = 1
+    elif kind == "moment":
+        cells[:, 0, :] = 4
+        tw[:, 0, :] = 1.0
+        cells[:, -1, :] = 4
+    elif kind == "outflow":
+        cells[:, :, 0] = 2
+        tw[:, :, 0] = 1.0
+        cells[:, :, -1] = 5
+    elif kind == "specular":
+        cells[:, 0, :] = 6
+        masks[:, 0, :] = 0x08
+        cells[:, -1, :] = 6
+        codes[:, -1, :] = 3
+        cells[nz // 2, ny // 2, nx // 2] = 2
+        tw[nz // 2, ny // 2, nx // 2] = 2.0
+    elif kind != "periodic":
+        raise ValueError(kind)
+    return cells, tw, codes, masks
+
+
+def scalar_fields(shape, lattice, seed):
+    """Seeded temperature (per padded node) and advecting velocity (interior)."""
+    nx, ny, nz = shape
+    rng = np.random.default_rng(seed)
+    u = [0.04 * rng.standard_normal((nz, ny, nx)) for _ in range(3)]
+    if lattice == 5:
+        u[2][:] = 0.0
+    return rng, [np.asarray(a, np.float32).astype(np.float64) for a in u]
+
+
+def run_scalar(backend, case, seed, T_ref=0.0, omega_field=False, source=False):
+    lat, op, shape, kind, om, steps, prec = case
+    nx, ny, nz = shape
+    per = SCALAR_PERIODIC[kind]
+    s = O.ScalarCpuSolver(backend, lattice=lat, op=op, nx=nx, ny=ny, nz=nz, px=per[0],
+                          py=per[1], pz=per[2], omega=om, T_ref=T_ref, precision=prec)
+    cells, tw, codes, masks = scalar_geometry(lat, shape, kind)
+    s.set_geometry(cells)
+    s.set_wall_values(tw)
+    if codes.any():
+        s.set_specular_walls(codes)
+    if masks.any():
+        s.set_specular_nodes(masks)
+    s.finalize_geometry()
+    rng, u = scalar_fields(shape, lat, seed)
+    s.set_velocity(*u)
+    if omega_field:
+        s.set_omega_field(np.asarray(om + 0.3 * rng.random((nz, ny, nx)), np.float32).astype(np.float64))
+    T = np.asarray(0.5 + 0.2 * rng.standard_normal(s.n_padded), np.float32).astype(np.float64)
+    s.initialize_field(T)
+    f0 = s.field()
+    dC = np.asarray(1e-3 * rng.standard_normal((nz, ny, nx)), np.float32).astype(np.float64)
+    for t in range(steps):
+        if source and t % 3 == 0:
+            s.add_source(dC)
+        s.step()
+    stored = s.field()
+    s.compute_field()
+    out = {"field0": f0, "stored": stored, "field": s.field(), "total": s.total()}
+    s.close()
+    return out
+
+
+# Thermal coupling: fluid (Boussinesq buoyancy, BoussinesqGuo) and scalar
+# advected by the fluid, in the reference's loop order (fluid step storing u,
+# then scalar step; validation/rayleigh_benard.cpp:178-188).  name ->
+# (fluid lattice, fluid op, scalar lattice, scalar op, shape, steps, precision).
+COUPLED_CASES = {
+    "d2q9_bgk_d2q5_convection_f64": (9, "bgk", 5, "bgk", (12, 9, 1), 30, "f64"),
+    "d3q27_cm_d3q7_convection_f32": (27, "cm", 7, "trt", (8, 7, 6), 20, "f32"),
+}
+
+
+def run_coupled(backend, case, seed):
+    """Heated floor (T = 1) and cooled lid (T = 0) as scalar Dirichlet rows on
+    the fluid's solid rows; periodic x (and z); buoyancy along +y."""
+    flat, fop, slat, sop, shape, steps, prec = case
+    nx, ny, nz = shape
+    fl_kw = dict(lattice=flat, op=fop, shifted=1, nx=nx, ny=ny, nz=nz, px=True, py=False, pz=True,
+                 omega=1.4, omega2=(1.1 if fop == "trt" else -1.0), precision=prec)
+    fl = O.CpuSolver(backend, forcing=(2 if backend == "ref" else 1), **fl_kw)
+    th = O.ScalarCpuSolver(backend, lattice=slat, op=sop, nx=nx, ny=ny, nz=nz, px=True, py=False,
+                           pz=True, omega=1.2, precision=prec)
+    flags = np.zeros((nz, ny, nx), np.uint8)
+    flags[:, 0, :] = 1
+    flags[:, -1, :] = 1
+    fl.set_geometry(flags)
+    cells = np.zeros((nz, ny, nx), np.uint8)
+    tw = np.zeros((nz, ny, nx))
+    cells[:, 0, :] = 2
+    tw[:, 0, :] = 1.0
+    cells[:, -1, :] = 2
+    th.set_geometry(cells)
+    th.set_wall_values(tw)
+    th.finalize_geometry()
+    rng = np.random.default_rng(seed)
+    T = np.asarray(0.5 + 0.05 * rng.standard_normal(th.n_padded), np.float32).astype(np.float64)
+    th.initialize_field(T)
+    fl.initialize(1.0)
+    g = (0.0, 1.0, 0.0)
+    for _ in range(steps):
+        fl.set_buoyancy(th.field(), g=g, rho0=1.0, beta=5e-3, T0=0.5)
+        fl.step(1, store_macro=True)
+        _, ux, uy, uz = fl.stored_macro()
+        th.set_velocity(ux, uy, uz)
+        th.step()
+    stored_T = th.field()
+    th.compute_field()
+    out = {"pops": fl.gather(), "stored": np.stack(fl.stored_macro()), "macro": np.stack(fl.macro()),
+           "T_stored": stored_T, "T": th.field(), "mass": fl.total_mass(), "total": th.total()}
+    fl.close()
+    th.close()
+    return out
+
+
 def main():
     if not O.ref_available("f64"):
         raise SystemExit("reference build missing: make -C oracle ref")
@@ -251,6 +397,14 @@ def main():
     for k, (name, case) in enumerate(SPEC_CASES.items()):
         r = run_spec("ref", case, seed=200 + k)
         np.savez_compressed(HERE / f"{name}.npz", case=np.array(repr(case)), seed=200 + k, **r)
+        print(name, "mass", r["mass"])
+    for k, (name, case) in enumerate(SCALAR_CASES.items()):
+        r = run_scalar("ref", case, seed=400 + k, T_ref=0.25, omega_field=k % 2 == 1, source=True)
+        np.savez_compressed(HERE / f"{name}.npz", case=np.array(repr(case)), seed=400 + k, **r)
+        print(name, "total", r["total"])
+    for k, (name, case) in enumerate(COUPLED_CASES.items()):
+        r = run_coupled("ref", case, seed=500 + k)
+        np.savez_compressed(HERE / f"{name}.npz", case=np.array(repr(case)), seed=500 + k, **r)
         print(name, "mass", r["mass"])
     for k, (name, case) in enumerate(WALL_CASES.items()):
         r = run_wall("ref", case, seed=300 + k)

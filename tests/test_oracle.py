@@ -380,3 +380,104 @@ def test_oracle_couette_between_regularized_walls_is_exact():
     ux = s.macro()[1][0, :, 0]
     np.testing.assert_allclose(ux, U * np.arange(ny) / (ny - 1), rtol=0, atol=1e-10)
     s.close()
+
+
+# ------------------------------------------------ scalar lattice and coupling
+@pytest.mark.parametrize("name", list(G.SCALAR_CASES))
+def test_oracle_reproduces_scalar_golden(name):
+    """D2Q5 / D3Q7 fixtures made by the reference's ScalarSolver."""
+    d = np.load(GOLDEN / f"{name}.npz")
+    k = list(G.SCALAR_CASES).index(name)
+    r = G.run_scalar("oracle", G.SCALAR_CASES[name], int(d["seed"]), T_ref=0.25,
+                     omega_field=k % 2 == 1, source=True)
+    for key in ("field0", "stored", "field"):
+        np.testing.assert_array_equal(r[key], d[key], err_msg=key)
+    assert r["total"] == float(d["total"])
+
+
+@needs_ref
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+@pytest.mark.parametrize("kind", list(G.SCALAR_PERIODIC))
+def test_oracle_scalar_bit_identical_to_reference(prec, kind):
+    """Every scalar operator on both lattices, every cell type, with and
+    without a storage reference T_ref, per-node rates and sources."""
+    O.set_ref_threads(1, prec)
+    for lat, op, tref, omf, src in itertools.product([5, 7], ["bgk", "trt", "regularised"],
+                                                    [0.0, 0.5], [False, True], [False, True]):
+        shape = (10, 9, 1) if lat == 5 else (8, 7, 5)
+        case = (lat, op, shape, kind, 1.2, 9, prec)
+        a = G.run_scalar("oracle", case, 3, T_ref=tref, omega_field=omf, source=src)
+        b = G.run_scalar("ref", case, 3, T_ref=tref, omega_field=omf, source=src)
+        for k in a:
+            np.testing.assert_array_equal(a[k], b[k], err_msg=f"{case} {tref} {omf} {src} {k}")
+
+
+@pytest.mark.parametrize("name", list(G.COUPLED_CASES))
+def test_oracle_reproduces_coupled_golden(name):
+    """Fluid with Boussinesq buoyancy + scalar advected by the fluid: fixtures
+    made by the reference's FluidSolver<..., BoussinesqGuo> and ScalarSolver."""
+    d = np.load(GOLDEN / f"{name}.npz")
+    r = G.run_coupled("oracle", G.COUPLED_CASES[name], int(d["seed"]))
+    for key in ("pops", "stored", "macro", "T_stored", "T"):
+        np.testing.assert_array_equal(r[key], d[key], err_msg=key)
+    assert r["mass"] == float(d["mass"]) and r["total"] == float(d["total"])
+
+
+@needs_ref
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_oracle_buoyancy_bit_identical_to_reference(prec):
+    """The per-node Boussinesq force on every fluid operator, with and without
+    walls, against BoussinesqGuo in the reference build."""
+    O.set_ref_threads(1, prec)
+    for lat, (op, eq, om2), shifted, walls in itertools.product(
+            [9, 27], [("bgk", 0, -1.0), ("bgk", 1, -1.0), ("trt", 0, 1.1), ("mrt", 0, 1.5),
+                      ("cm", 0, -1.0)], [1, 0], [0, 1]):
+        nx, ny, nz = (10, 9, 1) if lat == 9 else (8, 7, 5)
+        kw = dict(lattice=lat, op=op, eq=eq, shifted=shifted, nx=nx, ny=ny, nz=nz, px=True,
+                  py=not walls, pz=True, omega=1.3, omega2=om2, fx=1e-5, fy=0.0,
+                  fz=2e-6 if lat == 27 else 0.0, precision=prec)
+        a = O.CpuSolver("oracle", forcing=1, **kw)
+        b = O.CpuSolver("ref", forcing=2, **kw)
+        rng = np.random.default_rng(4)
+        sh = (nz, ny, nx)
+        fl = np.zeros(sh, np.uint8)
+        if walls:
+            fl[:, 0, :] = 1
+            fl[:, -1, :] = 1
+        fields = [np.asarray(x, np.float32).astype(np.float64) for x in
+                  [1 + 0.01 * rng.standard_normal(sh)] + [0.03 * rng.standard_normal(sh) for _ in range(3)]]
+        if lat == 9:
+            fields[3][:] = 0
+        for s in (a, b):
+            s.set_geometry(fl)
+            s.initialize_field(*fields)
+        for _ in range(6):
+            T = np.asarray(0.3 * rng.standard_normal(sh), np.float32).astype(np.float64)
+            for s in (a, b):
+                s.set_buoyancy(T, g=(0.0, 1.0, 0.5 if lat == 27 else 0.0), rho0=1.0, beta=2e-4, T0=0.1)
+                s.step(1, store_macro=True)
+        np.testing.assert_array_equal(a.gather(), b.gather())
+        for x, y in zip(a.stored_macro() + a.macro(), b.stored_macro() + b.macro()):
+            np.testing.assert_array_equal(x, y)
+        assert a.total_mass() == b.total_mass()
+        a.close()
+        b.close()
+
+
+def test_oracle_scalar_diffusion_rate():
+    """A sinusoid decays at D k^2 with D = cs2 (1/omega - 1/2) (ScalarBGK.hpp:20-27,
+    validation/thermal.cpp): cs2 = 1/3 on D2Q5, 1/4 on D3Q7."""
+    for lat, cs2 in ((5, 1 / 3), (7, 1 / 4)):
+        N, om, steps = 64, 1.2, 400
+        nz = 1 if lat == 5 else 4
+        s = O.ScalarCpuSolver("oracle", lattice=lat, op="bgk", nx=N, ny=4, nz=nz, omega=om)
+        x = np.arange(N)
+        T = np.broadcast_to(0.01 * np.sin(2 * np.pi * x / N), (nz, 4, N)).ravel()
+        s.initialize_field(T)
+        s.step(steps)
+        s.compute_field()
+        amp = s.field()[0, 0] @ np.sin(2 * np.pi * x / N) * 2 / N
+        D = cs2 * (1 / om - 0.5)
+        k = 2 * np.pi / N
+        assert abs(amp / 0.01 / np.exp(-D * k * k * steps) - 1) < 1e-3
+        s.close()
