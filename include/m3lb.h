@@ -179,6 +179,22 @@ int m3lb_set_outflow_order(m3lb_solver* h, int order);
 /* set_outflow_density (:1330): target density of arbitrary-face outflows. */
 int m3lb_set_outflow_density(m3lb_solver* h, double rho);
 
+/* Boussinesq buoyancy (BoussinesqGuo, src/forcing/Forcing.hpp:93-127): the
+ * body force at a node becomes (fx, fy, fz) + g rho0 beta (T - T0), with
+ * (fx, fy, fz) from m3lb_set_params, g = (gx, gy, gz) the direction a warmer
+ * parcel is pushed, and T a device array of one value per interior node (x
+ * fastest) in the solver's arithmetic type (FP64 for FP64 storage, else
+ * FP32), read at every step; NULL returns to the uniform force.  Needs a
+ * solver created with forcing.  While it is set the step runs in the paired
+ * or the one-node kernel. */
+int m3lb_set_buoyancy(m3lb_solver* h, const void* T, double gx, double gy, double gz, double rho0,
+                      double beta, double T0);
+/* Device arrays of the stored rho and u (written by m3lb_step with
+ * store_macro and by m3lb_macro_device), without computing them. */
+int m3lb_macro_pointers(const m3lb_solver* h, void** rho, void** ux, void** uy, void** uz);
+/* The CUDA stream the handle queues its work on. */
+int m3lb_get_stream(const m3lb_solver* h, void** stream);
+
 /* initialize(rho0, ux, uy, uz) (:553-561): equilibrium on fluid nodes, rest
  * equilibrium at rho0 elsewhere; resets the time step to 0. */
 int m3lb_init_eq(m3lb_solver* h, double rho0, double ux, double uy, double uz);
@@ -255,6 +271,74 @@ int m3lb_reduce_static(int lattice, int nx, int ny, int nz, int px, int py, int 
                        int storage, int shifted, int forcing, double fx, double fy, double fz,
                        const void* populations, const uint8_t* flags, long long timestep,
                        void* stream, double* out);
+
+/* ------------------------------------------------------------ scalar lattice
+ * ScalarSolver<L, EsotericPull<L>, Collision> (src/solver/ScalarSolver.hpp):
+ * an advection-diffusion lattice, D2Q5 (lattice 5, nz = 1) or D3Q7 (7),
+ * stored in FP32 or FP64, with the collision operators ScalarBGK,
+ * ScalarTRT and ScalarRegularised (src/collision/Scalar*.hpp).  Cell types
+ * per interior node (ScalarBGK.hpp ScalarCell): 0 bulk, 1 adiabatic (zero
+ * flux), 2 Dirichlet (anti-bounce-back to the wall value), 3 excluded,
+ * 4 moment (the wall value imposed ON the node, MomentDirichlet.hpp), 5
+ * outflow (equilibrium at a bulk donor's value), 6 specular (on-node zero
+ * flux, with faces from the two specular calls). */
+typedef struct m3lb_scalar m3lb_scalar;
+
+#define M3LB_SOP_BGK 1
+#define M3LB_SOP_TRT 2
+#define M3LB_SOP_REGULARISED 3
+
+int m3lb_scalar_create(int lattice, int nx, int ny, int nz, int px, int py, int pz, int op,
+                       int storage, m3lb_scalar** out);
+int m3lb_scalar_destroy(m3lb_scalar* h);
+/* ScalarBGK::omega, T_ref (the storage reference, 0 = raw), ScalarTRT::Lambda. */
+int m3lb_scalar_set_params(m3lb_scalar* h, double omega, double T_ref, double Lambda);
+int m3lb_scalar_set_stream(m3lb_scalar* h, void* stream);
+/* set_geometry(fn -> ScalarCell) (:92-99): cell types 0..6 per interior node. */
+int m3lb_scalar_set_cells(m3lb_scalar* h, const uint8_t* cells);
+/* set_wall_values (:101-108): the value Dirichlet and moment cells impose. */
+int m3lb_scalar_set_wall_values(m3lb_scalar* h, const double* values);
+/* set_specular_walls (:113-132, codes 1..6) / set_specular_nodes (:140-164,
+ * face masks): the faces of specular cells. */
+int m3lb_scalar_set_specular_walls(m3lb_scalar* h, const uint8_t* normal_codes);
+int m3lb_scalar_set_specular_nodes(m3lb_scalar* h, const uint8_t* face_masks);
+/* ScalarBGK::omega_of: a relaxation rate per interior node (NULL: uniform). */
+int m3lb_scalar_set_omega_field(m3lb_scalar* h, const double* omega);
+/* set_velocity (:166-168): device arrays of the advecting velocity per
+ * interior node in the arithmetic type, read at every step (NULL: at rest). */
+int m3lb_scalar_set_velocity_device(m3lb_scalar* h, const void* ux, const void* uy, const void* uz);
+/* finalize_geometry (:223-296): moment-cell unknowns and outflow donors. */
+int m3lb_scalar_finalize_geometry(m3lb_scalar* h);
+/* initialize(T0) / initialize_field(fn(n)) (:170-190); the field is given
+ * per PADDED node (n_padded values, x fastest). */
+int m3lb_scalar_init(m3lb_scalar* h, double T0);
+int m3lb_scalar_init_field(m3lb_scalar* h, const double* T_padded);
+/* step() (:192-203): the lattice step, then the outflow pass. */
+int m3lb_scalar_step(m3lb_scalar* h, int nsteps);
+/* add_source(fn(n)) (:205-208, 421-437): dC per interior node. */
+int m3lb_scalar_add_source(m3lb_scalar* h, const double* dC);
+int m3lb_scalar_add_source_device(m3lb_scalar* h, const void* dC);
+/* compute_field() (:210-212), then temperature(): the field per interior
+ * node on the host, or its device array. */
+int m3lb_scalar_compute_field(m3lb_scalar* h);
+int m3lb_scalar_field(m3lb_scalar* h, double* T);
+int m3lb_scalar_field_device(m3lb_scalar* h, void** T);
+/* total_population() (:219-228), summed in FP64. */
+int m3lb_scalar_total(m3lb_scalar* h, double* out);
+/* Logical populations per padded node (n_padded x Q doubles). */
+int m3lb_scalar_gather(m3lb_scalar* h, double* out);
+int m3lb_scalar_info(const m3lb_scalar* h, long long* n_padded, long long* timestep,
+                     long long* launches);
+int m3lb_scalar_sync(m3lb_scalar* h);
+/* Two-way thermal coupling of lattices of the same extent and arithmetic
+ * type, as the reference's drivers wire it (force.T = th.temperature();
+ * th.set_velocity(fl.ux(), fl.uy(), fl.uz()), validation/rayleigh_benard.cpp):
+ * the fluid's Boussinesq force reads the scalar's field, the scalar is
+ * advected by the fluid's stored velocity (store_macro), and the scalar's
+ * work goes onto the fluid's stream so the two alternate in order.  Destroy
+ * the scalar before the fluid, or give it another stream first. */
+int m3lb_couple_thermal(m3lb_solver* fluid, m3lb_scalar* scalar, double gx, double gy, double gz,
+                        double rho0, double beta, double T0);
 
 /* ------------------------------------------------------------ serving loop
  * Many independent lattices resident on one GPU and advanced together (no

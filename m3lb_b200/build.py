@@ -47,6 +47,7 @@ def _units():
     units.append((CSRC / "lbm_noalloc.cu", BUILD / "noalloc.o", []))
     units.append((CSRC / "lbm_serve.cu", BUILD / "serve.o", []))
     units.append((CSRC / "lbm_walls.cu", BUILD / "walls.o", []))
+    units.append((CSRC / "lbm_scalar.cu", BUILD / "scalar.o", []))
     return units
 
 
@@ -64,7 +65,8 @@ def up_to_date() -> bool:
         return False
     t = LIB.stat().st_mtime
     srcs = [CSRC / "lbm_inst.cu", CSRC / "lbm_capi.cu", CSRC / "lbm_noalloc.cu",
-            CSRC / "lbm_serve.cu", CSRC / "lbm_walls.cu", CSRC / "lbm_host.h",
+            CSRC / "lbm_serve.cu", CSRC / "lbm_walls.cu", CSRC / "lbm_scalar.cu",
+            CSRC / "lbm_host.h",
             *[CSRC / h for h in HEADERS],
             PKG.parent / "include" / "m3lb.h"]
     return all(p.stat().st_mtime <= t for p in srcs if p.exists())

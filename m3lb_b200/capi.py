@@ -87,6 +87,33 @@ SIGNATURES = {
     "m3lb_set_force_correction": (_i, [_vp, _i]),
     "m3lb_set_outflow_order": (_i, [_vp, _i]),
     "m3lb_set_outflow_density": (_i, [_vp, _d]),
+    "m3lb_set_buoyancy": (_i, [_vp, _vp] + [_d] * 6),
+    "m3lb_macro_pointers": (_i, [_vp] + [_pp] * 4),
+    "m3lb_get_stream": (_i, [_vp, _pp]),
+    "m3lb_scalar_create": (_i, [_i] * 9 + [_pp]),
+    "m3lb_scalar_destroy": (_i, [_vp]),
+    "m3lb_scalar_set_params": (_i, [_vp] + [_d] * 3),
+    "m3lb_scalar_set_stream": (_i, [_vp, _vp]),
+    "m3lb_scalar_set_cells": (_i, [_vp, _vp]),
+    "m3lb_scalar_set_wall_values": (_i, [_vp, _vp]),
+    "m3lb_scalar_set_specular_walls": (_i, [_vp, _vp]),
+    "m3lb_scalar_set_specular_nodes": (_i, [_vp, _vp]),
+    "m3lb_scalar_set_omega_field": (_i, [_vp, _vp]),
+    "m3lb_scalar_set_velocity_device": (_i, [_vp] * 4),
+    "m3lb_scalar_finalize_geometry": (_i, [_vp]),
+    "m3lb_scalar_init": (_i, [_vp, _d]),
+    "m3lb_scalar_init_field": (_i, [_vp, _vp]),
+    "m3lb_scalar_step": (_i, [_vp, _i]),
+    "m3lb_scalar_add_source": (_i, [_vp, _vp]),
+    "m3lb_scalar_add_source_device": (_i, [_vp, _vp]),
+    "m3lb_scalar_compute_field": (_i, [_vp]),
+    "m3lb_scalar_field": (_i, [_vp, _vp]),
+    "m3lb_scalar_field_device": (_i, [_vp, _pp]),
+    "m3lb_scalar_total": (_i, [_vp, C.POINTER(C.c_double)]),
+    "m3lb_scalar_gather": (_i, [_vp, _vp]),
+    "m3lb_scalar_info": (_i, [_vp] + [C.POINTER(C.c_longlong)] * 3),
+    "m3lb_scalar_sync": (_i, [_vp]),
+    "m3lb_couple_thermal": (_i, [_vp, _vp] + [_d] * 6),
     "m3lb_init_eq": (_i, [_vp] + [_d] * 4),
     "m3lb_init_field_f32": (_i, [_vp] + [_vp] * 4),
     "m3lb_init_field_f64": (_i, [_vp] + [_vp] * 4),

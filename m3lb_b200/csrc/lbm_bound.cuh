@@ -33,6 +33,13 @@ __device__ __forceinline__ void padded_coords(const Geo& g, long long n, int& x,
   z = (int)(n / ((long long)g.sx * g.sy));
 }
 
+// Interior index (x fastest) of a padded node.
+__device__ __forceinline__ size_t interior_index(const Geo& g, long long n) {
+  int x, y, z;
+  padded_coords(g, n, x, y, z);
+  return ((size_t)(z - g.hz) * g.ny + (y - g.hy)) * g.nx + (x - g.hx);
+}
+
 // The Q populations about to arrive at node n (Access::load_pair, parity P).
 template <class L, int ST, class R>
 __device__ __forceinline__ void load_pops(const StepArgs& a, long long n, R* f) {
@@ -261,7 +268,10 @@ __device__ __forceinline__ bool regwall(const StepArgs& a, const BoundArgs& b, i
   wall_velocity(b, nd, uw);
   // has_forcing looks for a ForcingPolicy member type, which only BGK declares
   R Fv[3] = {0, 0, 0};
-  if constexpr (FORCE && OP == 1) { Fv[0] = R(a.fx); Fv[1] = R(a.fy); Fv[2] = R(a.fz); }
+  if constexpr (FORCE && OP == 1) {
+    const CollideParams<R> fp = node_params<FORCE, R>(a, interior_index(a.g, nd.n));
+    Fv[0] = fp.fx; Fv[1] = fp.fy; Fv[2] = fp.fz;
+  }
   R ur[3] = {uw[0], uw[1], uw[2]};
   R rw;
   if (code == kNrmOutFree) {                             // donor rescaled to the target density
@@ -420,14 +430,10 @@ __global__ void __launch_bounds__(kBndThreads) bnd_step(StepArgs a, BoundArgs b)
   }
   if (nd.type == kSpecNode) spec_node_mirror<L>(f, nd.code);
   else if (regwall<L, ST, OP, EQ, SH, FORCE>(a, b, i, f)) return;
-  const CollideParams<R> prm{(R)a.omega, (R)a.omega2, (R)a.fx, (R)a.fy, (R)a.fz};
-  const Macro<R> mc = collide<L, OP, EQ, SH, FORCE>(f, prm);
+  const size_t k = interior_index(a.g, nd.n);
+  const Macro<R> mc = collide<L, OP, EQ, SH, FORCE>(f, node_params<FORCE, R>(a, k));
   store_pops<L, ST>(a, nd.n, f);
   if (a.rho) {
-    const Geo& g = a.g;
-    int x, y, z;
-    padded_coords(g, nd.n, x, y, z);
-    const size_t k = ((size_t)(z - g.hz) * g.ny + (y - g.hy)) * g.nx + (x - g.hx);
     reinterpret_cast<R*>(a.rho)[k] = mc.rho;
     reinterpret_cast<R*>(a.ux)[k] = mc.ux;
     reinterpret_cast<R*>(a.uy)[k] = mc.uy;

@@ -123,6 +123,9 @@ struct m3lb_solver {
   bool has_geometry = false;
   // wall nodes (regularised and free-slip) and their device list
   WallSet walls;
+  // Boussinesq buoyancy: temperature per interior node (arithmetic type)
+  const void* temp = nullptr;
+  double bg[3] = {0, 0, 0}, brho0 = 1, bbeta = 1, bT0 = 0;
   void* macro[4] = {nullptr, nullptr, nullptr, nullptr};  // interior, arithmetic type
   void* staging = nullptr;           // init_field uploads (4 interior arrays)
   double* partials = nullptr;        // reduction scratch
@@ -147,6 +150,11 @@ struct m3lb_solver {
     a.omega = omega; a.omega2 = omega2;
     a.fx = forcing ? fx : 0; a.fy = forcing ? fy : 0; a.fz = forcing ? fz : 0;
     a.err = err;
+    if (forcing && temp) {
+      a.temp = temp;
+      a.bgx = bg[0]; a.bgy = bg[1]; a.bgz = bg[2];
+      a.brho0 = brho0; a.bbeta = bbeta; a.bT0 = bT0;
+    }
     return a;
   }
   // The chunk kernels need a periodic x axis (no x halo) and even nx; the
@@ -154,6 +162,8 @@ struct m3lb_solver {
   bool chunk_ok() const { return g.px && g.hx == 0 && (g.nx % 2) == 0; }
   int step_kernel() const {
     if (node_kernel || !chunk_ok() || kernel == M3LB_KERNEL_NODES) return kKernelNodes;
+    // a per-node (Boussinesq) force runs in the paired kernel
+    if (forcing && temp) return kKernelPairs;
     // the streamed kernel addresses rows with 32-bit element counts
     const bool rows32 = (long long)g.nch * Q * 64 < (1LL << 31);
     // the row kernel: whole rows of at most 8 full chunks
@@ -424,6 +434,29 @@ int m3lb_set_outflow_order(m3lb_solver* h, int order) {
   }
   h->walls.out_order = order;
   return rebuild_walls(h);
+}
+int m3lb_set_buoyancy(m3lb_solver* h, const void* T, double gx, double gy, double gz, double rho0,
+                      double beta, double T0) {
+  if (!h) return fail(M3LB_ERR_INVALID, "set_buoyancy: null handle");
+  if (T && !h->forcing)
+    return fail(M3LB_ERR_INVALID, "set_buoyancy: the solver was created without forcing");
+  h->temp = T;
+  h->bg[0] = gx; h->bg[1] = gy; h->bg[2] = gz;
+  h->brho0 = rho0; h->bbeta = beta; h->bT0 = T0;
+  return M3LB_OK;
+}
+int m3lb_macro_pointers(const m3lb_solver* h, void** rho, void** ux, void** uy, void** uz) {
+  if (!h) return fail(M3LB_ERR_INVALID, "macro_pointers: null handle");
+  if (rho) *rho = h->macro[0];
+  if (ux) *ux = h->macro[1];
+  if (uy) *uy = h->macro[2];
+  if (uz) *uz = h->macro[3];
+  return M3LB_OK;
+}
+int m3lb_get_stream(const m3lb_solver* h, void** stream) {
+  if (!h || !stream) return fail(M3LB_ERR_INVALID, "get_stream: null argument");
+  *stream = (void*)h->stream;
+  return M3LB_OK;
 }
 int m3lb_set_outflow_density(m3lb_solver* h, double rho) {
   if (!h) return fail(M3LB_ERR_INVALID, "set_outflow_density: null handle");

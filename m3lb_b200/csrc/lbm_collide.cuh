@@ -40,10 +40,17 @@ __device__ __forceinline__ void static_for(Fn&& fn) {
   }
 }
 
-template <class S>
+template <class S, class FV = S>
 struct CollideParams {
-  S omega, omega2, fx, fy, fz;
+  S omega, omega2;
+  FV fx, fy, fz;  // the body force: one value for the lattice, or one per node of a pair
 };
+// The force as the arithmetic type V: broadcast when it is one value.
+template <class V, class FV>
+__device__ __forceinline__ V fvec(FV x) {
+  if constexpr (std::is_same_v<V, FV>) return x;
+  else return bc<V>(x);
+}
 
 // Macroscopic state of one node (or node pair).
 template <class V>
@@ -110,9 +117,9 @@ __device__ __forceinline__ void pair_sums(const V* f, V& dens, V& mx, V& my, V& 
 
 // rho, u from (dens, momentum), with Guo's half-force velocity shift
 // u += F / (2 rho) (Forcing.hpp:66-70).
-template <bool SH, bool FORCE, class V, class S>
+template <bool SH, bool FORCE, class V, class S, class FV>
 __device__ __forceinline__ Macro<V> finish_macro(V dens, V mx, V my, V mz,
-                                                 const CollideParams<S>& p) {
+                                                 const CollideParams<S, FV>& p) {
   Macro<V> m;
   m.dens = dens;
   m.rho = SH ? add(bc<V>(S(1)), dens) : dens;
@@ -122,9 +129,9 @@ __device__ __forceinline__ Macro<V> finish_macro(V dens, V mx, V my, V mz,
   m.uz = mul(mz, ir);
   if constexpr (FORCE) {
     const V h = mul(bc<V>(S(0.5)), ir);
-    m.ux = fma(h, bc<V>(p.fx), m.ux);
-    m.uy = fma(h, bc<V>(p.fy), m.uy);
-    m.uz = fma(h, bc<V>(p.fz), m.uz);
+    m.ux = fma(h, fvec<V>(p.fx), m.ux);
+    m.uy = fma(h, fvec<V>(p.fy), m.uy);
+    m.uz = fma(h, fvec<V>(p.fz), m.uz);
   }
   return m;
 }
@@ -165,9 +172,9 @@ __device__ __forceinline__ V phi_product(const V* dx, const V* dy, const V* dz) 
 // Second-order phi of a pair (c, -c): A +- B with A = 4.5 (c.u)^2 - 1.5 u.u,
 // B = 3 c.u (Equilibrium.hpp:49-60).  Guo source of a pair: sym +- anti with
 // sym = w (9 (c.u)(c.F) - 3 u.F), anti = 3 w c.F (Forcing.hpp:26-38).
-template <class L, int OP, int EQ, bool SH, bool FORCE, class V, class S>
+template <class L, int OP, int EQ, bool SH, bool FORCE, class V, class S, class FV>
 __device__ __forceinline__ void collide_bgk_trt(V* f, const Macro<V>& m,
-                                                const CollideParams<S>& p) {
+                                                const CollideParams<S, FV>& p) {
   const V om = bc<V>(p.omega);
   const V D0 = SH ? m.dens : m.rho;
   const V uu = fma(m.uz, m.uz, fma(m.uy, m.uy, mul(m.ux, m.ux)));
@@ -175,7 +182,7 @@ __device__ __forceinline__ void collide_bgk_trt(V* f, const Macro<V>& m,
   V m3uF = bc<V>(0);
   if constexpr (FORCE)
     m3uF = mul(bc<V>(S(-3)),
-               fma(m.uz, bc<V>(p.fz), fma(m.uy, bc<V>(p.fy), mul(m.ux, bc<V>(p.fx)))));
+               fma(m.uz, fvec<V>(p.fz), fma(m.uy, fvec<V>(p.fy), mul(m.ux, fvec<V>(p.fx)))));
   V dx[3], dy[3], dz[3];
   if constexpr (EQ == 1) {
     chi_deltas<V, S>(m.ux, dx);
@@ -217,7 +224,7 @@ __device__ __forceinline__ void collide_bgk_trt(V* f, const Macro<V>& m,
     }
     V ssym = bc<V>(0), santi = bc<V>(0);
     if constexpr (FORCE) {
-      const V cF = cdot<L, i>(bc<V>(p.fx), bc<V>(p.fy), bc<V>(p.fz));
+      const V cF = cdot<L, i>(fvec<V>(p.fx), fvec<V>(p.fy), fvec<V>(p.fz));
       ssym = mul(bc<V>(w), fma(mul(bc<V>(S(9)), cu), cF, m3uF));
       santi = mul(bc<V>(S(3) * w), cF);
     }
@@ -346,8 +353,8 @@ __device__ __forceinline__ V eqm(const V (&E1)[3][3]) {
   return e;
 }
 
-template <class L, int OP, bool SH, bool FORCE, class V, class S>
-__device__ __forceinline__ void collide_moments(V* f, Macro<V>& m, const CollideParams<S>& p) {
+template <class L, int OP, bool SH, bool FORCE, class V, class S, class FV>
+__device__ __forceinline__ void collide_moments(V* f, Macro<V>& m, const CollideParams<S, FV>& p) {
   constexpr bool central = (OP == 4);
   constexpr int D = L::D;
   constexpr S cs2 = S(1) / S(3);
@@ -417,7 +424,7 @@ __device__ __forceinline__ void collide_moments(V* f, Macro<V>& m, const Collide
   const S wb = p.omega2 < S(0) ? p.omega : p.omega2;
   const S w2 = S(1) - S(0.5) * om;
   const S invD = S(1) / S(D);
-  const V F[3] = {bc<V>(p.fx), bc<V>(p.fy), bc<V>(p.fz)};
+  const V F[3] = {fvec<V>(p.fx), fvec<V>(p.fy), fvec<V>(p.fz)};
   if constexpr (FORCE) {
 #pragma unroll
     for (int a = 0; a < D; ++a) K1[a] = add(K1[a], F[a]);
@@ -526,8 +533,8 @@ __device__ __forceinline__ void collide_moments(V* f, Macro<V>& m, const Collide
 
 // ---------------------------------------------------------------- dispatch
 // Collide one node (pair) in place; returns the macroscopic state.
-template <class L, int OP, int EQ, bool SH, bool FORCE, class V, class S>
-__device__ __forceinline__ Macro<V> collide(V* f, const CollideParams<S>& p) {
+template <class L, int OP, int EQ, bool SH, bool FORCE, class V, class S, class FV>
+__device__ __forceinline__ Macro<V> collide(V* f, const CollideParams<S, FV>& p) {
   Macro<V> m;
   if constexpr (OP == 0) {
     m.dens = bc<V>(1); m.rho = bc<V>(1);
@@ -544,8 +551,8 @@ __device__ __forceinline__ Macro<V> collide(V* f, const CollideParams<S>& p) {
 }
 
 // Macroscopic state only (compute_macroscopic, FluidSolver.hpp:1041-1179).
-template <class L, int OP, bool SH, bool FORCE, class V, class S>
-__device__ __forceinline__ Macro<V> macroscopic(const V* f, const CollideParams<S>& p) {
+template <class L, int OP, bool SH, bool FORCE, class V, class S, class FV>
+__device__ __forceinline__ Macro<V> macroscopic(const V* f, const CollideParams<S, FV>& p) {
   Macro<V> m;
   if constexpr (OP == 0) {
     m.dens = bc<V>(1); m.rho = bc<V>(1);

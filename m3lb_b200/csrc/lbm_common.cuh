@@ -34,6 +34,23 @@ struct D3Q27 {
                                  4,  4,  4,  4,  4,  1,  1,  1, 1, 1, 1, 1, 1};
 };
 
+// Scalar (advection-diffusion) lattices (src/lattice/Lattices.hpp:51-70,
+// 100-121): rest, then the axis pairs; cs2 = 1 / CS2D.
+struct D2Q5 {
+  static constexpr int Q = 5, D = 2, WDEN = 6, CS2D = 3;
+  static constexpr int cx[5] = {0, 1, -1, 0, 0};
+  static constexpr int cy[5] = {0, 0, 0, 1, -1};
+  static constexpr int cz[5] = {0, 0, 0, 0, 0};
+  static constexpr int wn[5] = {2, 1, 1, 1, 1};
+};
+struct D3Q7 {
+  static constexpr int Q = 7, D = 3, WDEN = 8, CS2D = 4;
+  static constexpr int cx[7] = {0, 1, -1, 0, 0, 0, 0};
+  static constexpr int cy[7] = {0, 0, 0, 1, -1, 0, 0};
+  static constexpr int cz[7] = {0, 0, 0, 0, 0, 1, -1};
+  static constexpr int wn[7] = {2, 1, 1, 1, 1, 1, 1};
+};
+
 template <class L>
 __host__ __device__ constexpr int cvel(int i, int a) {
   return a == 0 ? L::cx[i] : (a == 1 ? L::cy[i] : L::cz[i]);
@@ -205,6 +222,11 @@ struct StepArgs {
   double omega, omega2;    // BGK/TRT/MRT/CM rates (TRT: omega_p, omega_m; moments: omega, bulk)
   double fx, fy, fz;       // uniform Guo body force
   int* err;                // device status word: a kernel whose bounded wait ran out sets it
+  // Boussinesq buoyancy (BoussinesqGuo, src/forcing/Forcing.hpp:93-127): the
+  // force at a node is (fx, fy, fz) + g rho0 beta (T - T0) with T per
+  // interior node in the arithmetic type; temp == nullptr: (fx, fy, fz) alone
+  const void* temp;
+  double bgx, bgy, bgz, brho0, bbeta, bT0;
 };
 
 // ------------------------------------------------------------- wall nodes

@@ -31,6 +31,28 @@ __device__ __forceinline__ d2 sub(d2 a, d2 b) { return {__fma_rn(b.x, -1.0, a.x)
 __device__ __forceinline__ d2 neg(d2 a) { return {-a.x, -a.y}; }
 __device__ __forceinline__ d2 rcp(d2 a) { return {__drcp_rn(a.x), __drcp_rn(a.y)}; }
 template <> struct Lanes<d2> { using S = double; static constexpr int N = 2; };
+__device__ __forceinline__ f2 pack2(float a, float b) { return mk(a, b); }
+__device__ __forceinline__ d2 pack2(double a, double b) { return d2{a, b}; }
+
+// BoussinesqGuo::at (Forcing.hpp:113-117) for one node or a node pair at
+// temperature T: F = (fx, fy, fz) + g b, b = rho0 beta (T - T0), rounded op
+// by op so that paired and one-node kernels agree bit for bit.
+template <class V>
+__device__ __forceinline__ void buoyant_force(const StepArgs& a, V T, V& fx, V& fy, V& fz) {
+  using S = typename Lanes<V>::S;
+  const V b = mul(bc<V>(S(a.brho0) * S(a.bbeta)), sub(T, bc<V>(S(a.bT0))));
+  fx = add(bc<V>(S(a.fx)), mul(bc<V>(S(a.bgx)), b));
+  fy = add(bc<V>(S(a.fy)), mul(bc<V>(S(a.bgy)), b));
+  fz = add(bc<V>(S(a.fz)), mul(bc<V>(S(a.bgz)), b));
+}
+// Collision parameters of one node (interior index k) in the one-node kernels.
+template <bool FORCE, class R>
+__device__ __forceinline__ CollideParams<R> node_params(const StepArgs& a, size_t k) {
+  CollideParams<R> p{(R)a.omega, (R)a.omega2, (R)a.fx, (R)a.fy, (R)a.fz};
+  if constexpr (FORCE)
+    if (a.temp) buoyant_force<R>(a, reinterpret_cast<const R*>(a.temp)[k], p.fx, p.fy, p.fz);
+  return p;
+}
 template <> __device__ __forceinline__ d2 bc<d2>(double a) { return {a, a}; }
 __device__ __forceinline__ double lane_of(d2 a, int k) { return k ? a.y : a.x; }
 
@@ -237,8 +259,19 @@ __device__ __forceinline__ void pairs_unit(const StepArgs& a, long long warp, in
     for (int q = 0; q < Q; ++q) f[q] = WO::unpack(w[q]);
 
     // ---- collide
-    const CollideParams<S> prm{(S)a.omega, (S)a.omega2, (S)a.fx, (S)a.fy, (S)a.fz};
-    m = collide<L, OP, EQ, SH, FORCE>(f, prm);
+    if constexpr (FORCE) {  // the force as one value per node of the pair
+      CollideParams<S, V> prm{(S)a.omega, (S)a.omega2, bc<V>((S)a.fx), bc<V>((S)a.fy),
+                              bc<V>((S)a.fz)};
+      if (a.temp) {
+        const S* T = reinterpret_cast<const S*>(a.temp);
+        const size_t kk = ((size_t)zi * g.ny + yi) * g.nx + x0;
+        buoyant_force<V>(a, c.active ? pack2(T[kk], T[kk + 1]) : bc<V>(S(0)), prm.fx, prm.fy, prm.fz);
+      }
+      m = collide<L, OP, EQ, SH, FORCE>(f, prm);
+    } else {
+      const CollideParams<S> prm{(S)a.omega, (S)a.omega2, (S)a.fx, (S)a.fy, (S)a.fz};
+      m = collide<L, OP, EQ, SH, FORCE>(f, prm);
+    }
 #pragma unroll
     for (int q = 0; q < Q; ++q) w[q] = WO::pack(f[q]);
   } else {  // pure streaming reports rest: rho 1, u 0 (the no-collision mock)
@@ -458,7 +491,7 @@ step_nodes(StepArgs a) {
     f[i] = to_real(A[slot<Q>(g, x, y, z, i + P)]);
     f[i + 1] = to_real(A[slot<Q>(g, m[0], m[1], m[2], i + 1 - P)]);
   }
-  const CollideParams<R> prm{(R)a.omega, (R)a.omega2, (R)a.fx, (R)a.fy, (R)a.fz};
+  const CollideParams<R> prm = node_params<FORCE, R>(a, (size_t)k);
   const Macro<R> mc = collide<L, OP, EQ, SH, FORCE>(f, prm);
   A[slot<Q>(g, x, y, z, 0)] = from_real<E>(f[0]);
 #pragma unroll
@@ -692,8 +725,7 @@ __global__ void macro_kernel(StepArgs a) {
     spec_node_mirror<L>(f, a.spec[pn]);
     m = spec_node_moments<L, OP, SH>(f);
   } else {
-    const CollideParams<R> prm{(R)a.omega, (R)a.omega2, (R)a.fx, (R)a.fy, (R)a.fz};
-    m = macroscopic<L, OP, SH, FORCE>(f, prm);
+    m = macroscopic<L, OP, SH, FORCE>(f, node_params<FORCE, R>(a, (size_t)k));
   }
   rho[k] = m.rho; ux[k] = m.ux; uy[k] = m.uy; uz[k] = m.uz;
 }
@@ -744,7 +776,7 @@ reduce_kernel(StepArgs a, double* partials) {
 #pragma unroll
     for (int i = 0; i < Q; ++i) f[i] = to_real(A[load_slot<L>(g, nb, a.parity, i)]);
     if (spec_node) spec_node_mirror<L>(f, a.spec[pn]);  // reduce, FluidSolver.hpp:1221-1222
-    const Macro<R> m = macroscopic<L, OP, SH, FORCE>(f, prm);
+    const Macro<R> m = macroscopic<L, OP, SH, FORCE>(f, FORCE ? node_params<FORCE, R>(a, (size_t)k) : prm);
     const double r = (double)m.rho, u = (double)m.ux, v = (double)m.uy, w = (double)m.uz;
     acc[0] += r;
     acc[1] += r * u;

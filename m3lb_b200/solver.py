@@ -46,6 +46,28 @@ class D3Q27:
                                   4, 4, 4, 4, 4, 1, 1, 1, 1, 1, 1, 1, 1))
 
 
+class D2Q5:
+    """Scalar lattice (Lattices.hpp:51-70): advection-diffusion only."""
+    name = "D2Q5"
+    D, Q = 2, 5
+    cs2 = 1.0 / 3.0
+    cx = (0, 1, -1, 0, 0)
+    cy = (0, 0, 0, 1, -1)
+    cz = (0,) * 5
+    w = tuple(v / 6.0 for v in (2, 1, 1, 1, 1))
+
+
+class D3Q7:
+    """Scalar lattice (Lattices.hpp:100-121): cs2 = 1/4, not 1/3."""
+    name = "D3Q7"
+    D, Q = 3, 7
+    cs2 = 1.0 / 4.0
+    cx = (0, 1, -1, 0, 0, 0, 0)
+    cy = (0, 0, 0, 1, -1, 0, 0)
+    cz = (0, 0, 0, 0, 0, 1, -1)
+    w = tuple(v / 8.0 for v in (2, 1, 1, 1, 1, 1, 1))
+
+
 def opp(i: int) -> int:
     """Esoteric-Pull pairing rule (Lattices.hpp:43-45)."""
     return 0 if i == 0 else (i + 1 if i & 1 else i - 1)
@@ -456,6 +478,17 @@ class FluidSolver:
     def set_outflow_density(self, r):
         capi.check(capi.lib().m3lb_set_outflow_density(self._h, float(r)))
 
+    def set_buoyancy(self, T, g=(0.0, 1.0, 0.0), rho0=1.0, beta=1.0, T0=0.0):
+        """Boussinesq force (BoussinesqGuo): F = (fx, fy, fz) + g rho0 beta (T - T0)
+        with T a device array / tensor per interior node in the arithmetic
+        type, or None to return to the uniform force."""
+        ptr = None
+        if T is not None:
+            ptr = C.c_void_p(T.data_ptr() if hasattr(T, "data_ptr") else int(T))
+            self._buoy_keep = T
+        capi.check(capi.lib().m3lb_set_buoyancy(self._h, ptr, *map(float, g), float(rho0),
+                                               float(beta), float(T0)))
+
     def initialize(self, rho0=1.0, ux0=0.0, uy0=0.0, uz0=0.0):
         self._push_params()
         capi.check(capi.lib().m3lb_init_eq(self._h, rho0, ux0, uy0, uz0))
@@ -603,3 +636,239 @@ class FluidSolver:
         n = C.c_longlong()
         capi.check(capi.lib().m3lb_launch_count(self._h, C.byref(n)))
         return int(n.value)
+
+
+# ---------------------------------------------------------- scalar lattice
+class ScalarCell(enum.IntEnum):
+    """ScalarBGK.hpp ScalarCell."""
+    ScalarBulk = 0
+    ScalarAdiabatic = 1
+    ScalarDirichlet = 2
+    ScalarExcluded = 3
+    ScalarMoment = 4
+    ScalarOutflow = 5
+    ScalarSpecular = 6
+
+
+class ScalarBGK:
+    """ScalarBGK<L> (src/collision/ScalarBGK.hpp): raw storage with an
+    optional reference T_ref; D = cs2 (1/omega - 1/2)."""
+    code = 1
+
+    def __init__(self, lattice=D3Q7, omega=1.0, T_ref=0.0):
+        self.lattice, self.omega, self.T_ref = lattice, float(omega), float(T_ref)
+        self.Lambda = 0.25
+        self.omega_of = None
+
+    @staticmethod
+    def omega_from_diffusivity(d, lattice=D3Q7):
+        return 1.0 / (d / lattice.cs2 + 0.5)
+
+    @staticmethod
+    def diffusivity_from_omega(w, lattice=D3Q7):
+        return (1.0 / w - 0.5) * lattice.cs2
+
+
+class ScalarTRT(ScalarBGK):
+    """ScalarTRT<L> (src/collision/ScalarTRT.hpp): the odd moments at omega,
+    the even ones at omega_plus from the magic parameter Lambda."""
+    code = 2
+
+    def __init__(self, lattice=D3Q7, omega=1.0, T_ref=0.0, Lambda=0.25):
+        super().__init__(lattice, omega, T_ref)
+        self.Lambda = float(Lambda)
+
+
+class ScalarRegularised(ScalarBGK):
+    """ScalarRegularised<L> (src/collision/ScalarRegularised.hpp)."""
+    code = 3
+
+
+class ScalarSolver:
+    """ScalarSolver<L, EsotericPull<L>, Collision> (src/solver/ScalarSolver.hpp)
+    on the device.  Interior arrays are (nz, ny, nx); ``storage`` is "f32" or
+    "f64"."""
+
+    def __init__(self, domain: Domain, collision, storage="f32"):
+        self.dom, self.coll = domain, collision
+        self.storage = storage
+        L = collision.lattice
+        self.Q = L.Q
+        d = domain
+        h = C.c_void_p()
+        capi.check(capi.lib().m3lb_scalar_create(L.Q, d.nx, d.ny, d.nz, int(d.periodic[0]),
+                                                 int(d.periodic[1]), int(d.periodic[2]),
+                                                 collision.code, capi.STORAGE_NAMES[storage],
+                                                 C.byref(h)))
+        self._h = h
+        self._keep = []
+        self._cells = np.zeros((d.nz, d.ny, d.nx), np.uint8)
+        self._push()
+        if collision.omega_of is not None:
+            self.set_omega_field(collision.omega_of)
+
+    def _push(self):
+        c = self.coll
+        capi.check(capi.lib().m3lb_scalar_set_params(self._h, c.omega, c.T_ref, c.Lambda))
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            capi.lib().m3lb_scalar_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _u8(self, fn_or_array):
+        d = self.dom
+        if callable(fn_or_array):
+            z, y, x = np.meshgrid(np.arange(d.nz), np.arange(d.ny), np.arange(d.nx), indexing="ij")
+            a = np.vectorize(lambda p, q, r: int(fn_or_array(p, q, r)), otypes=[np.uint8])(x, y, z)
+        else:
+            a = np.asarray(fn_or_array)
+        return np.ascontiguousarray(np.broadcast_to(a, (d.nz, d.ny, d.nx)), dtype=np.uint8)
+
+    def _f64(self, fn_or_array, shape):
+        d = self.dom
+        if callable(fn_or_array):
+            z, y, x = np.meshgrid(np.arange(d.nz), np.arange(d.ny), np.arange(d.nx), indexing="ij")
+            a = fn_or_array(x, y, z)
+        else:
+            a = fn_or_array
+        return np.ascontiguousarray(np.broadcast_to(a, shape), dtype=np.float64)
+
+    def set_geometry(self, fn_or_cells):
+        """fn(x, y, z) -> ScalarCell, or the cells as an (nz, ny, nx) array (:92-99)."""
+        c = self._u8(fn_or_cells)
+        capi.check(capi.lib().m3lb_scalar_set_cells(self._h, _ptr(c)))
+        self._cells = c.copy()
+
+    def set_wall_values(self, fn_or_values):
+        d = self.dom
+        v = self._f64(fn_or_values, (d.nz, d.ny, d.nx))
+        capi.check(capi.lib().m3lb_scalar_set_wall_values(self._h, _ptr(v)))
+
+    def set_specular_walls(self, fn_or_codes):
+        capi.check(capi.lib().m3lb_scalar_set_specular_walls(self._h, _ptr(self._u8(fn_or_codes))))
+
+    def set_specular_nodes(self, fn_or_masks):
+        capi.check(capi.lib().m3lb_scalar_set_specular_nodes(self._h, _ptr(self._u8(fn_or_masks))))
+
+    def set_omega_field(self, fn_or_values):
+        d = self.dom
+        v = None if fn_or_values is None else self._f64(fn_or_values, (d.nz, d.ny, d.nx))
+        capi.check(capi.lib().m3lb_scalar_set_omega_field(self._h, None if v is None else _ptr(v)))
+
+    def set_velocity(self, ux, uy=None, uz=None):
+        """The advecting velocity: device tensors / pointers of the arithmetic
+        type, or host arrays (uploaded once), or None (at rest)."""
+        if ux is None:
+            capi.check(capi.lib().m3lb_scalar_set_velocity_device(self._h, None, None, None))
+            self._keep = []
+            return
+        import torch
+        dt = torch.float64 if self.storage == "f64" else torch.float32
+        d = self.dom
+        ts = []
+        for a in (ux, uy, uz):
+            if isinstance(a, torch.Tensor):
+                t = a.to(device="cuda", dtype=dt).contiguous()
+            else:
+                t = torch.as_tensor(np.array(np.broadcast_to(a, (d.nz, d.ny, d.nx))),
+                                    dtype=dt, device="cuda")
+            ts.append(t)
+        torch.cuda.synchronize()
+        self._keep = ts
+        capi.check(capi.lib().m3lb_scalar_set_velocity_device(
+            self._h, *[C.c_void_p(t.data_ptr()) for t in ts]))
+
+    def finalize_geometry(self):
+        capi.check(capi.lib().m3lb_scalar_finalize_geometry(self._h))
+
+    def initialize(self, T0):
+        self._push()
+        capi.check(capi.lib().m3lb_scalar_init(self._h, float(T0)))
+
+    def initialize_field(self, T_padded):
+        """T per padded node (n_padded values), as the reference's fn(n)."""
+        self._push()
+        v = np.ascontiguousarray(np.ravel(T_padded), dtype=np.float64)
+        if v.size != self.dom.n_padded:
+            raise ValueError(f"initialize_field: {v.size} values, the lattice has {self.dom.n_padded} padded nodes")
+        capi.check(capi.lib().m3lb_scalar_init_field(self._h, _ptr(v)))
+
+    def step(self):
+        self._push()
+        capi.check(capi.lib().m3lb_scalar_step(self._h, 1))
+
+    def steps(self, n):
+        self._push()
+        capi.check(capi.lib().m3lb_scalar_step(self._h, int(n)))
+
+    def add_source(self, fn_or_values):
+        d = self.dom
+        v = self._f64(fn_or_values, (d.nz, d.ny, d.nx))
+        capi.check(capi.lib().m3lb_scalar_add_source(self._h, _ptr(v)))
+
+    def compute_field(self):
+        capi.check(capi.lib().m3lb_scalar_compute_field(self._h))
+
+    def temperature(self):
+        """The field per interior node as it stands (ScalarSolver::temperature)."""
+        d = self.dom
+        out = np.empty((d.nz, d.ny, d.nx), np.float64)
+        capi.check(capi.lib().m3lb_scalar_field(self._h, _ptr(out)))
+        return out
+
+    def field_device(self):
+        p = C.c_void_p()
+        capi.check(capi.lib().m3lb_scalar_field_device(self._h, C.byref(p)))
+        return p.value
+
+    def total_population(self):
+        out = C.c_double()
+        capi.check(capi.lib().m3lb_scalar_total(self._h, C.byref(out)))
+        return out.value
+
+    def gather_populations(self):
+        out = np.empty((self.dom.n_padded, self.Q), np.float64)
+        capi.check(capi.lib().m3lb_scalar_gather(self._h, _ptr(out)))
+        return out
+
+    def flags(self):
+        return self._cells
+
+    def timestep(self):
+        t = C.c_longlong()
+        capi.check(capi.lib().m3lb_scalar_info(self._h, None, C.byref(t), None))
+        return int(t.value)
+
+    def domain(self):
+        return self.dom
+
+    def sync(self):
+        capi.check(capi.lib().m3lb_scalar_sync(self._h))
+
+
+def couple_thermal(fluid: "FluidSolver", scalar: ScalarSolver, g=(0.0, 1.0, 0.0), rho0=1.0,
+                   beta=1.0, T0=0.0):
+    """Two-way coupling (BoussinesqGuo + set_velocity, as in the reference's
+    validation/rayleigh_benard.cpp): the fluid's force reads the scalar's
+    field, the scalar is advected by the fluid's stored velocity, both on the
+    fluid's stream.  Step as fluid.step(True); scalar.step()."""
+    capi.check(capi.lib().m3lb_couple_thermal(fluid.handle, scalar.handle, *map(float, g),
+                                             float(rho0), float(beta), float(T0)))
+    scalar._keep = [fluid]
