@@ -189,6 +189,13 @@ int m3lb_set_outflow_density(m3lb_solver* h, double rho);
  * or the one-node kernel. */
 int m3lb_set_buoyancy(m3lb_solver* h, const void* T, double gx, double gy, double gz, double rho0,
                       double beta, double T0);
+/* The same with T given on the host (doubles per interior node), copied to a
+ * device array the handle owns; call again when T changes. */
+int m3lb_set_buoyancy_host(m3lb_solver* h, const double* T, double gx, double gy, double gz,
+                           double rho0, double beta, double T0);
+/* Make the work queued on stream `then` after this call wait for what is
+ * queued on stream `first` now (an event; no host wait). */
+int m3lb_stream_order(void* first, void* then);
 /* Device arrays of the stored rho and u (written by m3lb_step with
  * store_macro and by m3lb_macro_device), without computing them. */
 int m3lb_macro_pointers(const m3lb_solver* h, void** rho, void** ux, void** uy, void** uz);
@@ -274,9 +281,10 @@ int m3lb_reduce_static(int lattice, int nx, int ny, int nz, int px, int py, int 
 
 /* ------------------------------------------------------------ scalar lattice
  * ScalarSolver<L, EsotericPull<L>, Collision> (src/solver/ScalarSolver.hpp):
- * an advection-diffusion lattice, D2Q5 (lattice 5, nz = 1) or D3Q7 (7),
- * stored in FP32 or FP64, with the collision operators ScalarBGK,
- * ScalarTRT and ScalarRegularised (src/collision/Scalar*.hpp).  Cell types
+ * an advection-diffusion lattice, D2Q5 (lattice 5, nz = 1) or D3Q7 (7) with
+ * the collision operators ScalarBGK, ScalarTRT and ScalarRegularised
+ * (src/collision/Scalar*.hpp), or D2Q9 (9) / D3Q27 (27) with ScalarBGK,
+ * stored in FP32 or FP64.  Cell types
  * per interior node (ScalarBGK.hpp ScalarCell): 0 bulk, 1 adiabatic (zero
  * flux), 2 Dirichlet (anti-bounce-back to the wall value), 3 excluded,
  * 4 moment (the wall value imposed ON the node, MomentDirichlet.hpp), 5
@@ -293,6 +301,7 @@ int m3lb_scalar_create(int lattice, int nx, int ny, int nz, int px, int py, int 
 int m3lb_scalar_destroy(m3lb_scalar* h);
 /* ScalarBGK::omega, T_ref (the storage reference, 0 = raw), ScalarTRT::Lambda. */
 int m3lb_scalar_set_params(m3lb_scalar* h, double omega, double T_ref, double Lambda);
+/* Queue the handle's work on `stream` (NULL: on the handle's own stream). */
 int m3lb_scalar_set_stream(m3lb_scalar* h, void* stream);
 /* set_geometry(fn -> ScalarCell) (:92-99): cell types 0..6 per interior node. */
 int m3lb_scalar_set_cells(m3lb_scalar* h, const uint8_t* cells);
@@ -307,6 +316,11 @@ int m3lb_scalar_set_omega_field(m3lb_scalar* h, const double* omega);
 /* set_velocity (:166-168): device arrays of the advecting velocity per
  * interior node in the arithmetic type, read at every step (NULL: at rest). */
 int m3lb_scalar_set_velocity_device(m3lb_scalar* h, const void* ux, const void* uy, const void* uz);
+/* The advecting velocity given on the host (doubles per interior node),
+ * copied to arrays the handle owns (NULL: at rest). */
+int m3lb_scalar_set_velocity_host(m3lb_scalar* h, const double* ux, const double* uy,
+                                  const double* uz);
+int m3lb_scalar_get_stream(const m3lb_scalar* h, void** stream);
 /* finalize_geometry (:223-296): moment-cell unknowns and outflow donors. */
 int m3lb_scalar_finalize_geometry(m3lb_scalar* h);
 /* initialize(T0) / initialize_field(fn(n)) (:170-190); the field is given
@@ -335,8 +349,9 @@ int m3lb_scalar_sync(m3lb_scalar* h);
  * th.set_velocity(fl.ux(), fl.uy(), fl.uz()), validation/rayleigh_benard.cpp):
  * the fluid's Boussinesq force reads the scalar's field, the scalar is
  * advected by the fluid's stored velocity (store_macro), and the scalar's
- * work goes onto the fluid's stream so the two alternate in order.  Destroy
- * the scalar before the fluid, or give it another stream first. */
+ * work goes onto the fluid's stream so the two alternate in order.  The
+ * scalar must not be stepped after the fluid is destroyed (destroying the
+ * scalar afterwards is safe). */
 int m3lb_couple_thermal(m3lb_solver* fluid, m3lb_scalar* scalar, double gx, double gy, double gz,
                         double rho0, double beta, double T0);
 

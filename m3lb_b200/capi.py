@@ -88,6 +88,10 @@ SIGNATURES = {
     "m3lb_set_outflow_order": (_i, [_vp, _i]),
     "m3lb_set_outflow_density": (_i, [_vp, _d]),
     "m3lb_set_buoyancy": (_i, [_vp, _vp] + [_d] * 6),
+    "m3lb_set_buoyancy_host": (_i, [_vp, _vp] + [_d] * 6),
+    "m3lb_stream_order": (_i, [_vp, _vp]),
+    "m3lb_scalar_set_velocity_host": (_i, [_vp] * 4),
+    "m3lb_scalar_get_stream": (_i, [_vp, _pp]),
     "m3lb_macro_pointers": (_i, [_vp] + [_pp] * 4),
     "m3lb_get_stream": (_i, [_vp, _pp]),
     "m3lb_scalar_create": (_i, [_i] * 9 + [_pp]),

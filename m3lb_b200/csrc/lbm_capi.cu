@@ -126,6 +126,7 @@ struct m3lb_solver {
   // Boussinesq buoyancy: temperature per interior node (arithmetic type)
   const void* temp = nullptr;
   double bg[3] = {0, 0, 0}, brho0 = 1, bbeta = 1, bT0 = 0;
+  void* temp_own = nullptr;          // m3lb_set_buoyancy_host's copy of T
   void* macro[4] = {nullptr, nullptr, nullptr, nullptr};  // interior, arithmetic type
   void* staging = nullptr;           // init_field uploads (4 interior arrays)
   double* partials = nullptr;        // reduction scratch
@@ -271,6 +272,7 @@ int m3lb_destroy(m3lb_solver* h) {
   if (h->stream) cudaStreamSynchronize(h->stream);
   cudaFree(h->f);
   cudaFree(h->flags);
+  cudaFree(h->temp_own);
   h->walls.release();
   for (void* p : h->macro) cudaFree(p);
   cudaFree(h->staging);
@@ -443,6 +445,36 @@ int m3lb_set_buoyancy(m3lb_solver* h, const void* T, double gx, double gy, doubl
   h->temp = T;
   h->bg[0] = gx; h->bg[1] = gy; h->bg[2] = gz;
   h->brho0 = rho0; h->bbeta = beta; h->bT0 = T0;
+  return M3LB_OK;
+}
+int m3lb_set_buoyancy_host(m3lb_solver* h, const double* T, double gx, double gy, double gz,
+                           double rho0, double beta, double T0) {
+  if (!h) return fail(M3LB_ERR_INVALID, "set_buoyancy: null handle");
+  if (!T) return m3lb_set_buoyancy(h, nullptr, gx, gy, gz, rho0, beta, T0);
+  if (!h->forcing) return fail(M3LB_ERR_INVALID, "set_buoyancy: the solver was created without forcing");
+  DeviceGuard dg(h->device);
+  const size_t n = (size_t)h->n_interior(), rb = real_bytes(h->storage);
+  if (!h->temp_own && cudaMalloc(&h->temp_own, n * rb) != cudaSuccess) {
+    h->temp_own = nullptr;
+    return fail(M3LB_ERR_MEMORY, "set_buoyancy: cannot allocate %zu bytes", n * rb);
+  }
+  std::vector<char> tmp(n * rb);
+  for (size_t i = 0; i < n; ++i) {
+    if (rb == 8) reinterpret_cast<double*>(tmp.data())[i] = T[i];
+    else reinterpret_cast<float*>(tmp.data())[i] = (float)T[i];
+  }
+  CUDA_TRY(cudaMemcpyAsync(h->temp_own, tmp.data(), tmp.size(), cudaMemcpyHostToDevice, h->stream));
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return m3lb_set_buoyancy(h, h->temp_own, gx, gy, gz, rho0, beta, T0);
+}
+int m3lb_stream_order(void* first, void* then) {
+  if (first == then) return M3LB_OK;
+  cudaEvent_t e;
+  CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  cudaError_t r = cudaEventRecord(e, (cudaStream_t)first);
+  if (r == cudaSuccess) r = cudaStreamWaitEvent((cudaStream_t)then, e, 0);
+  cudaEventDestroy(e);
+  if (r != cudaSuccess) return fail(M3LB_ERR_CUDA, "stream_order: %s", cudaGetErrorString(r));
   return M3LB_OK;
 }
 int m3lb_macro_pointers(const m3lb_solver* h, void** rho, void** ux, void** uy, void** uz) {

@@ -16,14 +16,14 @@ namespace m3lb {
 
 // ---------------------------------------------------------------- lattices
 struct D2Q9 {
-  static constexpr int Q = 9, D = 2, WDEN = 36;
+  static constexpr int Q = 9, D = 2, WDEN = 36, CS2D = 3;
   static constexpr int cx[9] = {0, 1, -1, 0, 0, 1, -1, 1, -1};
   static constexpr int cy[9] = {0, 0, 0, 1, -1, 1, -1, -1, 1};
   static constexpr int cz[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
   static constexpr int wn[9] = {16, 4, 4, 4, 4, 1, 1, 1, 1};
 };
 struct D3Q27 {
-  static constexpr int Q = 27, D = 3, WDEN = 216;
+  static constexpr int Q = 27, D = 3, WDEN = 216, CS2D = 3;
   static constexpr int cx[27] = {0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1,
                                  0, 0, 0, 0, 1, -1, 1, -1, 1, -1, -1, 1};
   static constexpr int cy[27] = {0, 0, 0, 1, -1, 0, 0, 1, -1, -1, 1, 0, 0, 0, 0,

@@ -1,12 +1,13 @@
-// The scalar (advection-diffusion) lattice: D2Q5 / D3Q7 on Esoteric Pull,
+// The scalar (advection-diffusion) lattice: D2Q5 / D3Q7 (and, with ScalarBGK,
+// D2Q9 / D3Q27) on Esoteric Pull,
 // the reference's ScalarSolver (src/solver/ScalarSolver.hpp) with ScalarBGK,
 // ScalarTRT and ScalarRegularised (src/collision/Scalar*.hpp), its cell types
 // (adiabatic, Dirichlet, on-node moment, outflow, specular) and the thermal
 // coupling to a fluid handle: the fluid's stored velocity advects the scalar,
 // the scalar's field drives the fluid's Boussinesq force.
 //
-// Same storage layout as the fluid (x-chunked, lbm_common.cuh) with Q = 5 or
-// 7; one thread per node, x fastest, so each direction's loads and stores of
+// Same storage layout as the fluid (x-chunked, lbm_common.cuh) with Q = 5, 7,
+// 9 or 27; one thread per node, x fastest, so each direction's loads and stores of
 // a warp are contiguous.  FP32 or FP64 storage; arithmetic in the same type.
 #include <cuda_runtime.h>
 
@@ -363,9 +364,14 @@ struct ScalarOps {
   static cudaError_t step(const ScalarArgs& a, int op, cudaStream_t s) {
     const long long n = (long long)a.g.nx * a.g.ny * a.g.nz;
     const unsigned b = blocks(n, kScalarThreads);
-    if (op == 1) scalar_step<L, ST, 1><<<b, kScalarThreads, 0, s>>>(a);
-    else if (op == 2) scalar_step<L, ST, 2><<<b, kScalarThreads, 0, s>>>(a);
-    else scalar_step<L, ST, 3><<<b, kScalarThreads, 0, s>>>(a);
+    if (op == 1) {
+      scalar_step<L, ST, 1><<<b, kScalarThreads, 0, s>>>(a);
+    } else if constexpr (L::Q == 2 * L::D + 1) {  // TRT / regularised: axis-pair lattices
+      if (op == 2) scalar_step<L, ST, 2><<<b, kScalarThreads, 0, s>>>(a);
+      else scalar_step<L, ST, 3><<<b, kScalarThreads, 0, s>>>(a);
+    } else {
+      return cudaErrorInvalidValue;
+    }
     return cudaGetLastError();
   }
   static cudaError_t outflow(const ScalarArgs& a, const long long* nk, const long long* dk, int c,
@@ -414,8 +420,14 @@ const ScalarTable* table() {
   return &t;
 }
 const ScalarTable* scalar_table(int lattice, int storage) {
-  if (lattice == 5) return storage == M3LB_STORE_F64 ? table<D2Q5, kF64>() : table<D2Q5, kF32>();
-  return storage == M3LB_STORE_F64 ? table<D3Q7, kF64>() : table<D3Q7, kF32>();
+  const bool f64 = storage == M3LB_STORE_F64;
+  switch (lattice) {
+    case 5: return f64 ? table<D2Q5, kF64>() : table<D2Q5, kF32>();
+    case 7: return f64 ? table<D3Q7, kF64>() : table<D3Q7, kF32>();
+    case 9: return f64 ? table<D2Q9, kF64>() : table<D2Q9, kF32>();
+    case 27: return f64 ? table<D3Q27, kF64>() : table<D3Q27, kF32>();
+    default: return nullptr;
+  }
 }
 
 int sfail(int code, const char* fmt, ...) {
@@ -442,8 +454,8 @@ struct m3lb_scalar {
   int lattice = 7, Q = 7, op = 1, storage = M3LB_STORE_F32;
   Geo g{};
   int device = 0;
-  cudaStream_t stream = nullptr;
-  bool own_stream = false;
+  cudaStream_t stream = nullptr;  // where the work is queued
+  cudaStream_t own = nullptr;     // the stream the handle created
   double omega = 1, T_ref = 0, Lambda = 0.25;
   long long t = 0, launches = 0;
   void* f = nullptr;
@@ -456,6 +468,7 @@ struct m3lb_scalar {
   const void* ux = nullptr;
   const void* uy = nullptr;
   const void* uz = nullptr;
+  void* u_own = nullptr;          // m3lb_scalar_set_velocity_host's copy (3 arrays)
   void* scratch = nullptr;        // host-array uploads and the source array
   size_t scratch_bytes = 0;
   double* partials = nullptr;     // total: per-block sums, then the result
@@ -532,8 +545,12 @@ int m3lb_scalar_create(int lattice, int nx, int ny, int nz, int px, int py, int 
                        int storage, m3lb_scalar** out) {
   if (!out) return sfail(M3LB_ERR_INVALID, "scalar_create: null output handle");
   *out = nullptr;
-  if (lattice != 5 && lattice != 7) return sfail(M3LB_ERR_INVALID, "scalar_create: lattice must be 5 or 7");
-  if (lattice == 5 && nz != 1) return sfail(M3LB_ERR_INVALID, "scalar_create: D2Q5 needs nz == 1");
+  if (lattice != 5 && lattice != 7 && lattice != 9 && lattice != 27)
+    return sfail(M3LB_ERR_INVALID, "scalar_create: lattice must be 5, 7, 9 or 27");
+  if ((lattice == 5 || lattice == 9) && nz != 1)
+    return sfail(M3LB_ERR_INVALID, "scalar_create: a 2-D lattice needs nz == 1");
+  if ((lattice == 9 || lattice == 27) && op != M3LB_SOP_BGK)
+    return sfail(M3LB_ERR_INVALID, "scalar_create: ScalarTRT and ScalarRegularised need D2Q5 or D3Q7");
   if (nx < 1 || ny < 1 || nz < 1) return sfail(M3LB_ERR_INVALID, "scalar_create: extents must be >= 1");
   if (op < M3LB_SOP_BGK || op > M3LB_SOP_REGULARISED)
     return sfail(M3LB_ERR_INVALID, "scalar_create: bad operator %d", op);
@@ -556,9 +573,9 @@ int m3lb_scalar_create(int lattice, int nx, int ny, int nz, int px, int py, int 
   h->nblocks = reduce_blocks(g);
   if (cudaMalloc((void**)&h->partials, ((size_t)h->nblocks + 1) * 8) != cudaSuccess)
     return cleanup(sfail(M3LB_ERR_MEMORY, "scalar_create: cannot allocate reduction scratch"));
-  if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess)
+  if (cudaStreamCreateWithFlags(&h->own, cudaStreamNonBlocking) != cudaSuccess)
     return cleanup(sfail(M3LB_ERR_CUDA, "scalar_create: cannot create stream"));
-  h->own_stream = true;
+  h->stream = h->own;
   // interior nodes bulk, halo excluded (ScalarSolver.hpp:81-86)
   h->cells_host.assign((size_t)g.n_padded, kSExcluded);
   for (int z = 0; z < nz; ++z)
@@ -577,11 +594,13 @@ int m3lb_scalar_create(int lattice, int nx, int ny, int nz, int px, int py, int 
 int m3lb_scalar_destroy(m3lb_scalar* h) {
   if (!h) return M3LB_OK;
   SGuard dg(h->device);
-  if (h->stream) cudaStreamSynchronize(h->stream);
+  // the queue may be another handle's stream, possibly gone already: wait
+  // for the whole device rather than for that stream
+  cudaDeviceSynchronize();
   for (void* p : {h->f, (void*)h->cells, (void*)h->spec, (void*)h->unk, h->wall, h->field, h->omega_of,
-                  h->scratch, (void*)h->partials, (void*)h->out_nodes, (void*)h->out_donor})
+                  h->u_own, h->scratch, (void*)h->partials, (void*)h->out_nodes, (void*)h->out_donor})
     cudaFree(p);
-  if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
+  if (h->own) cudaStreamDestroy(h->own);
   delete h;
   return M3LB_OK;
 }
@@ -596,14 +615,9 @@ int m3lb_scalar_set_stream(m3lb_scalar* h, void* stream) {
   if (!h) return sfail(M3LB_ERR_INVALID, "scalar_set_stream: null handle");
   SGuard dg(h->device);
   if (h->stream) cudaStreamSynchronize(h->stream);
-  if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
-  h->own_stream = false;
-  h->stream = (cudaStream_t)stream;
-  if (!h->stream) {
-    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess)
-      return sfail(M3LB_ERR_CUDA, "scalar_set_stream: cannot create stream");
-    h->own_stream = true;
-  }
+  // the handle's own stream lives until the handle does: callers may still
+  // order other work after it
+  h->stream = stream ? (cudaStream_t)stream : h->own;
   return M3LB_OK;
 }
 
@@ -692,6 +706,33 @@ int m3lb_scalar_set_velocity_device(m3lb_scalar* h, const void* ux, const void* 
   return M3LB_OK;
 }
 
+int m3lb_scalar_set_velocity_host(m3lb_scalar* h, const double* ux, const double* uy,
+                                  const double* uz) {
+  if (!h) return sfail(M3LB_ERR_INVALID, "scalar_set_velocity: null handle");
+  if (!ux || !uy || !uz) return m3lb_scalar_set_velocity_device(h, nullptr, nullptr, nullptr);
+  SGuard dg(h->device);
+  const size_t n = (size_t)h->nint(), rb = h->rb();
+  int rc = ensure(&h->u_own, 3 * n * rb);
+  if (rc) return rc;
+  std::vector<char> tmp(3 * n * rb);
+  const double* src[3] = {ux, uy, uz};
+  for (int c = 0; c < 3; ++c)
+    for (size_t i = 0; i < n; ++i) {
+      if (rb == 8) reinterpret_cast<double*>(tmp.data())[c * n + i] = src[c][i];
+      else reinterpret_cast<float*>(tmp.data())[c * n + i] = (float)src[c][i];
+    }
+  S_TRY(cudaMemcpyAsync(h->u_own, tmp.data(), tmp.size(), cudaMemcpyHostToDevice, h->stream));
+  S_TRY(cudaStreamSynchronize(h->stream));
+  char* b = static_cast<char*>(h->u_own);
+  return m3lb_scalar_set_velocity_device(h, b, b + n * rb, b + 2 * n * rb);
+}
+
+int m3lb_scalar_get_stream(const m3lb_scalar* h, void** stream) {
+  if (!h || !stream) return sfail(M3LB_ERR_INVALID, "scalar_get_stream: null argument");
+  *stream = (void*)h->stream;
+  return M3LB_OK;
+}
+
 int m3lb_scalar_finalize_geometry(m3lb_scalar* h) {
   if (!h) return sfail(M3LB_ERR_INVALID, "scalar_finalize_geometry: null handle");
   const Geo& g = h->g;
@@ -699,8 +740,12 @@ int m3lb_scalar_finalize_geometry(m3lb_scalar* h) {
   const int per[3] = {g.px, g.py, g.pz};
   const int* cv[3];
   int Q = h->Q;
-  if (Q == 5) { cv[0] = D2Q5::cx; cv[1] = D2Q5::cy; cv[2] = D2Q5::cz; }
-  else { cv[0] = D3Q7::cx; cv[1] = D3Q7::cy; cv[2] = D3Q7::cz; }
+  switch (Q) {
+    case 5: cv[0] = D2Q5::cx; cv[1] = D2Q5::cy; cv[2] = D2Q5::cz; break;
+    case 7: cv[0] = D3Q7::cx; cv[1] = D3Q7::cy; cv[2] = D3Q7::cz; break;
+    case 9: cv[0] = D2Q9::cx; cv[1] = D2Q9::cy; cv[2] = D2Q9::cz; break;
+    default: cv[0] = D3Q27::cx; cv[1] = D3Q27::cy; cv[2] = D3Q27::cz; break;
+  }
   // unknown directions of moment nodes (MomentDirichlet.hpp unknown_mask)
   std::vector<uint32_t> unk;
   bool any_moment = false;

@@ -57,7 +57,9 @@ class View {
       : label_(label), n0_(n0), n1_(rank >= 2 ? n1 : 1),
         data_(std::make_shared<std::vector<non_const_value_type>>(n0 * (rank >= 2 ? n1 : 1))) {}
   template <class D2, class... P2>
-  View(const View<D2, P2...>& o) : label_(o.label_), n0_(o.n0_), n1_(o.n1_), data_(o.data_) {}
+  View(const View<D2, P2...>& o)
+      : label_(o.label_), n0_(o.n0_), n1_(o.n1_), data_(o.data_), dev_(o.dev_),
+        dev_stream_(o.dev_stream_) {}
 
   value_type& operator()(std::size_t i) const { return (*data_)[i]; }
   value_type& operator()(std::size_t i, std::size_t j) const { return (*data_)[i * n1_ + j]; }
@@ -71,6 +73,12 @@ class View {
   std::string label_;
   std::size_t n0_ = 0, n1_ = 1;
   std::shared_ptr<std::vector<non_const_value_type>> data_;
+  // A view a solver hands out for a field it holds on the device: that
+  // field's device array (one value per interior node, the solver's
+  // arithmetic type) and the stream its writes are queued on.  Another
+  // solver given this view reads the device array directly.
+  const void* dev_ = nullptr;
+  void* dev_stream_ = nullptr;
 };
 
 template <class V> V create_mirror_view(const V& v) { return v; }
@@ -80,6 +88,11 @@ template <class D1, class... P1, class D2, class... P2>
 void deep_copy(const View<D1, P1...>& dst, const View<D2, P2...>& src) {
   if (dst.data() != src.data())
     for (std::size_t i = 0; i < dst.size() && i < src.size(); ++i) dst.data()[i] = src.data()[i];
+}
+
+template <class D1, class... P1>
+void deep_copy(const View<D1, P1...>& dst, const typename View<D1, P1...>::value_type& v) {
+  for (std::size_t i = 0; i < dst.size(); ++i) dst.data()[i] = v;
 }
 
 template <class Exec = DefaultExecutionSpace>

@@ -46,6 +46,34 @@ struct D3Q27 {
   LBM_FN static constexpr int w_num(int i) noexcept { return facade_tables::d3q27_w[i]; }
 };
 
+// Scalar lattices: advection-diffusion only (no Navier-Stokes).
+namespace facade_tables {
+constexpr int d2q5_c[2][5] = {{0, 1, -1, 0, 0}, {0, 0, 0, 1, -1}};
+constexpr int d3q7_c[3][7] = {{0, 1, -1, 0, 0, 0, 0}, {0, 0, 0, 1, -1, 0, 0}, {0, 0, 0, 0, 0, 1, -1}};
+constexpr int scalar_w[7] = {2, 1, 1, 1, 1, 1, 1};
+}  // namespace facade_tables
+struct D2Q5 {
+  static constexpr const char* name = "D2Q5";
+  static constexpr int D = 2, Q = 5;
+  static constexpr int cs2_num = 1, cs2_den = 3;
+  static constexpr int w_den = 6;
+  static constexpr bool supports_navier_stokes = false;
+  LBM_FN static constexpr int cx(int i) noexcept { return facade_tables::d2q5_c[0][i]; }
+  LBM_FN static constexpr int cy(int i) noexcept { return facade_tables::d2q5_c[1][i]; }
+  LBM_FN static constexpr int w_num(int i) noexcept { return facade_tables::scalar_w[i]; }
+};
+struct D3Q7 {
+  static constexpr const char* name = "D3Q7";
+  static constexpr int D = 3, Q = 7;
+  static constexpr int cs2_num = 1, cs2_den = 4;
+  static constexpr int w_den = 8;
+  static constexpr bool supports_navier_stokes = false;
+  LBM_FN static constexpr int cx(int i) noexcept { return facade_tables::d3q7_c[0][i]; }
+  LBM_FN static constexpr int cy(int i) noexcept { return facade_tables::d3q7_c[1][i]; }
+  LBM_FN static constexpr int cz(int i) noexcept { return facade_tables::d3q7_c[2][i]; }
+  LBM_FN static constexpr int w_num(int i) noexcept { return facade_tables::scalar_w[i]; }
+};
+
 template <class L, class T> LBM_FN constexpr T weight(int i) noexcept {
   return static_cast<T>(L::w_num(i)) / static_cast<T>(L::w_den);
 }

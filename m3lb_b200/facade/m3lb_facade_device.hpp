@@ -19,6 +19,7 @@ namespace m3lb_facade {
 struct Registry {
   std::mutex mu;
   std::set<m3lb_solver*> live;
+  std::set<m3lb_scalar*> live_scalar;
 };
 inline Registry& registry() {
   static Registry r;
@@ -32,6 +33,14 @@ inline void remove(m3lb_solver* h) {
   std::lock_guard<std::mutex> g(registry().mu);
   registry().live.erase(h);
 }
+inline void add(m3lb_scalar* h) {
+  std::lock_guard<std::mutex> g(registry().mu);
+  registry().live_scalar.insert(h);
+}
+inline void remove(m3lb_scalar* h) {
+  std::lock_guard<std::mutex> g(registry().mu);
+  registry().live_scalar.erase(h);
+}
 
 inline void check(int rc, const char* what) {
   if (rc != M3LB_OK) {
@@ -43,6 +52,7 @@ inline void check(int rc, const char* what) {
 inline void fence_all() {
   std::lock_guard<std::mutex> g(registry().mu);
   for (m3lb_solver* h : registry().live) check(m3lb_sync(h), "fence");
+  for (m3lb_scalar* h : registry().live_scalar) check(m3lb_scalar_sync(h), "fence");
 }
 
 }  // namespace m3lb_facade

@@ -61,6 +61,7 @@ template <class L> struct IsDeviceStreaming<TwoLattice<L>> : std::true_type {};
 template <class F> struct IsDeviceForcing : std::false_type {};
 template <> struct IsDeviceForcing<NoForcing> : std::true_type {};
 template <> struct IsDeviceForcing<Guo> : std::true_type {};
+template <> struct IsDeviceForcing<BoussinesqGuo> : std::true_type {};
 template <class C, class = void> struct EqCode { static constexpr int value = 0; };
 template <class C>
 struct EqCode<C, std::void_t<decltype(C::Equilibrium::device_code)>> {
@@ -86,7 +87,7 @@ class FluidSolver {
   static_assert(facade::IsDeviceStreaming<Streaming>::value,
                 "the B200 path streams with Esoteric Pull (TwoLattice runs as Esoteric Pull)");
   static_assert(facade::IsDeviceForcing<typename Collision::ForcingPolicy>::value,
-                "the B200 path runs NoForcing and the uniform Guo force");
+                "the B200 path runs NoForcing, the uniform Guo force and BoussinesqGuo");
 
   FluidSolver(const Domain& dom, const Collision& coll)
       : dom_(dom), coll_(coll), flags_("flags", dom.n_padded), rho_("rho", dom.n_padded),
@@ -99,6 +100,7 @@ class FluidSolver {
                     Collision::ForcingPolicy::active ? 1 : 0, &h_),
         "FluidSolver");
     m3lb_facade::add(h_);
+    bind_fields();
     for (Index n = 0; n < dom.n_padded; ++n) {
       Index px, py, pz;
       dom_.coords(n, px, py, pz);
@@ -325,7 +327,41 @@ class FluidSolver {
         for (Index x = 0; x < dom_.nx; ++x)
           if (a[(std::size_t(z) * dom_.ny + y) * dom_.nx + x]) flags_(dom_.id(x, y, z)) = type;
   }
+  // The field views carry the device arrays they mirror, so that a scalar
+  // solver given ux() / uy() / uz() reads the velocity on the device.
+  void bind_fields() {
+    void *r = nullptr, *u = nullptr, *v = nullptr, *w = nullptr, *st = nullptr;
+    m3lb_facade::check(m3lb_macro_pointers(h_, &r, &u, &v, &w), "fields");
+    m3lb_facade::check(m3lb_get_stream(h_, &st), "stream");
+    View1D<Real>* views[4] = {&rho_, &ux_, &uy_, &uz_};
+    void* ptrs[4] = {r, u, v, w};
+    for (int i = 0; i < 4; ++i) { views[i]->dev_ = ptrs[i]; views[i]->dev_stream_ = st; }
+  }
+  // BoussinesqGuo: the temperature the force reads, bound before each step.
+  void push_buoyancy() {
+    if constexpr (std::is_same_v<typename Collision::ForcingPolicy, BoussinesqGuo>) {
+      const BoussinesqGuo& F = coll_.forcing;
+      if (F.T.dev_) {
+        void* st = nullptr;
+        m3lb_facade::check(m3lb_get_stream(h_, &st), "stream");
+        m3lb_facade::check(m3lb_stream_order(F.T.dev_stream_, st), "stream order");
+        m3lb_facade::check(m3lb_set_buoyancy(h_, F.T.dev_, F.gx, F.gy, F.gz, F.rho0, F.beta, F.T0),
+                           "buoyancy");
+      } else if (F.T.data()) {
+        std::vector<double> t(std::size_t(dom_.n_interior()));
+        for (Index z = 0; z < dom_.nz; ++z)
+          for (Index y = 0; y < dom_.ny; ++y)
+            for (Index x = 0; x < dom_.nx; ++x)
+              t[(std::size_t(z) * dom_.ny + y) * dom_.nx + x] = double(F.T(dom_.id(x, y, z)));
+        m3lb_facade::check(m3lb_set_buoyancy_host(h_, t.data(), F.gx, F.gy, F.gz, F.rho0, F.beta,
+                                                  F.T0), "buoyancy");
+      } else {
+        m3lb_facade::check(m3lb_set_buoyancy(h_, nullptr, 0, 0, 0, 1, 1, 0), "buoyancy");
+      }
+    }
+  }
   void push_params() {
+    push_buoyancy();
     double w1 = 1, w2 = -1;
     coll_.device_rates(w1, w2);
     double f[3] = {0, 0, 0};

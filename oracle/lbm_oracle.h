@@ -75,6 +75,7 @@
 
 /* The scalar (advection-diffusion) lattice: src/solver/ScalarSolver.hpp.
  * lattice 5 (D2Q5) / 7 (D3Q7); op 1 ScalarBGK, 2 ScalarTRT, 3 ScalarRegularised;
+ * lattice 9 (D2Q9) / 27 (D3Q27) with ScalarBGK;
  * cells per interior node: 0 bulk, 1 adiabatic, 2 Dirichlet, 3 excluded,
  * 4 moment (on-node Dirichlet), 5 outflow, 6 specular.  initialize_field
  * takes one value per PADDED node, as the reference's fn(n) does. */

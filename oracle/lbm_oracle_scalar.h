@@ -29,16 +29,32 @@ typedef struct {
 } SS(solver);
 
 /* ---- D2Q5 / D3Q7: src/lattice/Lattices.hpp:51-70, 100-121 ---- */
+/* (and the fluid lattices D2Q9 / D3Q27, which ScalarBGK also runs on) */
 static inline int SS(c)(const SS(solver)* s, int i, int a) {
-  return s->Q == 5 ? (a == 2 ? 0 : D2Q5_C[a][i]) : D3Q7_C[a][i];
+  switch (s->Q) {
+    case 5: return a == 2 ? 0 : D2Q5_C[a][i];
+    case 7: return D3Q7_C[a][i];
+    case 9: return a == 0 ? D2Q9_CX[i] : (a == 1 ? D2Q9_CY[i] : 0);
+    default: return a == 0 ? D3Q27_CX[i] : (a == 1 ? D3Q27_CY[i] : D3Q27_CZ[i]);
+  }
 }
 static inline R SS(w)(const SS(solver)* s, int i) {
-  return s->Q == 5 ? (R)D2Q5_W[i] / (R)6 : (R)D3Q7_W[i] / (R)8;
+  switch (s->Q) {
+    case 5: return (R)D2Q5_W[i] / (R)6;
+    case 7: return (R)D3Q7_W[i] / (R)8;
+    case 9: return (R)D2Q9_W[i] / (R)36;
+    default: return (R)D3Q27_W[i] / (R)216;
+  }
 }
-static inline R SS(cs2)(const SS(solver)* s) { return s->Q == 5 ? (R)1 / (R)3 : (R)1 / (R)4; }
-static inline R SS(ics2)(const SS(solver)* s) { return s->Q == 5 ? (R)3 / (R)1 : (R)4 / (R)1; }
+static inline R SS(cs2)(const SS(solver)* s) { return s->Q == 7 ? (R)1 / (R)4 : (R)1 / (R)3; }
+static inline R SS(ics2)(const SS(solver)* s) { return s->Q == 7 ? (R)4 / (R)1 : (R)3 / (R)1; }
 static inline int SS(mir)(const SS(solver)* s, int a, int i) {
-  return s->Q == 5 ? D2Q5_MIR[a][i] : D3Q7_MIR[a][i];
+  switch (s->Q) {
+    case 5: return D2Q5_MIR[a][i];
+    case 7: return D3Q7_MIR[a][i];
+    case 9: return D2Q9_MIR[a][i];
+    default: return D3Q27_MIR[a][i];
+  }
 }
 
 static inline long long SS(idp)(const SS(solver)* s, int x, int y, int z) {
@@ -62,7 +78,7 @@ static inline int SS(shift)(int v, int h, int n, int sz, int per) {
   if (v >= sz) return sz - 1;
   return v;
 }
-static void SS(neighbours)(const SS(solver)* s, long long n, long long nb[7]) {
+static void SS(neighbours)(const SS(solver)* s, long long n, long long nb[27]) {
   int x, y, z;
   SS(coords)(s, n, &x, &y, &z);
   for (int i = 1; i < s->Q; i += 2)
@@ -152,7 +168,7 @@ static void SS(impose_moment)(const SS(solver)* s, R* g, R target, uint32_t unkn
     if (unknown & (1u << i)) g[i] = deficit * SS(w)(s, i) / wsum;
 }
 static void SS(mirror_faces)(const SS(solver)* s, R* f, uint8_t faces) {
-  R h[7];
+  R h[27];
   for (int i = 0; i < s->Q; ++i) h[i] = f[i];
   for (int i = 0; i < s->Q; ++i) {
     int j = i, unknown = 0;
@@ -167,10 +183,11 @@ static void SS(mirror_faces)(const SS(solver)* s, R* f, uint8_t faces) {
 /* ---- ScalarSolver (src/solver/ScalarSolver.hpp) ---- */
 void* SF(create)(int lattice, int op, int nx, int ny, int nz, int px, int py, int pz, double omega,
                  double T_ref, double Lambda) {
-  if ((lattice != 5 && lattice != 7) || op < 1 || op > 3) return 0;
-  if (lattice == 5 && nz != 1) return 0;
+  if ((lattice != 5 && lattice != 7 && lattice != 9 && lattice != 27) || op < 1 || op > 3) return 0;
+  if ((lattice == 5 || lattice == 9) && nz != 1) return 0;
+  if ((lattice == 9 || lattice == 27) && op != 1) return 0;   /* TRT / regularised: axis-pair lattices */
   SS(solver)* s = (SS(solver)*)calloc(1, sizeof(SS(solver)));
-  s->lattice = lattice; s->Q = lattice; s->D = lattice == 5 ? 2 : 3; s->op = op;
+  s->lattice = lattice; s->Q = lattice; s->D = (lattice == 5 || lattice == 9) ? 2 : 3; s->op = op;
   s->nx = nx; s->ny = ny; s->nz = nz;
   s->per[0] = px != 0; s->per[1] = py != 0; s->per[2] = pz != 0;
   s->hx = (nx <= 1 || s->per[0]) ? 0 : 1;
@@ -350,7 +367,7 @@ void SF(finalize_geometry)(void* h) {
 void SF(initialize_field)(void* h, const double* T) {
   SS(solver)* s = (SS(solver)*)h;
   s->t = 0;
-  long long nb[7];
+  long long nb[27];
   for (long long n = 0; n < s->n_padded; ++n) {
     SS(neighbours)(s, n, nb);
     const R Tn = (s->flags[n] == SB_DIRICHLET) ? s->wall[n] : (R)T[n];
@@ -374,8 +391,8 @@ void SF(step)(void* h, int nsteps) {
     for (long long n = 0; n < s->n_padded; ++n) {
       const uint8_t flag = s->flags[n];
       if (flag == SB_EXCLUDED || flag == SB_OUTFLOW || flag == SB_ADIABATIC) continue;
-      long long nb[7];
-      R g[7];
+      long long nb[27];
+      R g[27];
       SS(neighbours)(s, n, nb);
       SS(load_all)(s, par, n, nb, g);
       const R vx = s->have_u ? s->ux[n] : (R)0;
@@ -391,7 +408,7 @@ void SF(step)(void* h, int nsteps) {
       }
       if (flag == SB_DIRICHLET) {
         const R Tw = s->wall[n] - s->T_ref;
-        R o[7];
+        R o[27];
         o[0] = -g[0] + (R)2 * SS(w)(s, 0) * Tw;
         for (int i = 1; i < s->Q; i += 2) {
           o[i] = -g[i + 1] + (R)2 * SS(w)(s, i) * Tw;
@@ -411,13 +428,13 @@ void SF(step)(void* h, int nsteps) {
         if (s->flags[n] != SB_OUTFLOW) continue;
         const long long src = s->don[n];
         if (src == n) continue;
-        long long nb[7];
+        long long nb[27];
         SS(neighbours)(s, n, nb);
         const R dT = s->field[src] - s->T_ref;
         const R vx = s->have_u ? s->ux[n] : (R)0;
         const R vy = s->have_u ? s->uy[n] : (R)0;
         const R vz = s->have_u ? s->uz[n] : (R)0;
-        R o[7];
+        R o[27];
         for (int i = 0; i < s->Q; ++i) o[i] = SS(eq)(s, i, dT, vx, vy, vz);
         SS(store_all)(s, par, n, nb, o);
         s->field[n] = s->T_ref + dT;
@@ -429,7 +446,7 @@ void SF(step)(void* h, int nsteps) {
 void SF(add_source)(void* h, const double* dC) {
   SS(solver)* s = (SS(solver)*)h;
   const int par = (int)(s->t % 2);
-  long long nb[7];
+  long long nb[27];
   for (int z = 0; z < s->nz; ++z)
     for (int y = 0; y < s->ny; ++y)
       for (int x = 0; x < s->nx; ++x) {
@@ -449,14 +466,14 @@ void SF(add_source)(void* h, const double* dC) {
 void SF(compute_field)(void* h) {
   SS(solver)* s = (SS(solver)*)h;
   const int par = (int)(s->t % 2);
-  long long nb[7];
+  long long nb[27];
   for (long long n = 0; n < s->n_padded; ++n) {
     const uint8_t flag = s->flags[n];
     if (flag == SB_EXCLUDED) { s->field[n] = 0; continue; }
     if (flag == SB_DIRICHLET || flag == SB_MOMENT) { s->field[n] = s->wall[n]; continue; }
     if (flag == SB_ADIABATIC) { s->field[n] = 0; continue; }
     if (flag == SB_OUTFLOW) continue;
-    R g[7];
+    R g[27];
     SS(neighbours)(s, n, nb);
     SS(load_all)(s, par, n, nb, g);
     if (flag == SB_SPECULAR) SS(mirror_faces)(s, g, s->spec[n]);
@@ -482,7 +499,7 @@ double SF(total)(void* h) {
 void SF(gather)(void* h, double* out) {
   SS(solver)* s = (SS(solver)*)h;
   const int par = (int)(s->t % 2);
-  long long nb[7];
+  long long nb[27];
   for (long long n = 0; n < s->n_padded; ++n) {
     SS(neighbours)(s, n, nb);
     for (int i = 0; i < s->Q; ++i) out[n * s->Q + i] = (double)*SS(slot)(s, par, n, nb, i);

@@ -145,15 +145,25 @@ SBase* make_scalar(int op, const Domain& d, double omega, double T_ref, double L
   }
 }
 
+// ScalarBGK on the fluid lattices (ScalarTRT / ScalarRegularised need the
+// axis-pair lattices and do not compile for these).
+template <class L>
+SBase* make_scalar_bgk(int op, const Domain& d, double omega, double T_ref, double Lambda) {
+  return op == 1 ? new SImpl<L, ScalarBGK<L>>(d, omega, T_ref, Lambda) : nullptr;
+}
+
 }  // namespace refdrv
 
 extern "C" {
-// lattice 5 (D2Q5) or 7 (D3Q7); op 1 ScalarBGK, 2 ScalarTRT, 3 ScalarRegularised.
+// lattice 5 (D2Q5) or 7 (D3Q7); op 1 ScalarBGK, 2 ScalarTRT, 3 ScalarRegularised;
+// lattice 9 (D2Q9) / 27 (D3Q27) with ScalarBGK.
 void* ref_screate(int lattice, int op, int nx, int ny, int nz, int px, int py, int pz,
                   double omega, double T_ref, double Lambda) {
   const Domain d(nx, ny, nz, px != 0, py != 0, pz != 0);
   if (lattice == 5 && nz == 1) return refdrv::make_scalar<D2Q5>(op, d, omega, T_ref, Lambda);
   if (lattice == 7) return refdrv::make_scalar<D3Q7>(op, d, omega, T_ref, Lambda);
+  if (lattice == 9 && nz == 1) return refdrv::make_scalar_bgk<D2Q9>(op, d, omega, T_ref, Lambda);
+  if (lattice == 27) return refdrv::make_scalar_bgk<D3Q27>(op, d, omega, T_ref, Lambda);
   return nullptr;
 }
 void ref_sdestroy(void* h) { delete static_cast<refdrv::SBase*>(h); }

@@ -20,7 +20,8 @@ from pathlib import Path
 HERE = Path(__file__).resolve().parent
 ROOT = HERE.parent.parent
 OUT = HERE / "validation"
-PROGRAMS = ["specular", "specular_node", "specwall_unsteady", "regularized", "cavity"]
+PROGRAMS = ["specular", "specular_node", "specwall_unsteady", "regularized", "cavity", "thermal",
+            "natural_convection", "scalar_walls", "scalar_specular", "gaussian_plume", "scalar_mass"]
 
 
 def main(names):

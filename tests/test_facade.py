@@ -204,3 +204,29 @@ def test_reference_cavity_validation_on_device(cuda_device):
     assert len(got) == len(want) > 10
     for a, b in zip(got, want):
         np.testing.assert_allclose([float(v) for v in a], [float(v) for v in b], atol=2e-5)
+
+
+# Scalar and thermal validations: every number the device run prints equals
+# the reference's to 1e-6 relative, or to 1e-11 absolute where the figure is
+# a round-off residual.
+def _all_figures(text):
+    rows = [ln for ln in text.splitlines() if ln.strip() and "backend" not in ln]
+    return [[float(v) for v in re.findall(r"[-+]?\d+\.?\d*(?:e[-+]?\d+)?", ln)] for ln in rows]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["thermal", "natural_convection", "scalar_walls", "scalar_specular",
+                                  "scalar_mass", "gaussian_plume"])
+def test_reference_scalar_validation_on_device(cuda_device, name):
+    """validation/{thermal, natural_convection, scalar_walls, scalar_specular,
+    scalar_mass, gaussian_plume}.cpp built against the facade: the D2Q5 / D3Q7
+    scalar solver, its walls, sources and outflow, and the Boussinesq-coupled
+    de Vahl Davis cavity (Nusselt numbers and step counts) as the reference
+    prints them."""
+    rc, out, ref = _validation(name)
+    assert rc == 0, out
+    assert "FAIL" not in out
+    got, want = _all_figures(out), _all_figures(ref)
+    assert len(got) == len(want)
+    for a, b in zip(got, want):
+        np.testing.assert_allclose(a, b, rtol=1e-6, atol=1e-11)

@@ -27,7 +27,7 @@ SCOLL = {"bgk": S.ScalarBGK, "trt": S.ScalarTRT, "regularised": S.ScalarRegulari
 def _scalar_pair(lat, op, shape, kind, om, prec, T_ref):
     nx, ny, nz = shape
     per = G.SCALAR_PERIODIC[kind]
-    L = S.D2Q5 if lat == 5 else S.D3Q7
+    L = {5: S.D2Q5, 7: S.D3Q7, 9: S.D2Q9, 27: S.D3Q27}[lat]
     gpu = S.ScalarSolver(S.Domain(nx, ny, nz, *per), SCOLL[op](L, omega=om, T_ref=T_ref), storage=prec)
     cpu = O.ScalarCpuSolver("oracle", lattice=lat, op=op, nx=nx, ny=ny, nz=nz, px=per[0], py=per[1],
                             pz=per[2], omega=om, T_ref=T_ref, precision=prec)
@@ -91,13 +91,13 @@ def _check(out, prec, nodes):
 
 
 @pytest.mark.parametrize("kind", list(G.SCALAR_PERIODIC))
-@pytest.mark.parametrize("lat", [5, 7])
-@pytest.mark.parametrize("op", ["bgk", "trt", "regularised"])
+@pytest.mark.parametrize("lat,op", [(5, "bgk"), (5, "trt"), (5, "regularised"), (7, "bgk"),
+                                    (7, "trt"), (7, "regularised"), (9, "bgk"), (27, "bgk")])
 @pytest.mark.parametrize("prec", ["f32", "f64"])
 @pytest.mark.parametrize("extras", [(0.0, False, False), (0.5, True, True)])
 def test_scalar_matches_oracle(cuda_device, kind, lat, op, prec, extras):
     T_ref, omf, src = extras
-    shape = (10, 9, 1) if lat == 5 else (8, 7, 5)
+    shape = (10, 9, 1) if lat in (5, 9) else (8, 7, 5)
     out = _run_both((lat, op, shape, kind, 1.2, 9, prec), 3, T_ref=T_ref, omega_field=omf, source=src)
     _check(out, prec, int(np.prod(shape)) * lat)
 
