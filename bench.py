@@ -264,7 +264,63 @@ def gpu_arm(args, rank, world, dist):
         out["serving"] = serving_arm(args)
     if rank == 0 and world == 1 and args.walls_steps > 0:
         out["walls"] = walls_arm(args, stream, omega)
+    if rank == 0 and world == 1 and args.thermal_steps > 0:
+        out["thermal"] = thermal_arm(args, stream, omega)
     return out
+
+
+def thermal_arm(args, stream, omega):
+    """The coupled thermal step on the headline lattice: the D3Q27 CM fluid
+    with a Boussinesq force read from a D3Q7 BGK temperature lattice (FP32),
+    which is advected by the fluid's stored velocity (m3lb_couple_thermal;
+    the reference's validation/rayleigh_benard.cpp loop: fluid.step(true);
+    scalar.step()).  Periodic box, temperature seeded with a random field.
+    Timed: the coupled pair, and the scalar step alone; the scalar kernel's
+    algorithmic bytes per node are 7 x 4 x 2 (populations) + 12 (velocity)
+    + 4 (field) + 1 (cell type)."""
+    import torch
+    from m3lb_b200 import capi
+    from m3lb_b200 import solver as S
+
+    n = args.size
+    K = args.thermal_steps
+    dom = S.Domain(n, n, n, True, True, True)
+    coll = S.CentralMoments(S.D3Q27, S.Guo(0.0, 0.0, 0.0), S.ShiftedPopulations, omega=omega)
+    fl = S.FluidSolver(dom, coll, storage=args.storage)
+    fl.set_stream(stream)
+    fl.set_option(capi.OPT_KERNEL, KERNELS[args.kernel])
+    th = S.ScalarSolver(dom, S.ScalarBGK(S.D3Q7, omega=1.2), storage="f32")
+    rng = np.random.default_rng(0)
+    th.initialize_field(0.5 + 0.01 * rng.standard_normal(dom.n_padded))
+    fl.initialize(1.0)
+    S.couple_thermal(fl, th, g=(0.0, 1.0, 0.0), rho0=1.0, beta=1e-3, T0=0.5)
+    for _ in range(3):
+        fl.step(True)
+        th.step()
+    e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(K):
+        fl.step(True)
+        th.step()
+    e1.record(stream)
+    th.steps(K)
+    e2.record(stream)
+    torch.cuda.synchronize()
+    pair_ms = e0.elapsed_time(e1) / K
+    scalar_ms = e1.elapsed_time(e2) / K
+    th.compute_field()
+    finite = bool(np.isfinite(th.temperature()).all())
+    th.close()
+    fl.close()
+    nodes = n ** 3
+    sbytes = 7 * 4 * 2 + 12 + 4 + 1
+    return {"workload": f"D3Q27 CM {n}^3 {args.storage} + D3Q7 BGK FP32 temperature, Boussinesq "
+                        f"coupling both ways, {K} steps",
+            "coupled_ms_per_step": pair_ms, "coupled_glups": nodes / pair_ms / 1e6,
+            "scalar_ms_per_step": scalar_ms, "scalar_glups": nodes / scalar_ms / 1e6,
+            "scalar_bytes_per_node": sbytes,
+            "scalar_hbm_gbs": nodes * sbytes / scalar_ms / 1e6, "finite": finite}
 
 
 def walls_arm(args, stream, omega):
@@ -570,6 +626,8 @@ def main():
     ap.add_argument("--serve-round", type=int, default=100)
     ap.add_argument("--walls-steps", type=int, default=100,
                     help="steps of each wall-cost measurement (0: skip it)")
+    ap.add_argument("--thermal-steps", type=int, default=100,
+                    help="steps of the coupled thermal measurement (0: skip it)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -185,8 +185,7 @@ int m3lb_set_outflow_density(m3lb_solver* h, double rho);
  * parcel is pushed, and T a device array of one value per interior node (x
  * fastest) in the solver's arithmetic type (FP64 for FP64 storage, else
  * FP32), read at every step; NULL returns to the uniform force.  Needs a
- * solver created with forcing.  While it is set the step runs in the paired
- * or the one-node kernel. */
+ * solver created with forcing. */
 int m3lb_set_buoyancy(m3lb_solver* h, const void* T, double gx, double gy, double gz, double rho0,
                       double beta, double T0);
 /* The same with T given on the host (doubles per interior node), copied to a
@@ -301,7 +300,8 @@ int m3lb_scalar_create(int lattice, int nx, int ny, int nz, int px, int py, int 
 int m3lb_scalar_destroy(m3lb_scalar* h);
 /* ScalarBGK::omega, T_ref (the storage reference, 0 = raw), ScalarTRT::Lambda. */
 int m3lb_scalar_set_params(m3lb_scalar* h, double omega, double T_ref, double Lambda);
-/* Queue the handle's work on `stream` (NULL: on the handle's own stream). */
+/* Queue the handle's work on `stream` (NULL: the default stream), as
+ * m3lb_set_stream does for a fluid handle. */
 int m3lb_scalar_set_stream(m3lb_scalar* h, void* stream);
 /* set_geometry(fn -> ScalarCell) (:92-99): cell types 0..6 per interior node. */
 int m3lb_scalar_set_cells(m3lb_scalar* h, const uint8_t* cells);

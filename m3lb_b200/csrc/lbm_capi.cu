@@ -114,8 +114,8 @@ struct m3lb_solver {
   int lattice = 27, Q = 27, op = 0, eq = 0, storage = 0, shifted = 1, forcing = 0;
   Geo g{};
   int device = 0;
-  cudaStream_t stream = nullptr;
-  bool own_stream = false;
+  cudaStream_t stream = nullptr;     // where the work is queued
+  cudaStream_t own = nullptr;        // the stream the handle created
   void* f = nullptr;                 // populations
   size_t f_bytes = 0;
   uint8_t* flags = nullptr;          // per padded node
@@ -163,8 +163,6 @@ struct m3lb_solver {
   bool chunk_ok() const { return g.px && g.hx == 0 && (g.nx % 2) == 0; }
   int step_kernel() const {
     if (node_kernel || !chunk_ok() || kernel == M3LB_KERNEL_NODES) return kKernelNodes;
-    // a per-node (Boussinesq) force runs in the paired kernel
-    if (forcing && temp) return kKernelPairs;
     // the streamed kernel addresses rows with 32-bit element counts
     const bool rows32 = (long long)g.nch * Q * 64 < (1LL << 31);
     // the row kernel: whole rows of at most 8 full chunks
@@ -239,9 +237,9 @@ int m3lb_create(int lattice, int nx, int ny, int nz, int px, int py, int pz, int
   h->err = reinterpret_cast<int*>(h->red_out + kReduceVals);
   if (cudaMemset(h->err, 0, sizeof(int)) != cudaSuccess)
     return cleanup(fail(M3LB_ERR_CUDA, "create: cannot clear the status word"));
-  if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess)
+  if (cudaStreamCreateWithFlags(&h->own, cudaStreamNonBlocking) != cudaSuccess)
     return cleanup(fail(M3LB_ERR_CUDA, "create: cannot create stream"));
-  h->own_stream = true;
+  h->stream = h->own;
 
   // Every interior node Fluid, halo Excluded (FluidSolver.hpp:57-63).
   h->flags_host.assign((size_t)h->g.n_padded, 0);
@@ -269,7 +267,9 @@ int m3lb_create(int lattice, int nx, int ny, int nz, int px, int py, int pz, int
 int m3lb_destroy(m3lb_solver* h) {
   if (!h) return M3LB_OK;
   DeviceGuard dg(h->device);
-  if (h->stream) cudaStreamSynchronize(h->stream);
+  // the queue may be a caller's stream, possibly gone already: wait for the
+  // whole device rather than for that stream
+  cudaDeviceSynchronize();
   cudaFree(h->f);
   cudaFree(h->flags);
   cudaFree(h->temp_own);
@@ -277,7 +277,7 @@ int m3lb_destroy(m3lb_solver* h) {
   for (void* p : h->macro) cudaFree(p);
   cudaFree(h->staging);
   cudaFree(h->partials);
-  if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
+  if (h->own) cudaStreamDestroy(h->own);
   delete h;
   return M3LB_OK;
 }
@@ -780,12 +780,10 @@ int m3lb_populations(const m3lb_solver* h, void** ptr, size_t* bytes) {
 int m3lb_set_stream(m3lb_solver* h, void* stream) {
   if (!h) return fail(M3LB_ERR_INVALID, "set_stream: null handle");
   DeviceGuard dg(h->device);
-  if (h->own_stream && h->stream) {
-    cudaStreamSynchronize(h->stream);
-    cudaStreamDestroy(h->stream);
-  }
+  // the handle's own stream stays alive until the handle is destroyed: other
+  // work may have been ordered after it (m3lb_stream_order)
+  if (h->stream) cudaStreamSynchronize(h->stream);
   h->stream = static_cast<cudaStream_t>(stream);
-  h->own_stream = false;
   return M3LB_OK;
 }
 int m3lb_sync(m3lb_solver* h) {

@@ -380,7 +380,17 @@ step_rows(StepArgs a, const __grid_constant__ RowMaps<L> maps) {
       V f[Q];
 #pragma unroll
       for (int q = 0; q < Q; ++q) f[q] = WO::unpack(w[q]);
-      m = collide<L, OP, EQ, SH, FORCE>(f, prm);
+      if constexpr (FORCE) {  // the force per node of the pair (Boussinesq)
+        CollideParams<S, V> pv{prm.omega, prm.omega2, bc<V>(prm.fx), bc<V>(prm.fy), bc<V>(prm.fz)};
+        if (a.temp) {
+          const S* T = reinterpret_cast<const S*>(a.temp);
+          const size_t kk = ((size_t)cur.zi * g.ny + cur.yi) * g.nx + x0;
+          buoyant_force<V>(a, pack2(T[kk], T[kk + 1]), pv.fx, pv.fy, pv.fz);
+        }
+        m = collide<L, OP, EQ, SH, FORCE>(f, pv);
+      } else {
+        m = collide<L, OP, EQ, SH, FORCE>(f, prm);
+      }
 #pragma unroll
       for (int q = 0; q < Q; ++q) w[q] = WO::pack(f[q]);
     } else {  // pure streaming reports rest: rho 1, u 0 (the no-collision mock)

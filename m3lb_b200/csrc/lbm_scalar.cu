@@ -469,6 +469,8 @@ struct m3lb_scalar {
   const void* uy = nullptr;
   const void* uz = nullptr;
   void* u_own = nullptr;          // m3lb_scalar_set_velocity_host's copy (3 arrays)
+  void* src = nullptr;            // m3lb_scalar_add_source's array on the device
+  std::vector<double> src_host;   // ... and what it holds
   void* scratch = nullptr;        // host-array uploads and the source array
   size_t scratch_bytes = 0;
   double* partials = nullptr;     // total: per-block sums, then the result
@@ -598,7 +600,7 @@ int m3lb_scalar_destroy(m3lb_scalar* h) {
   // for the whole device rather than for that stream
   cudaDeviceSynchronize();
   for (void* p : {h->f, (void*)h->cells, (void*)h->spec, (void*)h->unk, h->wall, h->field, h->omega_of,
-                  h->u_own, h->scratch, (void*)h->partials, (void*)h->out_nodes, (void*)h->out_donor})
+                  h->u_own, h->src, h->scratch, (void*)h->partials, (void*)h->out_nodes, (void*)h->out_donor})
     cudaFree(p);
   if (h->own) cudaStreamDestroy(h->own);
   delete h;
@@ -615,9 +617,9 @@ int m3lb_scalar_set_stream(m3lb_scalar* h, void* stream) {
   if (!h) return sfail(M3LB_ERR_INVALID, "scalar_set_stream: null handle");
   SGuard dg(h->device);
   if (h->stream) cudaStreamSynchronize(h->stream);
-  // the handle's own stream lives until the handle does: callers may still
-  // order other work after it
-  h->stream = stream ? (cudaStream_t)stream : h->own;
+  // as m3lb_set_stream: NULL is the default stream; the handle's own stream
+  // lives until the handle does, as callers may still order work after it
+  h->stream = (cudaStream_t)stream;
   return M3LB_OK;
 }
 
@@ -868,11 +870,18 @@ int m3lb_scalar_step(m3lb_scalar* h, int nsteps) {
 int m3lb_scalar_add_source(m3lb_scalar* h, const double* dC) {
   if (!h || !dC) return sfail(M3LB_ERR_INVALID, "scalar_add_source: null argument");
   SGuard dg(h->device);
-  void* d = nullptr;
-  int rc = upload_real(h, dC, (size_t)h->nint(), &d);
-  if (rc) return rc;
-  S_TRY(h->T->source(h->args(), d, h->stream));
-  S_TRY(cudaStreamSynchronize(h->stream));
+  const size_t n = (size_t)h->nint();
+  // a source repeated step after step is copied to the device once
+  if (!h->src || h->src_host.size() != n || std::memcmp(h->src_host.data(), dC, n * 8) != 0) {
+    int rc = ensure(&h->src, n * h->rb());
+    if (rc) return rc;
+    void* d = nullptr;
+    rc = upload_real(h, dC, n, &d);
+    if (rc) return rc;
+    S_TRY(cudaMemcpyAsync(h->src, d, n * h->rb(), cudaMemcpyDeviceToDevice, h->stream));
+    h->src_host.assign(dC, dC + n);
+  }
+  S_TRY(h->T->source(h->args(), h->src, h->stream));
   h->launches += 1;
   return M3LB_OK;
 }

@@ -381,7 +381,17 @@ step_stream(StepArgs a) {
       V f[Q];
 #pragma unroll
       for (int q = 0; q < Q; ++q) f[q] = WO::unpack(w[q]);
-      m = collide<L, OP, EQ, SH, FORCE>(f, prm);
+      if constexpr (FORCE) {  // the force per node of the pair (Boussinesq)
+        CollideParams<S, V> pv{prm.omega, prm.omega2, bc<V>(prm.fx), bc<V>(prm.fy), bc<V>(prm.fz)};
+        if (a.temp) {
+          const S* T = reinterpret_cast<const S*>(a.temp);
+          const size_t kk = ((size_t)cur.zi * g.ny + cur.yi) * g.nx + lx.x0;
+          buoyant_force<V>(a, lx.active ? pack2(T[kk], T[kk + 1]) : bc<V>(S(0)), pv.fx, pv.fy, pv.fz);
+        }
+        m = collide<L, OP, EQ, SH, FORCE>(f, pv);
+      } else {
+        m = collide<L, OP, EQ, SH, FORCE>(f, prm);
+      }
 #pragma unroll
       for (int q = 0; q < Q; ++q) w[q] = WO::pack(f[q]);
     } else {  // pure streaming reports rest: rho 1, u 0 (the no-collision mock)

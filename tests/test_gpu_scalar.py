@@ -175,6 +175,36 @@ def test_buoyancy_matches_oracle(cuda_device, lat, op, eq, om2, storage, kernel)
     c.close()
 
 
+@pytest.mark.parametrize("kernel", [capi.KERNEL_NODES, capi.KERNEL_STREAM, capi.KERNEL_ROWS])
+def test_buoyancy_same_under_every_bulk_kernel(cuda_device, kernel):
+    """64-wide periodic rows with walls: the row and streamed kernels apply the
+    per-node force as the paired kernel does, bit for bit; the one-node
+    kernel's moment operator agrees to a few ulp (test_gpu_parity.py)."""
+    out = []
+    for k in (capi.KERNEL_PAIRS, kernel):
+        coll = S.CentralMoments(S.D3Q27, S.Guo(1e-5, 0.0, 0.0), S.ShiftedPopulations, omega=1.6)
+        s = S.FluidSolver(S.Domain(64, 6, 4, True, False, True), coll, storage="f16")
+        s.set_option(capi.OPT_KERNEL, k)
+        fl = np.zeros((4, 6, 64), np.uint8)
+        fl[:, 0, :] = 1
+        s.set_geometry(fl)
+        s.initialize(1.0, 0.01, 0.0, 0.0)
+        rng = np.random.default_rng(2)
+        T = torch.as_tensor(rng.standard_normal((4, 6, 64)), dtype=torch.float32, device="cuda")
+        torch.cuda.synchronize()
+        s.set_buoyancy(T, g=(0.0, 1.0, 0.3), beta=1e-3)
+        s.steps(6, True)
+        out.append((s.gather_populations(), s.stored_macroscopic()))
+        s.close()
+    if kernel == capi.KERNEL_NODES:
+        scale = float(np.max(np.abs(out[0][0])))
+        assert float(np.max(np.abs(out[0][0] - out[1][0]))) <= 8 * EPS["f16"] * scale
+        return
+    np.testing.assert_array_equal(out[0][0], out[1][0])
+    for a, b in zip(out[0][1], out[1][1]):
+        np.testing.assert_array_equal(a, b)
+
+
 def test_buoyancy_needs_forcing(cuda_device):
     coll = S.BGK(lattice=S.D3Q27, storage=S.ShiftedPopulations, omega=1.2)
     s = S.FluidSolver(S.Domain(8, 6, 4), coll, storage="f32")
