@@ -288,7 +288,8 @@ int m3lb_reduce_static(int lattice, int nx, int ny, int nz, int px, int py, int 
  * flux), 2 Dirichlet (anti-bounce-back to the wall value), 3 excluded,
  * 4 moment (the wall value imposed ON the node, MomentDirichlet.hpp), 5
  * outflow (equilibrium at a bulk donor's value), 6 specular (on-node zero
- * flux, with faces from the two specular calls). */
+ * flux, with faces from the two specular calls).  ny and nz are at most
+ * 65535. */
 typedef struct m3lb_scalar m3lb_scalar;
 
 #define M3LB_SOP_BGK 1

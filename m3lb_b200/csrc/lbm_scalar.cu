@@ -50,6 +50,56 @@ __device__ __forceinline__ void coords_of(const Geo& g, long long k, int& x, int
   y = (int)((k / g.nx) % g.ny) + g.hy;
   z = (int)(k / ((long long)g.nx * g.ny)) + g.hz;
 }
+// The per-node kernels run a 3-D grid: blockIdx.x the x segment of a row,
+// blockIdx.y and blockIdx.z the row's y and z, so a node's coordinates need
+// no division (ny and nz are at most 65535, checked at creation).
+__device__ __forceinline__ bool row_node(const Geo& g, long long& k, int& x, int& y, int& z) {
+  const int xi = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  if (xi >= g.nx) return false;
+  const int yi = (int)blockIdx.y, zi = (int)blockIdx.z;
+  k = ((long long)zi * g.ny + yi) * g.nx + xi;
+  x = xi + g.hx; y = yi + g.hy; z = zi + g.hz;
+  return true;
+}
+inline dim3 row_grid(const Geo& g, int threads) {
+  return dim3((unsigned)((g.nx + threads - 1) / threads), (unsigned)g.ny, (unsigned)g.nz);
+}
+
+// Element offsets from a node's slot to the same slot of the neighbour one
+// step down [0] or up [1] each axis (shift_coord's wrap or clamp).  A slot is
+// ((z sy + y) nch + x/64) Q 64 + q 64 + x%64, so a neighbour's address is the
+// node's own plus one offset per nonzero velocity component.
+template <int Q>
+struct AxisSteps {
+  long long x[2], y[2], z[2];
+};
+template <int Q>
+__device__ __forceinline__ long long x_part(int v) {
+  return ((long long)(v >> 6) * Q << 6) + (v & 63);
+}
+template <int Q>
+__device__ __forceinline__ AxisSteps<Q> axis_steps(const Geo& g, int x, int y, int z) {
+  AxisSteps<Q> s;
+  const long long row = (long long)g.nch * Q * kChunk, plane = row * g.sy;
+#pragma unroll
+  for (int u = 0; u < 2; ++u) {
+    const int d = 2 * u - 1;
+    s.x[u] = x_part<Q>(shift_coord(x + d, g.hx, g.nx, g.sx, g.px)) - x_part<Q>(x);
+    s.y[u] = (long long)(shift_coord(y + d, g.hy, g.ny, g.sy, g.py) - y) * row;
+    s.z[u] = (long long)(shift_coord(z + d, g.hz, g.nz, g.sz, g.pz) - z) * plane;
+  }
+  return s;
+}
+// Offset to the neighbour at x + c_I.
+template <class L, int I>
+__device__ __forceinline__ long long nb_offset(const AxisSteps<L::Q>& s) {
+  constexpr int cx = L::cx[I], cy = L::cy[I], cz = L::cz[I];
+  long long o = 0;
+  if constexpr (cx != 0) o += s.x[cx > 0];
+  if constexpr (cy != 0) o += s.y[cy > 0];
+  if constexpr (cz != 0) o += s.z[cz > 0];
+  return o;
+}
 
 // ScalarBGK::eq (ScalarBGK.hpp:43-49): w_i (dT + (T_ref + dT) c_i.u / cs2).
 template <class L, int I, class R>
@@ -135,33 +185,40 @@ __device__ __forceinline__ void velocity_at(const ScalarArgs& a, long long k, R&
 }
 
 // run_step<P> (ScalarSolver.hpp:302-372): one thread per interior node.
+// Every load a bulk node needs is issued before the cell type is examined
+// (each address is inside the lattice whatever the type), so a thread waits
+// for memory once.
 template <class L, int ST, int OP>
 __global__ void __launch_bounds__(kScalarThreads) scalar_step(ScalarArgs a) {
   using E = typename StoreT<ST>::elem;
   using R = typename StoreT<ST>::real;
   constexpr int Q = L::Q;
   const Geo& g = a.g;
-  const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= (long long)g.nx * g.ny * g.nz) return;
+  long long k;
   int x, y, z;
-  coords_of(g, k, x, y, z);
+  if (!row_node(g, k, x, y, z)) return;
   const long long pn = ((long long)z * g.sy + y) * g.sx + x;
   const uint8_t cell = a.cells[pn];
+  const AxisSteps<Q> st = axis_steps<Q>(g, x, y, z);
+  E* own = reinterpret_cast<E*>(a.f) + slot<Q>(g, x, y, z, 0);
+  const int P = a.parity;
+  // direction i (odd) sits at slot i + P of the node, i + 1 at slot i + 1 - P
+  // of the neighbour along c_i
+  E* up = own + P * kChunk;
+  E* dn = own + (1 - P) * kChunk;
+  R h[Q];
+  h[0] = to_real(own[0]);
+  static_for<1, Q, 2>([&](auto I) {
+    constexpr int i = decltype(I)::value;
+    h[i] = to_real(up[i * kChunk]);
+    h[i + 1] = to_real(dn[nb_offset<L, i>(st) + i * kChunk]);
+  });
+  R vx, vy, vz;
+  velocity_at(a, k, vx, vy, vz);
+  const R w = a.omega_of ? reinterpret_cast<const R*>(a.omega_of)[k] : R(a.omega);
   // excluded: not simulated; outflow: second pass; adiabatic: bounce-back,
   // the identity on this storage
   if (cell == kSExcluded || cell == kSOutflow || cell == kSAdiabatic) return;
-  NodeNb<L> nb;
-  node_neighbours<L>(g, x, y, z, nb);
-  E* A = reinterpret_cast<E*>(a.f);
-  const int P = a.parity;
-  R h[Q];
-  h[0] = to_real(A[slot<Q>(g, x, y, z, 0)]);
-#pragma unroll
-  for (int i = 1; i < Q; i += 2) {
-    const int* m = nb.nb[i];
-    h[i] = to_real(A[slot<Q>(g, x, y, z, i + P)]);
-    h[i + 1] = to_real(A[slot<Q>(g, m[0], m[1], m[2], i + 1 - P)]);
-  }
   const R T_ref = R(a.T_ref);
   R* field = reinterpret_cast<R*>(a.field);
   if (cell == kSDirichlet) {  // anti-bounce-back toward the wall value
@@ -180,19 +237,15 @@ __global__ void __launch_bounds__(kScalarThreads) scalar_step(ScalarArgs a) {
     else if (cell == kSSpecular && a.spec)
       spec_node_mirror<L>(h, a.spec[pn]);
     const R dT = deviation<L>(h);
-    R vx, vy, vz;
-    velocity_at(a, k, vx, vy, vz);
-    const R w = a.omega_of ? reinterpret_cast<const R*>(a.omega_of)[k] : R(a.omega);
     s_collide<L, OP>(h, dT, vx, vy, vz, w, T_ref, R(a.Lambda));
     field[k] = T_ref + dT;
   }
-  A[slot<Q>(g, x, y, z, 0)] = from_real<E>(h[0]);
-#pragma unroll
-  for (int i = 1; i < Q; i += 2) {
-    const int* m = nb.nb[i];
-    A[slot<Q>(g, m[0], m[1], m[2], i + 1 - P)] = from_real<E>(h[i]);
-    A[slot<Q>(g, x, y, z, i + P)] = from_real<E>(h[i + 1]);
-  }
+  own[0] = from_real<E>(h[0]);
+  static_for<1, Q, 2>([&](auto I) {
+    constexpr int i = decltype(I)::value;
+    dn[nb_offset<L, i>(st) + i * kChunk] = from_real<E>(h[i]);
+    up[i * kChunk] = from_real<E>(h[i + 1]);
+  });
 }
 
 // outflow_kernel<P> (:393-419): equilibrium at the donor's value and the
@@ -237,10 +290,9 @@ __global__ void __launch_bounds__(kScalarThreads) scalar_field(ScalarArgs a) {
   using R = typename StoreT<ST>::real;
   constexpr int Q = L::Q;
   const Geo& g = a.g;
-  const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= (long long)g.nx * g.ny * g.nz) return;
+  long long k;
   int x, y, z;
-  coords_of(g, k, x, y, z);
+  if (!row_node(g, k, x, y, z)) return;
   const long long pn = ((long long)z * g.sy + y) * g.sx + x;
   const uint8_t cell = a.cells[pn];
   R* field = reinterpret_cast<R*>(a.field);
@@ -264,10 +316,9 @@ __global__ void __launch_bounds__(kScalarThreads) scalar_source(ScalarArgs a, co
   using E = typename StoreT<ST>::elem;
   using R = typename StoreT<ST>::real;
   const Geo& g = a.g;
-  const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= (long long)g.nx * g.ny * g.nz) return;
+  long long k;
   int x, y, z;
-  coords_of(g, k, x, y, z);
+  if (!row_node(g, k, x, y, z)) return;
   const uint8_t cell = a.cells[((long long)z * g.sy + y) * g.sx + x];
   if (cell != kSBulk && cell != kSSpecular) return;
   const R d = reinterpret_cast<const R*>(dC)[k];
@@ -362,8 +413,7 @@ inline unsigned blocks(long long n, int t) { return (unsigned)((n + t - 1) / t);
 template <class L, int ST>
 struct ScalarOps {
   static cudaError_t step(const ScalarArgs& a, int op, cudaStream_t s) {
-    const long long n = (long long)a.g.nx * a.g.ny * a.g.nz;
-    const unsigned b = blocks(n, kScalarThreads);
+    const dim3 b = row_grid(a.g, kScalarThreads);
     if (op == 1) {
       scalar_step<L, ST, 1><<<b, kScalarThreads, 0, s>>>(a);
     } else if constexpr (L::Q == 2 * L::D + 1) {  // TRT / regularised: axis-pair lattices
@@ -380,11 +430,11 @@ struct ScalarOps {
     return cudaGetLastError();
   }
   static cudaError_t field(const ScalarArgs& a, cudaStream_t s) {
-    scalar_field<L, ST><<<blocks((long long)a.g.nx * a.g.ny * a.g.nz, kScalarThreads), kScalarThreads, 0, s>>>(a);
+    scalar_field<L, ST><<<row_grid(a.g, kScalarThreads), kScalarThreads, 0, s>>>(a);
     return cudaGetLastError();
   }
   static cudaError_t source(const ScalarArgs& a, const void* dC, cudaStream_t s) {
-    scalar_source<L, ST><<<blocks((long long)a.g.nx * a.g.ny * a.g.nz, kScalarThreads), kScalarThreads, 0, s>>>(a, dC);
+    scalar_source<L, ST><<<row_grid(a.g, kScalarThreads), kScalarThreads, 0, s>>>(a, dC);
     return cudaGetLastError();
   }
   static cudaError_t init(const ScalarArgs& a, const void* Tpad, cudaStream_t s) {
@@ -554,6 +604,8 @@ int m3lb_scalar_create(int lattice, int nx, int ny, int nz, int px, int py, int 
   if ((lattice == 9 || lattice == 27) && op != M3LB_SOP_BGK)
     return sfail(M3LB_ERR_INVALID, "scalar_create: ScalarTRT and ScalarRegularised need D2Q5 or D3Q7");
   if (nx < 1 || ny < 1 || nz < 1) return sfail(M3LB_ERR_INVALID, "scalar_create: extents must be >= 1");
+  if (ny > 65535 || nz > 65535)
+    return sfail(M3LB_ERR_INVALID, "scalar_create: ny and nz must be at most 65535");
   if (op < M3LB_SOP_BGK || op > M3LB_SOP_REGULARISED)
     return sfail(M3LB_ERR_INVALID, "scalar_create: bad operator %d", op);
   if (storage != M3LB_STORE_F32 && storage != M3LB_STORE_F64)
