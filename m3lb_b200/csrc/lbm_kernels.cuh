@@ -190,10 +190,19 @@ constexpr int pair_min_blocks() {
   return ST == kF64 ? 2 : ((OP == 1 || OP == 2 || (OP == 0 && ST == kF32)) ? 3 : (OP >= 3 && ST != kF32 ? 5 : 4));
 }
 
-// One 64-node chunk (unit `warp` of the lattice's ny * nz * nch chunks) by
-// one warp.  Shared by the paired kernel and the batched kernel of the
-// serving loop, so a lattice gets the same arithmetic in both.
-template <class L, int ST, int OP, int EQ, bool SH, bool FORCE>
+// One unit of 64 nodes by one warp.  Shared by the paired kernel and the
+// batched kernel of the serving loop, so a lattice gets the same arithmetic
+// in both.  Two mappings of units to nodes:
+//   * chunks (DENSE false): unit `warp` is chunk (row, k) of the lattice's
+//     ny * nz * nch chunks; lane l holds x0 = 64 k + 2 l, idle past nx;
+//   * dense: unit `warp` is interior nodes 64 warp ... 64 warp + 63 in x-fastest
+//     order, rows of any even length packed back to back, so every lane
+//     works whatever nx is; a warp spans parts of several rows, each lane
+//     addresses its own row, and the x neighbour of a row's last pair (its
+//     first pair, periodic wrap) comes by shuffle when that pair is in the
+//     same warp, else from memory.
+// The per-node arithmetic, and so the result, is the same in both.
+template <class L, int ST, int OP, int EQ, bool SH, bool FORCE, bool DENSE = false>
 __device__ __forceinline__ void pairs_unit(const StepArgs& a, long long warp, int lane) {
   using WO = WordOps<ST>;
   using W = typename WO::W;
@@ -203,24 +212,60 @@ __device__ __forceinline__ void pairs_unit(const StepArgs& a, long long warp, in
   constexpr int Q = L::Q;
   const Geo& g = a.g;
 
-  const long long nrows = (long long)g.ny * g.nz;
-  const bool warp_ok = warp < nrows * g.nch;
-  const long long wsafe = warp_ok ? warp : 0;
-  const int row = (int)(wsafe / g.nch);
-  const int k = (int)(wsafe - (long long)row * g.nch);
-  const int x0 = k * kChunk + 2 * lane;
-  const int yi = row % g.ny, zi = row / g.ny;
+  int x0, yi, zi, k;
+  bool ok;
+  int nx_ = 0, px_ = 0;  // x0 + 2 and x0 - 2, wrapped
+  bool nxt_in, prv_in;
+  int nxt_src, prv_src;
+  if constexpr (DENSE) {
+    const long long nodes = (long long)g.nx * g.ny * g.nz;
+    const long long f0 = warp * kChunk;  // first node of the unit
+    ok = f0 + 2 * lane < nodes;
+    const long long fs = f0 < nodes ? f0 : 0;  // (a unit past the end addresses node 0)
+    const long long row0 = fs / g.nx;
+    const int xs = (int)(fs - row0 * g.nx);  // x of the unit's first node
+    int x = xs + 2 * lane, dr = 0;
+    while (x >= g.nx) { x -= g.nx; ++dr; }  // at most 64 / nx + 1 rows
+    const long long row = ok ? row0 + dr : row0;
+    yi = (int)(row % g.ny);
+    zi = (int)(row / g.ny);
+    x0 = ok ? x : 0;
+    k = x0 >> 6;
+    nx_ = x0 + 2; if (nx_ >= g.nx) nx_ -= g.nx;
+    px_ = x0 - 2; if (px_ < 0) px_ += g.nx;
+    // position inside the unit of an x of this lane's row
+    const int rs = dr * g.nx - xs;
+    const int pn = rs + nx_, pp = rs + px_;
+    nxt_in = pn >= 0 && pn < kChunk;
+    prv_in = pp >= 0 && pp < kChunk;
+    nxt_src = nxt_in ? (pn >> 1) : lane;
+    prv_src = prv_in ? (pp >> 1) : lane;
+  } else {
+    const long long nrows = (long long)g.ny * g.nz;
+    const bool warp_ok = warp < nrows * g.nch;
+    const long long wsafe = warp_ok ? warp : 0;
+    const int row = (int)(wsafe / g.nch);
+    k = (int)(wsafe - (long long)row * g.nch);
+    x0 = k * kChunk + 2 * lane;
+    yi = row % g.ny;
+    zi = row / g.ny;
+    ok = warp_ok && x0 < g.nx;
+    nx_ = x0 + 2; if (nx_ >= g.nx) nx_ -= g.nx;
+    px_ = x0 - 2; if (px_ < 0) px_ += g.nx;
+    nxt_in = (nx_ >> 6) == k;
+    prv_in = (px_ >> 6) == k;
+    nxt_src = nxt_in ? ((nx_ & 63) >> 1) : lane;
+    prv_src = prv_in ? ((px_ & 63) >> 1) : lane;
+  }
   const int py = yi + g.hy, pz = zi + g.hz;
 
   PairCtx<L, ST> c;
-  c.active = warp_ok && x0 < g.nx;
+  c.active = ok;
   {
-    int nx_ = x0 + 2; if (nx_ >= g.nx) nx_ -= g.nx;
-    int px_ = x0 - 2; if (px_ < 0) px_ += g.nx;
-    c.nxt_in = (nx_ >> 6) == k;
-    c.prv_in = (px_ >> 6) == k;
-    c.nxt_src = c.nxt_in ? ((nx_ & 63) >> 1) : lane;
-    c.prv_src = c.prv_in ? ((px_ & 63) >> 1) : lane;
+    c.nxt_in = nxt_in;
+    c.prv_in = prv_in;
+    c.nxt_src = nxt_src;
+    c.prv_src = prv_src;
     int xn = x0 + 2; if (xn >= g.nx) xn -= g.nx;
     int xp = x0 - 1; if (xp < 0) xp += g.nx;
     c.nxt_off = chunk_delta(Q, x0, xn);

@@ -52,8 +52,9 @@ constexpr int kBatchThreads = 128;
 constexpr int kMaxItems = 1024;  // lattices in one launch (shared-memory search table)
 
 // One time step of every lattice in `items` (all with operator OP): warp u
-// of the grid updates chunk u - first_unit of the item whose range holds u.
-template <int ST, int OP, int EQ>
+// of the grid updates unit u - first_unit of the item whose range holds u,
+// a chunk (DENSE false) or 64 consecutive nodes (DENSE true) of pairs_unit.
+template <int ST, int OP, int EQ, bool DENSE>
 __global__ void __launch_bounds__(kBatchThreads, pair_min_blocks<OP, ST>())
 batch_step(const BatchItem* __restrict__ items, int n_items, long long n_units, int s) {
   __shared__ long long first[kMaxItems];
@@ -68,7 +69,7 @@ batch_step(const BatchItem* __restrict__ items, int n_items, long long n_units, 
   }
   StepArgs a = items[lo].a;
   a.parity = (int)((items[lo].t0 + s) & 1);
-  pairs_unit<D3Q27, ST, OP, EQ, true, false>(a, u - first[lo], threadIdx.x & 31);
+  pairs_unit<D3Q27, ST, OP, EQ, true, false, DENSE>(a, u - first[lo], threadIdx.x & 31);
 }
 
 // Taylor-Green benchmark initial field (the analytic pressure in rho, w = 0)
@@ -89,21 +90,21 @@ __global__ void tgv_field_kernel(int n, double u0, float* rho, float* ux, float*
 
 using BatchFn = void (*)(const BatchItem*, int, long long, int);
 
-template <int ST>
+template <int ST, bool DENSE>
 BatchFn batch_fn_st(int op) {
   switch (op) {
-    case M3LB_OP_BGK: return batch_step<ST, 1, 0>;
-    case M3LB_OP_TRT: return batch_step<ST, 2, 0>;
-    case M3LB_OP_MRT: return batch_step<ST, 3, 0>;
-    case M3LB_OP_CM: return batch_step<ST, 4, 0>;
+    case M3LB_OP_BGK: return batch_step<ST, 1, 0, DENSE>;
+    case M3LB_OP_TRT: return batch_step<ST, 2, 0, DENSE>;
+    case M3LB_OP_MRT: return batch_step<ST, 3, 0, DENSE>;
+    case M3LB_OP_CM: return batch_step<ST, 4, 0, DENSE>;
     default: return nullptr;
   }
 }
-BatchFn batch_fn(int storage, int op) {
+BatchFn batch_fn(int storage, int op, bool dense = false) {
   switch (storage) {
-    case M3LB_STORE_F16: return batch_fn_st<kF16>(op);
-    case M3LB_STORE_BF16: return batch_fn_st<kBF16>(op);
-    case M3LB_STORE_F32: return batch_fn_st<kF32>(op);
+    case M3LB_STORE_F16: return dense ? batch_fn_st<kF16, true>(op) : batch_fn_st<kF16, false>(op);
+    case M3LB_STORE_BF16: return dense ? batch_fn_st<kBF16, true>(op) : batch_fn_st<kBF16, false>(op);
+    case M3LB_STORE_F32: return dense ? batch_fn_st<kF32, true>(op) : batch_fn_st<kF32, false>(op);
     default: return nullptr;
   }
 }
@@ -137,6 +138,7 @@ struct Lattice {
   size_t bytes = 0;         // admission footprint
   long long t = 0;          // time steps done
   long long units = 0;      // chunks per time step
+  long long dense_units = 0;  // 64-node units per time step (dense mapping)
   double admitted = 0;
 };
 
@@ -176,6 +178,7 @@ struct m3lb_server {
   int flip = 0;
   int n_items[4] = {0, 0, 0, 0};
   long long n_units[4] = {0, 0, 0, 0};
+  bool dense[4] = {false, false, false, false};  // unit mapping of each operator's launch
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t graph_exec = nullptr;
   long long set_version = 0, graph_version = -1;
@@ -259,6 +262,7 @@ int admit(m3lb_server* s, const m3lb_request& r, double t_now) {
   l.L = table_for(27, s->cfg.storage);
   l.bytes = footprint(s->cfg, r.n);
   l.units = (long long)l.g.ny * l.g.nz * l.g.nch;
+  l.dense_units = ((long long)r.n * r.n * r.n + kChunk - 1) / kChunk;
   l.admitted = t_now;
   int rc = ensure_zero_flags(s, l.g.n_padded);
   if (rc) return rc;
@@ -354,8 +358,22 @@ int retire_oldest(m3lb_server* s, Clock::time_point t0) {
 // now; returns through n_items / n_units.
 BatchItem* host_table(m3lb_server* s) { return s->items_host + (size_t)s->flip * 4 * kMaxItems; }
 
+// The unit mapping of one operator's launch: as configured, or (automatic)
+// dense when a lattice of it has rows that leave chunk lanes idle (N not a
+// multiple of 64), chunks otherwise (the two are the same then).
+void choose_mapping(m3lb_server* s) {
+  for (int o = 0; o < 4; ++o) s->dense[o] = s->cfg.mapping == M3LB_MAP_DENSE;
+  if (s->cfg.mapping != M3LB_MAP_AUTO) return;
+  for (const Lattice& l : s->active) {
+    int o = 0;
+    while (kOps[o] != l.req.op) ++o;
+    if (l.req.n % kChunk != 0) s->dense[o] = true;
+  }
+}
+
 void build_items(m3lb_server* s) {
   BatchItem* tab = host_table(s);
+  choose_mapping(s);
   for (int o = 0; o < 4; ++o) {
     s->n_items[o] = 0;
     s->n_units[o] = 0;
@@ -367,7 +385,7 @@ void build_items(m3lb_server* s) {
     it.a = lattice_args(s, l);
     it.first_unit = s->n_units[o];
     it.t0 = l.t;
-    s->n_units[o] += l.units;
+    s->n_units[o] += s->dense[o] ? l.dense_units : l.units;
   }
 }
 
@@ -375,7 +393,7 @@ int launch_round(m3lb_server* s, int R) {
   for (int step = 0; step < R; ++step)
     for (int o = 0; o < 4; ++o) {
       if (!s->n_items[o]) continue;
-      BatchFn fn = batch_fn(s->cfg.storage, kOps[o]);
+      BatchFn fn = batch_fn(s->cfg.storage, kOps[o], s->dense[o]);
       const long long threads = s->n_units[o] * 32;
       const unsigned blocks = (unsigned)((threads + kBatchThreads - 1) / kBatchThreads);
       void* args[4];
@@ -438,7 +456,10 @@ int run_round(m3lb_server* s, int R) {
   }
   for (Lattice& l : s->active) l.t += R;
   s->stats.rounds += 1;
-  for (int o = 0; o < 4; ++o) s->stats.launches += (long long)R * (s->n_items[o] ? 1 : 0);
+  for (int o = 0; o < 4; ++o) {
+    s->stats.launches += (long long)R * (s->n_items[o] ? 1 : 0);
+    s->stats.dense_launches += (long long)R * (s->n_items[o] && s->dense[o] ? 1 : 0);
+  }
   return M3LB_OK;
 }
 
@@ -459,6 +480,8 @@ int m3lb_serve_create(const m3lb_serve_config* cfg, m3lb_server** out) {
     return fail(M3LB_ERR_UNSUPPORTED, "serve_create: storage %d is not served (F16, BF16, F32)",
                 cfg->storage);
   if (cfg->round_steps < 1) return fail(M3LB_ERR_INVALID, "serve_create: round_steps must be >= 1");
+  if (cfg->mapping < M3LB_MAP_AUTO || cfg->mapping > M3LB_MAP_DENSE)
+    return fail(M3LB_ERR_INVALID, "serve_create: mapping must be M3LB_MAP_AUTO, _CHUNKS or _DENSE");
   auto* s = new m3lb_server();
   s->cfg = *cfg;
   cudaGetDevice(&s->device);

@@ -75,11 +75,13 @@ def offered_lups(reqs) -> float:
 class Server:
     """One serving loop on the current CUDA device."""
 
+    MAPPINGS = {"auto": capi.MAP_AUTO, "chunks": capi.MAP_CHUNKS, "dense": capi.MAP_DENSE}
+
     def __init__(self, hbm_budget: int = 4 << 30, max_resident: int = 32, round_steps: int = 50,
-                 storage: str = "f16", keep_fields: bool = False):
+                 storage: str = "f16", keep_fields: bool = False, mapping: str = "auto"):
         self.storage = capi.STORAGE_NAMES[storage]
         cfg = capi.ServeConfig(hbm_budget, max_resident, round_steps, self.storage,
-                               int(keep_fields))
+                               int(keep_fields), self.MAPPINGS[mapping])
         h = C.c_void_p()
         capi.check(capi.lib().m3lb_serve_create(C.byref(cfg), C.byref(h)))
         self._h = h

@@ -1,9 +1,10 @@
 """Serving loop on the GPU (m3lb_serve_*).
 
 A request's result must not depend on what else is resident: the batched
-kernel runs the paired kernel's per-chunk code for every lattice, so results
-are bit-identical alone, in a mix, under a one-lattice admission limit, and
-through the single-lattice C ABI with the paired kernel.
+kernel runs the paired kernel's per-unit code for every lattice, so results
+are bit-identical alone, in a mix, under a one-lattice admission limit, with
+either warp-to-node mapping (chunks or dense), and through the single-lattice
+C ABI with the paired kernel.
 """
 import ctypes as C
 
@@ -53,6 +54,38 @@ def test_alone_equals_mix(cuda_device, storage):
     for r in MIX:
         alone, alone_f, _ = _serve([r], storage)
         _same((mix[r.id], mix_f[r.id]), (alone[r.id], alone_f[r.id]))
+
+
+# Small and ragged boxes: N = 6 and 10 put several rows in one 64-node unit
+# and leave the last unit partly empty (N^3 not a multiple of 64); 48 and 80
+# split rows across units.
+RAGGED = [SV.Request(10, 0.0, 6, capi.OP_CM, 11, 0.05),
+          SV.Request(11, 0.0, 10, capi.OP_BGK, 8, 0.04),
+          SV.Request(12, 0.0, 48, capi.OP_TRT, 13, 0.06),
+          SV.Request(13, 0.0, 80, capi.OP_MRT, 7, 0.03),
+          SV.Request(14, 0.0, 64, capi.OP_CM, 9, 0.05)]
+
+
+@pytest.mark.parametrize("storage", ["f16", "bf16", "f32"])
+def test_dense_mapping_equals_chunks(cuda_device, storage):
+    reqs = MIX + RAGGED
+    ch, ch_f, st_c = _serve(reqs, storage, mapping="chunks")
+    de, de_f, st_d = _serve(reqs, storage, mapping="dense")
+    assert st_c.dense_launches == 0 and st_d.dense_launches == st_d.launches > 0
+    for r in reqs:
+        assert ch[r.id].status == 0 and de[r.id].status == 0
+        _same((ch[r.id], ch_f[r.id]), (de[r.id], de_f[r.id]))
+        assert np.isfinite(de[r.id].mass)
+
+
+def test_auto_mapping_rule(cuda_device):
+    # every N a multiple of 64: chunks; one ragged lattice: dense for its operator
+    _, _, st = _serve([SV.Request(0, 0.0, 64, capi.OP_CM, 5, 0.05),
+                       SV.Request(1, 0.0, 128, capi.OP_BGK, 5, 0.05)])
+    assert st.dense_launches == 0
+    _, _, st = _serve([SV.Request(0, 0.0, 64, capi.OP_CM, 5, 0.05),
+                       SV.Request(1, 0.0, 96, capi.OP_BGK, 5, 0.05)])
+    assert st.dense_launches == 5 and st.launches == 10
 
 
 def test_one_resident_at_a_time_equals_mix(cuda_device):

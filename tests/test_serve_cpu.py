@@ -49,3 +49,17 @@ def test_summary_percentiles():
     assert abs(s["latency_p50_s"] - 50.5) < 1e-9
     assert s["latency_p99_s"] > 99 and s["latency_max_s"] == 100.0
     assert abs(s["aggregate_mlups"] - 100 / 100.0) < 1e-9
+
+
+def test_serve_config_is_checked_before_any_device_work():
+    import ctypes as C
+    lib = capi.lib()
+    h = C.c_void_p()
+    bad_mapping = capi.ServeConfig(1 << 30, 8, 50, capi.STORE_F16, 0, 3)
+    assert lib.m3lb_serve_create(C.byref(bad_mapping), C.byref(h)) == capi.ERR_INVALID
+    assert b"mapping" in lib.m3lb_last_error()
+    bad_round = capi.ServeConfig(1 << 30, 8, 0, capi.STORE_F16, 0, capi.MAP_DENSE)
+    assert lib.m3lb_serve_create(C.byref(bad_round), C.byref(h)) == capi.ERR_INVALID
+    f64 = capi.ServeConfig(1 << 30, 8, 50, capi.STORE_F64, 0, capi.MAP_AUTO)
+    assert lib.m3lb_serve_create(C.byref(f64), C.byref(h)) == capi.ERR_UNSUPPORTED
+    assert not h.value
