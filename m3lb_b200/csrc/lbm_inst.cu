@@ -145,8 +145,8 @@ cudaError_t step_t(const StepArgs& a, int kernel, cudaStream_t s) {
     const long long nthreads = (long long)g.ny * g.nz * g.nch * 32;
     step_pairs<L, ST, OP, EQ, SH, FORCE><<<blocks_for(nthreads, kPairThreads), kPairThreads, 0, s>>>(a);
   } else {
-    const long long nn = (long long)g.nx * g.ny * g.nz;
-    step_nodes<L, ST, OP, EQ, SH, FORCE><<<blocks_for(nn, kNodeThreads), kNodeThreads, 0, s>>>(a);
+    step_nodes<L, ST, OP, EQ, SH, FORCE>
+        <<<node_grid(g.nx, (long long)g.ny * g.nz, kNodeThreads), kNodeThreads, 0, s>>>(a);
   }
   return cudaGetLastError();
 }
@@ -177,7 +177,7 @@ cudaError_t step(const StepArgs& a, int op, int eq, bool sh, bool force, int ker
 
 template <int OP, int EQ, bool SH>
 cudaError_t seed_t(const SeedArgs& a, cudaStream_t s) {
-  seed_kernel<L, ST, OP, EQ, SH><<<blocks_for(a.g.n_padded, 128), 128, 0, s>>>(a);
+  seed_kernel<L, ST, OP, EQ, SH><<<node_grid(a.g.sx, (long long)a.g.sy * a.g.sz, 128), 128, 0, s>>>(a);
   return cudaGetLastError();
 }
 template <int OP, int EQ>
@@ -199,7 +199,7 @@ cudaError_t seed(const SeedArgs& a, int op, int eq, bool sh, cudaStream_t s) {
 
 cudaError_t gather(const Geo& g, const void* f, int parity, double* out, void* raw,
                    cudaStream_t s) {
-  gather_kernel<L, ST><<<blocks_for(g.n_padded, 128), 128, 0, s>>>(g, f, parity, out, raw);
+  gather_kernel<L, ST><<<node_grid(g.sx, (long long)g.sy * g.sz, 128), 128, 0, s>>>(g, f, parity, out, raw);
   return cudaGetLastError();
 }
 
@@ -207,11 +207,11 @@ cudaError_t gather(const Geo& g, const void* f, int parity, double* out, void* r
 // rest: every collision shares BGK's moment sums (BGK.hpp:63-78).
 template <bool SH, bool FORCE>
 cudaError_t macro_t(const StepArgs& a, int op, cudaStream_t s) {
-  const long long nn = (long long)a.g.nx * a.g.ny * a.g.nz;
+  const dim3 grid = node_grid(a.g.nx, (long long)a.g.ny * a.g.nz, 128);
   if (op == 0)
-    macro_kernel<L, ST, 0, true, false><<<blocks_for(nn, 128), 128, 0, s>>>(a);
+    macro_kernel<L, ST, 0, true, false><<<grid, 128, 0, s>>>(a);
   else
-    macro_kernel<L, ST, 1, SH, FORCE><<<blocks_for(nn, 128), 128, 0, s>>>(a);
+    macro_kernel<L, ST, 1, SH, FORCE><<<grid, 128, 0, s>>>(a);
   return cudaGetLastError();
 }
 cudaError_t macro(const StepArgs& a, int op, bool sh, bool force, cudaStream_t s) {

@@ -377,9 +377,11 @@ step_pairs(StepArgs a) {
 }
 
 // -------------------------------------------------- one-node step kernel
-// Any geometry: full neighbour arithmetic of Domain::fill_neighbours
-// (Domain.hpp:82-101) per node.  Used where the paired kernel does not apply
-// (non-periodic x, odd nx).
+// Any geometry: one node per thread, neighbours by the wrap / clamp of
+// Domain::fill_neighbours (Domain.hpp:82-101).  Used where the paired kernel
+// does not apply (non-periodic x, odd nx).  NodeNb holds the neighbour
+// coordinates (boundary pass); the per-node kernels below address slots
+// through per-axis offsets instead (AxisSteps).
 template <class L>
 struct NodeNb {
   int x, y, z;
@@ -404,6 +406,83 @@ __device__ __forceinline__ size_t load_slot(const Geo& g, const NodeNb<L>& nb, i
   if (i & 1) return slot<L::Q>(g, nb.x, nb.y, nb.z, par == 0 ? i : i + 1);
   const int* m = nb.nb[i - 1];
   return slot<L::Q>(g, m[0], m[1], m[2], par == 0 ? i : i - 1);
+}
+
+// The same slots without per-direction coordinate arithmetic.  A slot is
+// ((z sy + y) nch + x/64) Q 64 + q 64 + x%64, so the slot of direction q at
+// the neighbour along c is the node's own slot of direction 0, plus q 64,
+// plus one precomputed offset per nonzero component of c: the element offset
+// to the same slot one step down [0] or up [1] each axis (the wrap or clamp
+// of shift_coord folded in).
+template <int Q>
+struct AxisSteps {
+  long long x[2], y[2], z[2];
+};
+template <int Q>
+__device__ __forceinline__ long long x_part(int v) {
+  return ((long long)(v >> 6) * Q << 6) + (v & 63);
+}
+template <int Q>
+__device__ __forceinline__ AxisSteps<Q> axis_steps(const Geo& g, int x, int y, int z) {
+  AxisSteps<Q> s;
+  const long long row = (long long)g.nch * Q * kChunk, plane = row * g.sy;
+#pragma unroll
+  for (int u = 0; u < 2; ++u) {
+    const int d = 2 * u - 1;
+    s.x[u] = x_part<Q>(shift_coord(x + d, g.hx, g.nx, g.sx, g.px)) - x_part<Q>(x);
+    s.y[u] = (long long)(shift_coord(y + d, g.hy, g.ny, g.sy, g.py) - y) * row;
+    s.z[u] = (long long)(shift_coord(z + d, g.hz, g.nz, g.sz, g.pz) - z) * plane;
+  }
+  return s;
+}
+// Offset to the neighbour at x + c_I.
+template <class L, int I>
+__device__ __forceinline__ long long nb_offset(const AxisSteps<L::Q>& s) {
+  constexpr int cx = L::cx[I], cy = L::cy[I], cz = L::cz[I];
+  long long o = 0;
+  if constexpr (cx != 0) o += s.x[cx > 0];
+  if constexpr (cy != 0) o += s.y[cy > 0];
+  if constexpr (cz != 0) o += s.z[cz > 0];
+  return o;
+}
+// load_slot of direction I from the node's slot of direction 0.
+template <class L, int I>
+__device__ __forceinline__ size_t load_slot_at(size_t own, const AxisSteps<L::Q>& s, int par) {
+  if constexpr (I == 0) return own;
+  else if constexpr ((I & 1) != 0) return own + (size_t)((par == 0 ? I : I + 1) * kChunk);
+  else return own + nb_offset<L, I - 1>(s) + (long long)((par == 0 ? I : I - 1) * kChunk);
+}
+// The node's logical populations (Access::load at parity par) as reals.
+template <class L, class E, class R>
+__device__ __forceinline__ void load_node(const E* A, const Geo& g, int x, int y, int z, int par, R* f) {
+  const size_t own = slot<L::Q>(g, x, y, z, 0);
+  const AxisSteps<L::Q> st = axis_steps<L::Q>(g, x, y, z);
+  static_for<0, L::Q>([&](auto I) {
+    constexpr int i = decltype(I)::value;
+    f[i] = to_real(A[load_slot_at<L, i>(own, st, par)]);
+  });
+}
+
+// Per-node kernels other than the paired ones run a 2-D grid: blockIdx.x the
+// x segment, blockIdx.y the row (y + ny z), striding by gridDim.y, so a
+// node's coordinates come from additions, not 64-bit divisions.
+struct RowWalk {
+  int y, z, dy, dz, ny;
+  __device__ __forceinline__ explicit RowWalk(int ny_) : ny(ny_) {
+    y = (int)(blockIdx.y % (unsigned)ny_);
+    z = (int)(blockIdx.y / (unsigned)ny_);
+    dy = (int)(gridDim.y % (unsigned)ny_);
+    dz = (int)(gridDim.y / (unsigned)ny_);
+  }
+  __device__ __forceinline__ void next() {
+    y += dy;
+    z += dz;
+    if (y >= ny) { y -= ny; ++z; }
+  }
+};
+inline dim3 node_grid(int nx, long long rows, int threads) {
+  return dim3((unsigned)((nx + threads - 1) / threads),
+              (unsigned)(rows < 65535 ? (rows > 0 ? rows : 1) : 65535));
 }
 
 // ------------------------------------------------------- specular walls
@@ -509,48 +588,55 @@ __device__ __forceinline__ Macro<R> spec_node_moments(R* f) {
   return m;
 }
 
+// One interior node of step_nodes.
 template <class L, int ST, int OP, int EQ, bool SH, bool FORCE>
-__global__ void __launch_bounds__(kNodeThreads)
-step_nodes(StepArgs a) {
+__device__ __forceinline__ void node_step(const StepArgs& a, int xi, int yi, int zi) {
   using E = typename StoreT<ST>::elem;
   using R = typename StoreT<ST>::real;
   constexpr int Q = L::Q;
   const Geo& g = a.g;
-  const long long nint = (long long)g.nx * g.ny * g.nz;
-  const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= nint) return;
-  const int xi = (int)(k % g.nx), yi = (int)((k / g.nx) % g.ny), zi = (int)(k / ((long long)g.nx * g.ny));
+  const long long k = ((long long)zi * g.ny + yi) * g.nx + xi;
   const int x = xi + g.hx, y = yi + g.hy, z = zi + g.hz;
   // Solid and Excluded skip (bounce-back is the identity on this storage);
   // wall nodes are left to the boundary pass
   if (a.flags && a.flags[((long long)z * g.sy + y) * g.sx + x] != 0) return;
-  NodeNb<L> nb;
-  node_neighbours<L>(g, x, y, z, nb);
-  E* A = reinterpret_cast<E*>(a.f);
+  const AxisSteps<Q> st = axis_steps<Q>(g, x, y, z);
+  E* own = reinterpret_cast<E*>(a.f) + slot<Q>(g, x, y, z, 0);
   const int P = a.parity;
+  // direction i (odd) at slot i + P of the node, i + 1 at slot i + 1 - P of
+  // the neighbour along c_i
+  E* up = own + P * kChunk;
+  E* dn = own + (1 - P) * kChunk;
   R f[Q];
-  f[0] = to_real(A[slot<Q>(g, x, y, z, 0)]);
-#pragma unroll
-  for (int i = 1; i < Q; i += 2) {
-    const int* m = nb.nb[i];
-    f[i] = to_real(A[slot<Q>(g, x, y, z, i + P)]);
-    f[i + 1] = to_real(A[slot<Q>(g, m[0], m[1], m[2], i + 1 - P)]);
-  }
+  f[0] = to_real(own[0]);
+  static_for<1, Q, 2>([&](auto I) {
+    constexpr int i = decltype(I)::value;
+    f[i] = to_real(up[i * kChunk]);
+    f[i + 1] = to_real(dn[nb_offset<L, i>(st) + i * kChunk]);
+  });
   const CollideParams<R> prm = node_params<FORCE, R>(a, (size_t)k);
   const Macro<R> mc = collide<L, OP, EQ, SH, FORCE>(f, prm);
-  A[slot<Q>(g, x, y, z, 0)] = from_real<E>(f[0]);
-#pragma unroll
-  for (int i = 1; i < Q; i += 2) {
-    const int* m = nb.nb[i];
-    A[slot<Q>(g, m[0], m[1], m[2], i + 1 - P)] = from_real<E>(f[i]);
-    A[slot<Q>(g, x, y, z, i + P)] = from_real<E>(f[i + 1]);
-  }
+  own[0] = from_real<E>(f[0]);
+  static_for<1, Q, 2>([&](auto I) {
+    constexpr int i = decltype(I)::value;
+    dn[nb_offset<L, i>(st) + i * kChunk] = from_real<E>(f[i]);
+    up[i * kChunk] = from_real<E>(f[i + 1]);
+  });
   if (a.rho) {
     reinterpret_cast<R*>(a.rho)[k] = mc.rho;
     reinterpret_cast<R*>(a.ux)[k] = mc.ux;
     reinterpret_cast<R*>(a.uy)[k] = mc.uy;
     reinterpret_cast<R*>(a.uz)[k] = mc.uz;
   }
+}
+
+template <class L, int ST, int OP, int EQ, bool SH, bool FORCE>
+__global__ void __launch_bounds__(kNodeThreads)
+step_nodes(StepArgs a) {
+  const Geo& g = a.g;
+  const int xi = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  if (xi >= g.nx) return;
+  for (RowWalk rw(g.ny); rw.z < g.nz; rw.next()) node_step<L, ST, OP, EQ, SH, FORCE>(a, xi, rw.y, rw.z);
 }
 
 // ------------------------------------------------------- initialisation
@@ -666,15 +752,14 @@ __device__ __forceinline__ bool axis_winner(int v, int c, int t, int per, int s)
 }
 
 
+// One padded node of seed_kernel.
 template <class L, int ST, int OP, int EQ, bool SH>
-__global__ void seed_kernel(SeedArgs a) {
+__device__ __forceinline__ void seed_node(const SeedArgs& a, int x, int y, int z) {
   using E = typename StoreT<ST>::elem;
   using R = typename StoreT<ST>::real;
   constexpr int Q = L::Q;
   const Geo& g = a.g;
-  const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (n >= g.n_padded) return;
-  const int x = (int)(n % g.sx), y = (int)((n / g.sx) % g.sy), z = (int)(n / ((long long)g.sx * g.sy));
+  const long long n = ((long long)z * g.sy + y) * g.sx + x;
   // RegWall and SpecNode are fluid nodes and seed as such (FluidSolver.hpp:553-579)
   const bool fluid = a.flags[n] == 0 || a.flags[n] == kRegWall || a.flags[n] == kSpecNode;
   R rho = (R)a.rho0, ux = 0, uy = 0, uz = 0;
@@ -690,8 +775,16 @@ __global__ void seed_kernel(SeedArgs a) {
       uz = reinterpret_cast<const R*>(a.uz)[k];
     }
   }
-  NodeNb<L> nb;
-  node_neighbours<L>(g, x, y, z, nb);
+  // neighbour coordinate one step down [0] / up [1] each axis
+  int xn[2], yn[2], zn[2];
+#pragma unroll
+  for (int u = 0; u < 2; ++u) {
+    xn[u] = shift_coord(x + 2 * u - 1, g.hx, g.nx, g.sx, g.px);
+    yn[u] = shift_coord(y + 2 * u - 1, g.hy, g.ny, g.sy, g.py);
+    zn[u] = shift_coord(z + 2 * u - 1, g.hz, g.nz, g.sz, g.pz);
+  }
+  const size_t own = slot<Q>(g, x, y, z, 0);
+  const AxisSteps<Q> st = axis_steps<Q>(g, x, y, z);
   E* A = reinterpret_cast<E*>(a.f);
   const int P = a.parity;
   R sv[Q];
@@ -700,12 +793,13 @@ __global__ void seed_kernel(SeedArgs a) {
     constexpr int i = decltype(I)::value;
     if constexpr (i > 0 && (i & 1) == 0) {
       constexpr int cx = L::cx[i - 1], cy = L::cy[i - 1], cz = L::cz[i - 1];
-      const int* m = nb.nb[i - 1];
-      if (!axis_winner(x, cx, m[0], g.px, g.sx) || !axis_winner(y, cy, m[1], g.py, g.sy) ||
-          !axis_winner(z, cz, m[2], g.pz, g.sz))
+      const int mx = cx == 0 ? x : xn[cx > 0], my = cy == 0 ? y : yn[cy > 0];
+      const int mz = cz == 0 ? z : zn[cz > 0];
+      if (!axis_winner(x, cx, mx, g.px, g.sx) || !axis_winner(y, cy, my, g.py, g.sy) ||
+          !axis_winner(z, cz, mz, g.pz, g.sz))
         return;
     }
-    const size_t s = load_slot<L>(g, nb, P, i);
+    const size_t s = load_slot_at<L, i>(own, st, P);
     if (a.mode == 2) {
       if (a.pops) A[s] = from_real<E>(a.pops[n * Q + i]);
       else A[s] = reinterpret_cast<const E*>(a.raw)[n * Q + i];
@@ -715,38 +809,46 @@ __global__ void seed_kernel(SeedArgs a) {
   });
 }
 
+template <class L, int ST, int OP, int EQ, bool SH>
+__global__ void seed_kernel(SeedArgs a) {
+  const Geo& g = a.g;
+  const int x = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  if (x >= g.sx) return;
+  for (RowWalk rw(g.sy); rw.z < g.sz; rw.next()) seed_node<L, ST, OP, EQ, SH>(a, x, rw.y, rw.z);
+}
+
 // gather_populations (FluidSolver.hpp:620-624, 1243-1253): logical
 // populations of every padded node, as double or as raw storage elements.
 template <class L, int ST>
 __global__ void gather_kernel(Geo g, const void* f, int parity, double* out, void* raw) {
   using E = typename StoreT<ST>::elem;
   constexpr int Q = L::Q;
-  const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (n >= g.n_padded) return;
-  const int x = (int)(n % g.sx), y = (int)((n / g.sx) % g.sy), z = (int)(n / ((long long)g.sx * g.sy));
-  NodeNb<L> nb;
-  node_neighbours<L>(g, x, y, z, nb);
+  const int x = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  if (x >= g.sx) return;
   const E* A = reinterpret_cast<const E*>(f);
-#pragma unroll
-  for (int i = 0; i < Q; ++i) {
-    const E e = A[load_slot<L>(g, nb, parity, i)];
-    if (out) out[n * Q + i] = (double)to_real(e);
-    else reinterpret_cast<E*>(raw)[n * Q + i] = e;
+  for (RowWalk rw(g.sy); rw.z < g.sz; rw.next()) {
+    const int y = rw.y, z = rw.z;
+    const long long n = ((long long)z * g.sy + y) * g.sx + x;
+    const size_t own = slot<Q>(g, x, y, z, 0);
+    const AxisSteps<Q> st = axis_steps<Q>(g, x, y, z);
+    static_for<0, Q>([&](auto I) {
+      constexpr int i = decltype(I)::value;
+      const E e = A[load_slot_at<L, i>(own, st, parity)];
+      if (out) out[n * Q + i] = (double)to_real(e);
+      else reinterpret_cast<E*>(raw)[n * Q + i] = e;
+    });
   }
 }
 
 // compute_macroscopic (FluidSolver.hpp:1041-1179): rho, u of every interior
-// node at the current parity; non-fluid nodes report zeros.
+// node at the current parity; non-fluid nodes report zeros.  One node:
 template <class L, int ST, int OP, bool SH, bool FORCE>
-__global__ void macro_kernel(StepArgs a) {
+__device__ __forceinline__ void macro_node(const StepArgs& a, int xi, int yi, int zi) {
   using E = typename StoreT<ST>::elem;
   using R = typename StoreT<ST>::real;
   constexpr int Q = L::Q;
   const Geo& g = a.g;
-  const long long nint = (long long)g.nx * g.ny * g.nz;
-  const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= nint) return;
-  const int xi = (int)(k % g.nx), yi = (int)((k / g.nx) % g.ny), zi = (int)(k / ((long long)g.nx * g.ny));
+  const long long k = ((long long)zi * g.ny + yi) * g.nx + xi;
   const int x = xi + g.hx, y = yi + g.hy, z = zi + g.hz;
   R* rho = reinterpret_cast<R*>(a.rho);
   R* ux = reinterpret_cast<R*>(a.ux);
@@ -759,12 +861,8 @@ __global__ void macro_kernel(StepArgs a) {
     rho[k] = ux[k] = uy[k] = uz[k] = R(0);
     return;
   }
-  NodeNb<L> nb;
-  node_neighbours<L>(g, x, y, z, nb);
-  const E* A = reinterpret_cast<const E*>(a.f);
   R f[Q];
-#pragma unroll
-  for (int i = 0; i < Q; ++i) f[i] = to_real(A[load_slot<L>(g, nb, a.parity, i)]);
+  load_node<L>(reinterpret_cast<const E*>(a.f), g, x, y, z, a.parity, f);
   Macro<R> m;
   if (spec_node) {
     spec_node_mirror<L>(f, a.spec[pn]);
@@ -773,6 +871,14 @@ __global__ void macro_kernel(StepArgs a) {
     m = macroscopic<L, OP, SH, FORCE>(f, node_params<FORCE, R>(a, (size_t)k));
   }
   rho[k] = m.rho; ux[k] = m.ux; uy[k] = m.uy; uz[k] = m.uz;
+}
+
+template <class L, int ST, int OP, bool SH, bool FORCE>
+__global__ void macro_kernel(StepArgs a) {
+  const Geo& g = a.g;
+  const int xi = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  if (xi >= g.nx) return;
+  for (RowWalk rw(g.ny); rw.z < g.nz; rw.next()) macro_node<L, ST, OP, SH, FORCE>(a, xi, rw.y, rw.z);
 }
 
 // ------------------------------------------------------------ reductions
@@ -794,6 +900,42 @@ __device__ __forceinline__ double block_sum(double v, double* sh) {
   return r;
 }
 
+// Sum in FP64 of every stored slot (all padded rows and chunks, all
+// directions, x < sx), this thread's share: 16-byte words t0, t0 + stride,
+// ... of the population array in that order, each word's elements in lane
+// order.  A word lies inside one 64-element segment (direction q of chunk ch
+// of a row); its position advances by the stride's parts with carries.
+template <int Q, class E>
+__device__ __forceinline__ double slot_sum_part(const E* A, const Geo& g, long long t0,
+                                                long long stride) {
+  constexpr int EPW = 16 / (int)sizeof(E);  // elements per word
+  constexpr int WPS = kChunk / EPW;         // words per segment
+  const long long nw = (long long)g.sz * g.sy * g.nch * Q * WPS;
+  const long long seg0 = t0 / WPS, sseg = stride / WPS;
+  int sub = (int)(t0 % WPS), q = (int)(seg0 % Q), ch = (int)(seg0 / Q % g.nch);
+  const int ss = (int)(stride % WPS), sq = (int)(sseg % Q), sc = (int)(sseg / Q % g.nch);
+  const uint4* W = reinterpret_cast<const uint4*>(A);
+  double acc = 0;
+#pragma unroll 4
+  for (long long w = t0; w < nw; w += stride) {
+    const uint4 v = W[w];
+    const E* e = reinterpret_cast<const E*>(&v);
+    const int x0 = ch * kChunk + sub * EPW;
+#pragma unroll
+    for (int j = 0; j < EPW; ++j)
+      if (x0 + j < g.sx) acc += (double)to_real(e[j]);
+    sub += ss;
+    const int c0 = sub >= WPS;
+    sub -= c0 * WPS;
+    q += sq + c0;
+    const int c1 = q >= Q;
+    q -= c1 * Q;
+    ch += sc + c1;
+    if (ch >= g.nch) ch -= g.nch;
+  }
+  return acc;
+}
+
 template <class L, int ST, int OP, bool SH, bool FORCE>
 __global__ void __launch_bounds__(kReduceThreads)
 reduce_kernel(StepArgs a, double* partials) {
@@ -807,19 +949,27 @@ reduce_kernel(StepArgs a, double* partials) {
   const long long nint = (long long)g.nx * g.ny * g.nz;
   const long long stride = (long long)gridDim.x * blockDim.x;
   const CollideParams<R> prm{(R)a.omega, (R)a.omega2, (R)a.fx, (R)a.fy, (R)a.fz};
-  for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < nint; k += stride) {
-    const int xi = (int)(k % g.nx), yi = (int)((k / g.nx) % g.ny), zi = (int)(k / ((long long)g.nx * g.ny));
+  // thread t sums nodes t, t + stride, ... in that order; the coordinates
+  // advance by the stride's (x, y, z) parts with carries
+  const long long k0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long nxy = (long long)g.nx * g.ny;
+  int xi = (int)(k0 % g.nx), yi = (int)((k0 / g.nx) % g.ny), zi = (int)(k0 / nxy);
+  const int sxs = (int)(stride % g.nx), sys = (int)((stride / g.nx) % g.ny);
+  const int szs = (int)(stride / nxy);
+  for (long long k = k0; k < nint; k += stride) {
     const int x = xi + g.hx, y = yi + g.hy, z = zi + g.hz;
+    xi += sxs;
+    if (xi >= g.nx) { xi -= g.nx; ++yi; }
+    yi += sys;
+    if (yi >= g.ny) { yi -= g.ny; ++zi; }
+    zi += szs;
     const long long pn = ((long long)z * g.sy + y) * g.sx + x;
     const unsigned fl = a.flags ? a.flags[pn] : 0u;
     const bool spec_node = fl == kSpecNode && a.spec;
     // fluid-like: Fluid, RegWall and SpecNode (FluidSolver.hpp:1215)
     if (fl != 0 && !spec_node && !(fl == kRegWall && a.spec)) continue;
-    NodeNb<L> nb;
-    node_neighbours<L>(g, x, y, z, nb);
     R f[Q];
-#pragma unroll
-    for (int i = 0; i < Q; ++i) f[i] = to_real(A[load_slot<L>(g, nb, a.parity, i)]);
+    load_node<L>(A, g, x, y, z, a.parity, f);
     if (spec_node) spec_node_mirror<L>(f, a.spec[pn]);  // reduce, FluidSolver.hpp:1221-1222
     const Macro<R> m = macroscopic<L, OP, SH, FORCE>(f, FORCE ? node_params<FORCE, R>(a, (size_t)k) : prm);
     const double r = (double)m.rho, u = (double)m.ux, v = (double)m.uy, w = (double)m.uz;
@@ -830,13 +980,7 @@ reduce_kernel(StepArgs a, double* partials) {
     acc[4] += 0.5 * r * (u * u + v * v + w * w);
   }
   // every stored slot (all padded rows and chunks, all directions, x < sx)
-  const long long nseg = (long long)g.sz * g.sy * g.nch * Q;
-  const long long nslot = nseg * kChunk;
-  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < nslot; e += stride) {
-    const long long seg = e >> 6;
-    const int x = (int)(((seg / Q) % g.nch) * kChunk + (e & 63));
-    if (x < g.sx) acc[5] += (double)to_real(A[e]);
-  }
+  acc[5] = slot_sum_part<Q>(A, g, k0, stride);
 #pragma unroll
   for (int v = 0; v < kReduceVals; ++v) {
     const double s = block_sum(acc[v], sh);
@@ -844,12 +988,23 @@ reduce_kernel(StepArgs a, double* partials) {
   }
 }
 
+// The partials of `nvals` interleaved sums, added by one warp in a fixed
+// order: lane l takes blocks l, l + 32, ..., then a fixed shuffle tree.
+__device__ __forceinline__ void warp_fixed_sums(const double* partials, int nblocks, int nvals,
+                                                double* out) {
+  const int lane = threadIdx.x & 31;
+  for (int v = 0; v < nvals; ++v) {
+    double s = 0;
+    for (int b = lane; b < nblocks; b += 32) s += partials[(size_t)b * nvals + v];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if (lane == 0) out[v] = s;
+  }
+}
+
+// Launched with one warp.
 static __global__ void reduce_finish(const double* partials, int nblocks, double* out) {
-  const int v = threadIdx.x;
-  if (v >= kReduceVals) return;
-  double s = 0;
-  for (int b = 0; b < nblocks; ++b) s += partials[(size_t)b * kReduceVals + v];
-  out[v] = s;
+  if (threadIdx.x < 32) warp_fixed_sums(partials, nblocks, kReduceVals, out);
 }
 
 }  // namespace m3lb

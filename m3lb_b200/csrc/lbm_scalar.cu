@@ -65,42 +65,6 @@ inline dim3 row_grid(const Geo& g, int threads) {
   return dim3((unsigned)((g.nx + threads - 1) / threads), (unsigned)g.ny, (unsigned)g.nz);
 }
 
-// Element offsets from a node's slot to the same slot of the neighbour one
-// step down [0] or up [1] each axis (shift_coord's wrap or clamp).  A slot is
-// ((z sy + y) nch + x/64) Q 64 + q 64 + x%64, so a neighbour's address is the
-// node's own plus one offset per nonzero velocity component.
-template <int Q>
-struct AxisSteps {
-  long long x[2], y[2], z[2];
-};
-template <int Q>
-__device__ __forceinline__ long long x_part(int v) {
-  return ((long long)(v >> 6) * Q << 6) + (v & 63);
-}
-template <int Q>
-__device__ __forceinline__ AxisSteps<Q> axis_steps(const Geo& g, int x, int y, int z) {
-  AxisSteps<Q> s;
-  const long long row = (long long)g.nch * Q * kChunk, plane = row * g.sy;
-#pragma unroll
-  for (int u = 0; u < 2; ++u) {
-    const int d = 2 * u - 1;
-    s.x[u] = x_part<Q>(shift_coord(x + d, g.hx, g.nx, g.sx, g.px)) - x_part<Q>(x);
-    s.y[u] = (long long)(shift_coord(y + d, g.hy, g.ny, g.sy, g.py) - y) * row;
-    s.z[u] = (long long)(shift_coord(z + d, g.hz, g.nz, g.sz, g.pz) - z) * plane;
-  }
-  return s;
-}
-// Offset to the neighbour at x + c_I.
-template <class L, int I>
-__device__ __forceinline__ long long nb_offset(const AxisSteps<L::Q>& s) {
-  constexpr int cx = L::cx[I], cy = L::cy[I], cz = L::cz[I];
-  long long o = 0;
-  if constexpr (cx != 0) o += s.x[cx > 0];
-  if constexpr (cy != 0) o += s.y[cy > 0];
-  if constexpr (cz != 0) o += s.z[cz > 0];
-  return o;
-}
-
 // ScalarBGK::eq (ScalarBGK.hpp:43-49): w_i (dT + (T_ref + dT) c_i.u / cs2).
 template <class L, int I, class R>
 __device__ __forceinline__ R s_eq(R T_ref, R dT, R ux, R uy, R uz) {
@@ -375,22 +339,13 @@ __global__ void __launch_bounds__(kReduceThreads) scalar_total(ScalarArgs a, dou
   __shared__ double sh[kReduceThreads / 32];
   const Geo& g = a.g;
   const E* A = reinterpret_cast<const E*>(a.f);
-  const long long nslot = (long long)g.sz * g.sy * g.nch * L::Q * kChunk;
-  double acc = 0;
-  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < nslot;
-       e += (long long)gridDim.x * blockDim.x) {
-    const long long seg = e >> 6;
-    const int x = (int)(((seg / L::Q) % g.nch) * kChunk + (e & 63));
-    if (x < g.sx) acc += (double)to_real(A[e]);
-  }
+  const double acc = slot_sum_part<L::Q>(A, g, (long long)blockIdx.x * blockDim.x + threadIdx.x,
+                                         (long long)gridDim.x * blockDim.x);
   const double s = block_sum(acc, sh);
   if (threadIdx.x == 0) partials[blockIdx.x] = s;
 }
 __global__ void scalar_total_finish(const double* partials, int nb, double* out) {
-  if (threadIdx.x != 0) return;
-  double s = 0;
-  for (int b = 0; b < nb; ++b) s += partials[b];
-  *out = s;
+  if (threadIdx.x < 32) warp_fixed_sums(partials, nb, 1, out);
 }
 
 // Logical populations per padded node as double (tests).
