@@ -54,8 +54,17 @@ constexpr int kMaxItems = 1024;  // lattices in one launch (shared-memory search
 // One time step of every lattice in `items` (all with operator OP): warp u
 // of the grid updates unit u - first_unit of the item whose range holds u,
 // a chunk (DENSE false) or 64 consecutive nodes (DENSE true) of pairs_unit.
+// Resident 128-thread blocks per SM of the batched kernel: as the paired
+// kernel, except that 16-bit BGK / TRT run four (128 registers, with a few
+// spills) instead of three; measured on the serving stream, 16 warps per SM
+// beat the spill-free 12 (BGK sets 27.6 -> 29.5 GLUPS, TRT 26.7 -> 28.3).
+template <int OP, int ST>
+constexpr int batch_min_blocks() {
+  return (OP == 1 || OP == 2) && (ST == kF16 || ST == kBF16) ? 4 : pair_min_blocks<OP, ST>();
+}
+
 template <int ST, int OP, int EQ, bool DENSE>
-__global__ void __launch_bounds__(kBatchThreads, pair_min_blocks<OP, ST>())
+__global__ void __launch_bounds__(kBatchThreads, batch_min_blocks<OP, ST>())
 batch_step(const BatchItem* __restrict__ items, int n_items, long long n_units, int s) {
   __shared__ long long first[kMaxItems];
   for (int i = threadIdx.x; i < n_items; i += blockDim.x) first[i] = items[i].first_unit;
