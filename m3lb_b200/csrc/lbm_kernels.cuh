@@ -55,6 +55,44 @@ __device__ __forceinline__ CollideParams<R> node_params(const StepArgs& a, size_
 }
 template <> __device__ __forceinline__ d2 bc<d2>(double a) { return {a, a}; }
 __device__ __forceinline__ double lane_of(d2 a, int k) { return k ? a.y : a.x; }
+__device__ __forceinline__ f2 pack2v(float2 v) { return pack2(v.x, v.y); }
+__device__ __forceinline__ d2 pack2v(double2 v) { return pack2(v.x, v.y); }
+
+// Two adjacent elements (x0, x0 + 1; x0 even, so the pair is one aligned
+// 8- or 16-byte word when the array is aligned) of a per-node array.
+template <class R> struct Vec2;
+template <> struct Vec2<float> { using T = float2; };
+template <> struct Vec2<double> { using T = double2; };
+template <class R>
+__device__ __forceinline__ bool pair_aligned(const void* p) {
+  return (reinterpret_cast<uintptr_t>(p) & (2 * sizeof(R) - 1)) == 0;
+}
+template <class R>
+__device__ __forceinline__ typename Vec2<R>::T load_pair2(const R* p, size_t k) {
+  if (pair_aligned<R>(p)) return *reinterpret_cast<const typename Vec2<R>::T*>(p + k);
+  return typename Vec2<R>::T{p[k], p[k + 1]};
+}
+// rho, u of a node pair into the macroscopic arrays at interior index kk
+// (even); a solid node of the pair keeps its value.
+template <class R, class V>
+__device__ __forceinline__ void store_macro_pair(const StepArgs& a, size_t kk, const Macro<V>& m,
+                                                 bool solid0, bool solid1) {
+  R* dst[4] = {reinterpret_cast<R*>(a.rho), reinterpret_cast<R*>(a.ux), reinterpret_cast<R*>(a.uy),
+               reinterpret_cast<R*>(a.uz)};
+  const V val[4] = {m.rho, m.ux, m.uy, m.uz};
+  const bool whole = !solid0 && !solid1 && pair_aligned<R>(a.rho) && pair_aligned<R>(a.ux) &&
+                     pair_aligned<R>(a.uy) && pair_aligned<R>(a.uz);
+#pragma unroll
+  for (int f = 0; f < 4; ++f) {
+    if (whole) {
+      *reinterpret_cast<typename Vec2<R>::T*>(dst[f] + kk) =
+          typename Vec2<R>::T{(R)lane_of(val[f], 0), (R)lane_of(val[f], 1)};
+    } else {
+      if (!solid0) dst[f][kk] = (R)lane_of(val[f], 0);
+      if (!solid1) dst[f][kk + 1] = (R)lane_of(val[f], 1);
+    }
+  }
+}
 
 // ------------------------------------------------------------ word traits
 // A word holds one direction of two x-adjacent nodes (lo = even x).
@@ -310,7 +348,7 @@ __device__ __forceinline__ void pairs_unit(const StepArgs& a, long long warp, in
       if (a.temp) {
         const S* T = reinterpret_cast<const S*>(a.temp);
         const size_t kk = ((size_t)zi * g.ny + yi) * g.nx + x0;
-        buoyant_force<V>(a, c.active ? pack2(T[kk], T[kk + 1]) : bc<V>(S(0)), prm.fx, prm.fy, prm.fz);
+        buoyant_force<V>(a, c.active ? pack2v(load_pair2(T, kk)) : bc<V>(S(0)), prm.fx, prm.fy, prm.fz);
       }
       m = collide<L, OP, EQ, SH, FORCE>(f, prm);
     } else {
@@ -354,18 +392,8 @@ __device__ __forceinline__ void pairs_unit(const StepArgs& a, long long warp, in
   });
 
   {
-    if (a.rho && c.active) {
-      using R = S;
-      const size_t kk = ((size_t)zi * g.ny + yi) * g.nx + x0;
-#pragma unroll
-      for (int e = 0; e < 2; ++e) {
-        if (e == 0 ? solid0 : solid1) continue;
-        reinterpret_cast<R*>(a.rho)[kk + e] = (R)lane_of(m.rho, e);
-        reinterpret_cast<R*>(a.ux)[kk + e] = (R)lane_of(m.ux, e);
-        reinterpret_cast<R*>(a.uy)[kk + e] = (R)lane_of(m.uy, e);
-        reinterpret_cast<R*>(a.uz)[kk + e] = (R)lane_of(m.uz, e);
-      }
-    }
+    if (a.rho && c.active)
+      store_macro_pair<S>(a, ((size_t)zi * g.ny + yi) * g.nx + x0, m, solid0, solid1);
   }
 }
 

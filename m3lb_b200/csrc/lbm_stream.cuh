@@ -386,7 +386,7 @@ step_stream(StepArgs a) {
         if (a.temp) {
           const S* T = reinterpret_cast<const S*>(a.temp);
           const size_t kk = ((size_t)cur.zi * g.ny + cur.yi) * g.nx + lx.x0;
-          buoyant_force<V>(a, lx.active ? pack2(T[kk], T[kk + 1]) : bc<V>(S(0)), pv.fx, pv.fy, pv.fz);
+          buoyant_force<V>(a, lx.active ? pack2v(load_pair2(T, kk)) : bc<V>(S(0)), pv.fx, pv.fy, pv.fz);
         }
         m = collide<L, OP, EQ, SH, FORCE>(f, pv);
       } else {
@@ -464,18 +464,8 @@ step_stream(StepArgs a) {
     });
 
     {
-      if (a.rho && lx.active) {
-        using R = S;
-        const size_t kk = ((size_t)cur.zi * g.ny + cur.yi) * g.nx + lx.x0;
-#pragma unroll
-        for (int e = 0; e < 2; ++e) {
-          if (e == 0 ? solid0 : solid1) continue;
-          reinterpret_cast<R*>(a.rho)[kk + e] = (R)lane_of(m.rho, e);
-          reinterpret_cast<R*>(a.ux)[kk + e] = (R)lane_of(m.ux, e);
-          reinterpret_cast<R*>(a.uy)[kk + e] = (R)lane_of(m.uy, e);
-          reinterpret_cast<R*>(a.uz)[kk + e] = (R)lane_of(m.uz, e);
-        }
-      }
+      if (a.rho && lx.active)
+        store_macro_pair<S>(a, ((size_t)cur.zi * g.ny + cur.yi) * g.nx + lx.x0, m, solid0, solid1);
     }
     cur.advance(tw, dk, dy, dz, g.nch, g.ny);
   }

@@ -101,3 +101,16 @@ def test_policy_mirror_defaults():
         for i in range(L.Q):
             j = S.opp(i)
             assert (L.cx[j], L.cy[j], L.cz[j]) == (-L.cx[i], -L.cy[i], -L.cz[i])
+
+
+def test_scalar_create_checks_extents_before_device_work():
+    # the scalar kernels take y and z from the grid, so ny and nz are at most 65535
+    lib = capi.lib()
+    h = C.c_void_p()
+    bgk = 1  # M3LB_SOP_BGK
+    assert lib.m3lb_scalar_create(7, 4, 70000, 2, 1, 1, 1, bgk, capi.STORE_F32, C.byref(h)) == \
+        capi.ERR_INVALID
+    assert "65535" in capi.last_error()
+    assert lib.m3lb_scalar_create(7, 4, 4, 4, 1, 1, 1, 2, capi.STORE_F16, C.byref(h)) == \
+        capi.ERR_UNSUPPORTED
+    assert not h.value

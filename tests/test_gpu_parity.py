@@ -203,3 +203,30 @@ def test_row_kernel_equals_paired_kernel(cuda_device, storage, lat, shape, op):
             np.testing.assert_array_equal(x, y)
     for c in cases:
         c.close()
+
+
+@pytest.mark.parametrize("lat,shape", [(9, (6, 70000, 1)), (27, (4, 300, 250))])
+def test_rows_beyond_one_grid_dimension(cuda_device, lat, shape):
+    """More rows (y, z pairs) than one grid dimension holds (65535): the
+    per-node kernels (one-node step, seed, gather, macroscopic readout,
+    reduction) stride over rows.  A non-periodic x axis selects the one-node
+    step kernel."""
+    op = 4 if lat == 27 else 1
+    c = Case(lat=lat, op=op, storage="f32", shape=shape, periodic=(False, True, True),
+             omega2=1.6 if op == 4 else -1.0)
+    c.init_random(seed=5)
+    o0 = c.cpu.gather()
+    scale = float(np.max(np.abs(o0)))
+    tol = _tol("f32", scale)
+    assert np.max(np.abs(c.gpu.gather_populations() - o0)) <= tol
+    c.step(3, store=True)
+    assert float(np.max(np.abs(c.gpu.gather_populations() - c.cpu.gather()))) <= tol
+    ar = EPS["f32"]
+    for a, b in zip(c.gpu.compute_macroscopic(), c.cpu.macro()):
+        sc = max(float(np.max(np.abs(b))), 1e-3)
+        assert float(np.max(np.abs(a - b))) <= lat * tol / 0.9 + 64 * ar * sc
+    red = c.gpu.reduce()
+    nf = float(np.prod(shape))
+    assert abs(red[0] - c.cpu.total_mass()) <= nf * lat * tol + 8 * ar * nf * np.sqrt(nf)
+    assert abs(red[5] - c.cpu.slot_sum()) <= c.dom.n_padded * lat * tol + 1e-12 * nf * lat
+    c.close()
