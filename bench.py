@@ -388,7 +388,7 @@ def serving_arm(args):
 
     reqs = SV.request_stream(count=args.serve_requests, rate=50.0, seed=0)
     srv = SV.Server(hbm_budget=args.serve_budget_gb << 30, max_resident=args.serve_resident,
-                    round_steps=args.serve_round, storage="f16")
+                    round_steps=args.serve_round, storage="f16", mapping="tune")
     for r in reqs:
         srv.submit(r)
     srv.run(time_limit=900)
@@ -412,6 +412,10 @@ def serving_arm(args):
                  "graph_captures": st.graph_captures, "graph_launches": st.graph_launches,
                  "hbm_budget_gib": args.serve_budget_gb, "max_resident": args.serve_resident,
                  "round_steps": args.serve_round},
+        "mapping_tuner": {"chosen": {1: "chunks", 2: "dense"}.get(st.tuned_mapping, "none"),
+                          "chunks_mlups": round(st.tuned_chunks_mlups, 1),
+                          "dense_mlups": round(st.tuned_dense_mlups, 1),
+                          "dense_launches": st.dense_launches},
         "workload": "seed 0, Poisson 50/s, N in {32..160 step 16}, op in {BGK, TRT, CM}, "
                     "u0 ~ U[0.02, 0.08], steps ~ U[200, 2000], FP16, tau 0.6",
     }

@@ -379,17 +379,22 @@ typedef struct {
   int storage;        /* M3LB_STORE_F16, _BF16 or _F32, for every request */
   int keep_fields;    /* 1: keep rho, u of finished requests for m3lb_serve_fields */
   int mapping;        /* warp-to-node mapping of the batched launches: M3LB_MAP_AUTO (0),
-                         _CHUNKS or _DENSE (same results, different speed) */
+                         _CHUNKS, _DENSE or _TUNE (same results, different speed) */
 } m3lb_serve_config;
 
 /* M3LB_MAP_CHUNKS: a warp updates one 64-slot chunk of a row (lanes past the
  * row's end idle when N is not a multiple of 64).  M3LB_MAP_DENSE: a warp
  * updates 64 consecutive nodes in x-fastest order, rows packed back to back,
  * so no lane idles.  M3LB_MAP_AUTO: dense for an operator's launch when one
- * of its lattices has N not a multiple of 64, chunks otherwise. */
+ * of its lattices has N not a multiple of 64, chunks otherwise.
+ * M3LB_MAP_TUNE: an autotuner on the live stream: the first rounds alternate
+ * the two mappings, each timed on the device (CUDA events around the round's
+ * launches) for 6 rounds, and the one with more lattice updates per second
+ * serves every later round (reported in m3lb_serve_stats). */
 #define M3LB_MAP_AUTO 0
 #define M3LB_MAP_CHUNKS 1
 #define M3LB_MAP_DENSE 2
+#define M3LB_MAP_TUNE 3
 
 typedef struct {
   long long id;         /* caller's tag */
@@ -418,6 +423,9 @@ typedef struct {
   long long node_steps;     /* sum of n^3 * steps over completed requests */
   double makespan;          /* seconds from the start of the last run to its end */
   long long dense_launches; /* batched launches with the dense mapping */
+  int tuned_mapping;         /* M3LB_MAP_TUNE: the mapping chosen (_CHUNKS or _DENSE), 0 before */
+  double tuned_chunks_mlups; /* the tuner's measured rates of both mappings (MLUPS) */
+  double tuned_dense_mlups;
 } m3lb_serve_stats;
 
 int m3lb_serve_create(const m3lb_serve_config* cfg, m3lb_server** out);

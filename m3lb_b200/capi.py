@@ -23,7 +23,7 @@ STORE_F32, STORE_F16, STORE_BF16, STORE_F64 = 0, 1, 2, 3
 OPT_NODE_KERNEL = 1
 OPT_KERNEL = 2
 KERNEL_AUTO, KERNEL_NODES, KERNEL_PAIRS, KERNEL_STREAM, KERNEL_ROWS = 0, 1, 2, 3, 4
-MAP_AUTO, MAP_CHUNKS, MAP_DENSE = 0, 1, 2
+MAP_AUTO, MAP_CHUNKS, MAP_DENSE, MAP_TUNE = 0, 1, 2, 3
 
 STORAGE_NAMES = {"f32": STORE_F32, "f16": STORE_F16, "bf16": STORE_BF16, "f64": STORE_F64}
 STORAGE_BYTES = {STORE_F32: 4, STORE_F16: 2, STORE_BF16: 2, STORE_F64: 8}
@@ -62,7 +62,9 @@ class ServeStats(C.Structure):
     _fields_ = [("rounds", C.c_longlong), ("launches", C.c_longlong),
                 ("graph_captures", C.c_longlong), ("graph_launches", C.c_longlong),
                 ("finished", C.c_longlong), ("node_steps", C.c_longlong),
-                ("makespan", C.c_double), ("dense_launches", C.c_longlong)]
+                ("makespan", C.c_double), ("dense_launches", C.c_longlong),
+                ("tuned_mapping", C.c_int), ("tuned_chunks_mlups", C.c_double),
+                ("tuned_dense_mlups", C.c_double)]
 
 
 _vp = C.c_void_p

@@ -158,11 +158,19 @@ struct Finished {
 
 constexpr int kOps[4] = {M3LB_OP_BGK, M3LB_OP_TRT, M3LB_OP_MRT, M3LB_OP_CM};
 
-// A launched round: its end event and the requests whose readout it carries.
+// A launched round: its end event and the requests whose readout it carries;
+// for a round the mapping tuner measures, timing events around its launches,
+// the mapping it ran and its lattice updates.
 struct Inflight {
   cudaEvent_t end = nullptr;
   std::vector<size_t> finishing;  // indices into done
+  cudaEvent_t t0 = nullptr, t1 = nullptr;
+  int cand = -1;                  // 0 chunks, 1 dense
+  double lups = 0;
 };
+
+// Rounds the tuner measures with each mapping before it fixes the faster.
+constexpr int kTuneRounds = 6;
 
 }  // namespace
 
@@ -194,6 +202,14 @@ struct m3lb_server {
   int graph_R = -1;
   long long prev_version = -1;      // resident set and R of the previous round
   int prev_R = -1;
+  int graph_map = -1, prev_map = -1;  // unit mappings (bit o: operator o dense) of both
+  // M3LB_MAP_TUNE: rounds launched / measured with each mapping, their time
+  // and lattice updates, the mapping of the round being built (-1: the
+  // automatic rule), and the choice once made (-1 until then)
+  int tune_launched[2] = {0, 0}, tune_measured[2] = {0, 0};
+  double tune_ms[2] = {0, 0}, tune_lups[2] = {0, 0};
+  int tune_cand = -1, tuned = -1;
+  std::vector<cudaEvent_t> free_timing;
   double* red_slots = nullptr;      // pinned, kReduceVals per request of a run
   int red_cap = 0;
   std::deque<Inflight> inflight;    // launched rounds not yet observed complete
@@ -348,6 +364,24 @@ int retire_oldest(m3lb_server* s, Clock::time_point t0) {
   s->inflight.pop_front();
   SRV_TRY(cudaEventSynchronize(f.end));
   const double t = now_s(t0);
+  if (f.cand >= 0) {
+    float ms = 0;
+    SRV_TRY(cudaEventElapsedTime(&ms, f.t0, f.t1));
+    s->tune_ms[f.cand] += ms;
+    s->tune_lups[f.cand] += f.lups;
+    s->tune_measured[f.cand] += 1;
+    s->free_timing.push_back(f.t0);
+    s->free_timing.push_back(f.t1);
+    if (s->tuned < 0 && s->tune_measured[0] >= kTuneRounds && s->tune_measured[1] >= kTuneRounds) {
+      // the higher rate of lattice updates per second of GPU time
+      const double r0 = s->tune_lups[0] / std::max(s->tune_ms[0], 1e-9);
+      const double r1 = s->tune_lups[1] / std::max(s->tune_ms[1], 1e-9);
+      s->tuned = r1 > r0 ? 1 : 0;
+      s->stats.tuned_mapping = s->tuned ? M3LB_MAP_DENSE : M3LB_MAP_CHUNKS;
+      s->stats.tuned_chunks_mlups = r0 * 1e-3;
+      s->stats.tuned_dense_mlups = r1 * 1e-3;
+    }
+  }
   for (size_t i : f.finishing) {
     m3lb_result& r = s->done[i].res;
     const double* v = s->red_slots + i * kReduceVals;
@@ -371,8 +405,15 @@ BatchItem* host_table(m3lb_server* s) { return s->items_host + (size_t)s->flip *
 // dense when a lattice of it has rows that leave chunk lanes idle (N not a
 // multiple of 64), chunks otherwise (the two are the same then).
 void choose_mapping(m3lb_server* s) {
+  if (s->cfg.mapping == M3LB_MAP_TUNE) {
+    const int m = s->tuned >= 0 ? s->tuned : s->tune_cand;
+    if (m >= 0) {
+      for (int o = 0; o < 4; ++o) s->dense[o] = m == 1;
+      return;
+    }
+  }
   for (int o = 0; o < 4; ++o) s->dense[o] = s->cfg.mapping == M3LB_MAP_DENSE;
-  if (s->cfg.mapping != M3LB_MAP_AUTO) return;
+  if (s->cfg.mapping != M3LB_MAP_AUTO && s->cfg.mapping != M3LB_MAP_TUNE) return;
   for (const Lattice& l : s->active) {
     int o = 0;
     while (kOps[o] != l.req.op) ++o;
@@ -432,10 +473,14 @@ int run_round(m3lb_server* s, int R) {
     if (s->n_items[o])
       SRV_TRY(cudaMemcpyAsync(s->items_dev + (size_t)o * kMaxItems, tab + (size_t)o * kMaxItems,
                               s->n_items[o] * sizeof(BatchItem), cudaMemcpyHostToDevice, s->stream));
-  const bool cached = s->graph_exec && s->graph_version == s->set_version && s->graph_R == R;
-  const bool repeat = s->prev_version == s->set_version && s->prev_R == R;
+  int map = 0;
+  for (int o = 0; o < 4; ++o) map |= (s->dense[o] ? 1 : 0) << o;
+  const bool cached = s->graph_exec && s->graph_version == s->set_version && s->graph_R == R &&
+                      s->graph_map == map;
+  const bool repeat = s->prev_version == s->set_version && s->prev_R == R && s->prev_map == map;
   s->prev_version = s->set_version;
   s->prev_R = R;
+  s->prev_map = map;
   if (!cached && !repeat) {
     const int rc = launch_round(s, R);
     if (rc) return rc;
@@ -458,6 +503,7 @@ int run_round(m3lb_server* s, int R) {
       SRV_TRY(cudaGraphInstantiate(&s->graph_exec, s->graph, 0));
       s->graph_version = s->set_version;
       s->graph_R = R;
+      s->graph_map = map;
       s->stats.graph_captures += 1;
     }
     SRV_TRY(cudaGraphLaunch(s->graph_exec, s->stream));
@@ -489,8 +535,9 @@ int m3lb_serve_create(const m3lb_serve_config* cfg, m3lb_server** out) {
     return fail(M3LB_ERR_UNSUPPORTED, "serve_create: storage %d is not served (F16, BF16, F32)",
                 cfg->storage);
   if (cfg->round_steps < 1) return fail(M3LB_ERR_INVALID, "serve_create: round_steps must be >= 1");
-  if (cfg->mapping < M3LB_MAP_AUTO || cfg->mapping > M3LB_MAP_DENSE)
-    return fail(M3LB_ERR_INVALID, "serve_create: mapping must be M3LB_MAP_AUTO, _CHUNKS or _DENSE");
+  if (cfg->mapping < M3LB_MAP_AUTO || cfg->mapping > M3LB_MAP_TUNE)
+    return fail(M3LB_ERR_INVALID,
+                "serve_create: mapping must be M3LB_MAP_AUTO, _CHUNKS, _DENSE or _TUNE");
   auto* s = new m3lb_server();
   s->cfg = *cfg;
   cudaGetDevice(&s->device);
@@ -569,12 +616,34 @@ int m3lb_serve_run(m3lb_server* s, double time_limit) {
     }
     long long R = s->cfg.round_steps;
     for (const Lattice& l : s->active) R = std::min<long long>(R, l.req.steps - l.t);
+    Inflight f;
     if (R > 0) {
+      // the mapping tuner alternates the two mappings over its first rounds
+      s->tune_cand = -1;
+      if (s->cfg.mapping == M3LB_MAP_TUNE && s->tuned < 0) {
+        const int c = s->tune_launched[0] <= s->tune_launched[1] ? 0 : 1;
+        if (s->tune_launched[c] < kTuneRounds) s->tune_cand = c;
+      }
+      if (s->tune_cand >= 0) {
+        for (int k = 0; k < 2; ++k) {
+          if (s->free_timing.empty()) {
+            cudaEvent_t e = nullptr;
+            SRV_TRY(cudaEventCreate(&e));
+            s->free_timing.push_back(e);
+          }
+          (k ? f.t1 : f.t0) = s->free_timing.back();
+          s->free_timing.pop_back();
+        }
+        f.cand = s->tune_cand;
+        for (const Lattice& l : s->active) f.lups += (double)l.req.n * l.req.n * l.req.n * (double)R;
+        s->tune_launched[f.cand] += 1;
+        SRV_TRY(cudaEventRecord(f.t0, s->stream));
+      }
       const int rc = run_round(s, (int)R);
       if (rc) return rc;
+      if (f.cand >= 0) SRV_TRY(cudaEventRecord(f.t1, s->stream));
     }
     // lattices done after this round: readout and release follow it on the stream
-    Inflight f;
     for (size_t i = 0; i < s->active.size();) {
       Lattice& l = s->active[i];
       if (l.t >= l.req.steps) {
@@ -652,8 +721,13 @@ int m3lb_serve_destroy(m3lb_server* s) {
   if (s->items_dev) cudaFree(s->items_dev);
   if (s->items_host) cudaFreeHost(s->items_host);
   if (s->red_slots) cudaFreeHost(s->red_slots);
-  for (Inflight& f : s->inflight) cudaEventDestroy(f.end);
+  for (Inflight& f : s->inflight) {
+    cudaEventDestroy(f.end);
+    if (f.t0) cudaEventDestroy(f.t0);
+    if (f.t1) cudaEventDestroy(f.t1);
+  }
   for (cudaEvent_t e : s->free_events) cudaEventDestroy(e);
+  for (cudaEvent_t e : s->free_timing) cudaEventDestroy(e);
   if (s->stream) cudaStreamDestroy(s->stream);
   delete s;
   return M3LB_OK;

@@ -88,6 +88,21 @@ def test_auto_mapping_rule(cuda_device):
     assert st.dense_launches == 5 and st.launches == 10
 
 
+def test_tuned_mapping_measures_both_and_keeps_results(cuda_device):
+    # 200 steps in rounds of 10: 20 rounds, the first 12 alternate the mappings
+    reqs = [SV.Request(i, 0.0, n, op, 200, 0.05)
+            for i, (n, op) in enumerate([(48, capi.OP_CM), (80, capi.OP_BGK), (32, capi.OP_TRT)])]
+    tu, tu_f, st = _serve(reqs, round_steps=10, mapping="tune")
+    ch, ch_f, _ = _serve(reqs, round_steps=10, mapping="chunks")
+    assert st.tuned_mapping in (capi.MAP_CHUNKS, capi.MAP_DENSE)
+    assert st.tuned_chunks_mlups > 0 and st.tuned_dense_mlups > 0
+    faster = capi.MAP_DENSE if st.tuned_dense_mlups > st.tuned_chunks_mlups else capi.MAP_CHUNKS
+    assert st.tuned_mapping == faster
+    assert 0 < st.dense_launches < st.launches
+    for r in reqs:
+        _same((tu[r.id], tu_f[r.id]), (ch[r.id], ch_f[r.id]))
+
+
 def test_one_resident_at_a_time_equals_mix(cuda_device):
     mix, mix_f, _ = _serve(MIX)
     seq, seq_f, _ = _serve(MIX, max_resident=1, round_steps=7)

@@ -55,7 +55,7 @@ def test_serve_config_is_checked_before_any_device_work():
     import ctypes as C
     lib = capi.lib()
     h = C.c_void_p()
-    bad_mapping = capi.ServeConfig(1 << 30, 8, 50, capi.STORE_F16, 0, 3)
+    bad_mapping = capi.ServeConfig(1 << 30, 8, 50, capi.STORE_F16, 0, 4)
     assert lib.m3lb_serve_create(C.byref(bad_mapping), C.byref(h)) == capi.ERR_INVALID
     assert b"mapping" in lib.m3lb_last_error()
     bad_round = capi.ServeConfig(1 << 30, 8, 0, capi.STORE_F16, 0, capi.MAP_DENSE)
