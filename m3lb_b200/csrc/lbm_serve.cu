@@ -54,13 +54,16 @@ constexpr int kMaxItems = 1024;  // lattices in one launch (shared-memory search
 // One time step of every lattice in `items` (all with operator OP): warp u
 // of the grid updates unit u - first_unit of the item whose range holds u,
 // a chunk (DENSE false) or 64 consecutive nodes (DENSE true) of pairs_unit.
-// Resident 128-thread blocks per SM of the batched kernel: as the paired
-// kernel, except that 16-bit BGK / TRT run four (128 registers, with a few
-// spills) instead of three; measured on the serving stream, 16 warps per SM
-// beat the spill-free 12 (BGK sets 27.6 -> 29.5 GLUPS, TRT 26.7 -> 28.3).
+// Resident 128-thread blocks per SM of the batched kernel: four (128
+// registers) for every operator on 16-bit storage, where the paired kernel
+// runs three for BGK / TRT and five for MRT / CM.  Measured on sets of
+// resident lattices (dense mapping, N = 160 / 96 / 48): BGK 27.6 -> 29.5
+// GLUPS and TRT 26.7 -> 28.3 at N = 160 (a few bytes of spills buy 16 warps
+// per SM instead of 12); CM 26.2 / 26.3 / 24.6 -> 26.8-28.9 / 28.8 / 27.2
+// (five blocks spill more at 102 registers; six, at 80, lose 15 %).
 template <int OP, int ST>
 constexpr int batch_min_blocks() {
-  return (OP == 1 || OP == 2) && (ST == kF16 || ST == kBF16) ? 4 : pair_min_blocks<OP, ST>();
+  return (ST == kF16 || ST == kBF16) ? 4 : pair_min_blocks<OP, ST>();
 }
 
 template <int ST, int OP, int EQ, bool DENSE>
