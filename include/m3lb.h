@@ -60,15 +60,15 @@ extern "C" {
 #define M3LB_OPT_KERNEL 2      /* value: one of M3LB_KERNEL_* below */
 
 /* Step kernel choice (M3LB_OPT_KERNEL).  The chunk kernels (pairs, stream,
- * rows) need a periodic x axis and even nx, the row kernel also nx a
- * multiple of 64 up to 256 (and FP64 storage up to 128); a choice that does not apply falls back to the
+ * rows) need a periodic x axis and even nx, the row kernel also nx up to 256
+ * (and FP64 storage up to 128); a choice that does not apply falls back to the
  * paired kernel, and without a periodic x axis to the one-node kernel.  All choices give identical stored bits for BGK/TRT and
  * agree to a few ulp for the moment operators (different FMA contraction). */
 #define M3LB_KERNEL_AUTO 0   /* the fastest kernel for the lattice */
 #define M3LB_KERNEL_NODES 1  /* one node per thread */
 #define M3LB_KERNEL_PAIRS 2  /* one warp per 64-node chunk, two nodes per lane */
 #define M3LB_KERNEL_STREAM 3 /* persistent chunk kernel, asynchronous copy pipeline */
-#define M3LB_KERNEL_ROWS 4   /* whole rows through shared memory by TMA (nx % 64 == 0, nx <= 256) */
+#define M3LB_KERNEL_ROWS 4   /* whole rows through shared memory by TMA (nx <= 256) */
 
 typedef struct m3lb_solver m3lb_solver;
 

@@ -165,13 +165,13 @@ struct m3lb_solver {
     if (node_kernel || !chunk_ok() || kernel == M3LB_KERNEL_NODES) return kKernelNodes;
     // the streamed kernel addresses rows with 32-bit element counts
     const bool rows32 = (long long)g.nch * Q * 64 < (1LL << 31);
-    // the row kernel: whole rows of at most 8 full chunks
-    const bool rows_ok = (g.nx % 64) == 0 && g.nch <= 4 &&
+    // the row kernel: whole rows of at most 4 chunks (the last may be partial)
+    const bool rows_ok = g.nch <= 4 &&
                          4LL * Q * 256 * elem_bytes(storage) + 64 <= 227LL * 1024;
     if (kernel == M3LB_KERNEL_ROWS && rows_ok) return kKernelRows;
     if (kernel == M3LB_KERNEL_STREAM && rows32) return kKernelStream;
     // auto, from measurements on B200: with 16-bit storage the row kernel
-    // for rows of 3 or 4 full chunks (256^3 CM: 0.34 ms against 0.49 ms for
+    // for rows of 3 or 4 chunks (256^3 CM: 0.34 ms against 0.49 ms for
     // the paired kernel), else the streamed kernel for BGK/TRT and pure
     // streaming; the paired kernel for everything else (32/64-bit storage
     // is already near the copy bandwidth with it)

@@ -105,7 +105,7 @@ template <int OP, int EQ, bool SH, bool FORCE>
 cudaError_t launch_rows(const StepArgs& a, cudaStream_t s) {
   using Cfg = RowsCfg<L, ST>;
   const Geo& g = a.g;
-  if (g.nch < 1 || g.nch > kRowsMaxWarps || (g.nx % kChunk) != 0 || Cfg::SMEM > kRowsSmemMax)
+  if (g.nch < 1 || g.nch > kRowsMaxWarps || (g.nx % 2) != 0 || Cfg::SMEM > kRowsSmemMax)
     return cudaErrorInvalidValue;
   auto kern = step_rows<L, ST, OP, EQ, SH, FORCE>;
   const int threads = g.nch * 32;

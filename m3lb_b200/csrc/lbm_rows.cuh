@@ -24,8 +24,8 @@
 //     row in the update itself;
 //   * rows are independent: CTAs never exchange data, and a row's global
 //     lines are read and written only by its own CTA within a step.
-// Warp w of a CTA takes chunk w of the row (nch <= 4 warps, nx a multiple of
-// 64, periodic x).  Rows stream through a kRowsStages-stage ring with the
+// Warp w of a CTA takes chunk w of the row (nch <= 4 warps, nx even,
+// periodic x; lanes past nx in a partial last chunk store nothing).  Rows stream through a kRowsStages-stage ring with the
 // rows ahead of the one being updated in flight.
 //
 // Waits on the load barriers are bounded: past the limit the CTA records a
@@ -320,7 +320,11 @@ step_rows(StepArgs a, const __grid_constant__ RowMaps<L> maps) {
   // `count` lines ([chunk][count][64]): (x >> 6) * count * 64 + (x & 63).
   // The pair's word at x0, the words at x0 + 2 and x0 - 2 and the element
   // at x0 - 1 (periodic wrap), for the block shapes the plan uses.
-  const int x0 = k * kChunk + 2 * lane;
+  // A lane past the end of a partial last chunk (x0 >= nx) takes lane 0's
+  // positions, so its shared-memory reads stay inside the row, and counts as
+  // solid, so it stores nothing.
+  const bool lane_ok = k * kChunk + 2 * lane < g.nx;
+  const int x0 = lane_ok ? k * kChunk + 2 * lane : 0;
   const int xn = (x0 + 2 == g.nx) ? 0 : x0 + 2;
   const int xm = (x0 == 0) ? g.nx - 2 : x0 - 2;
   const int xe = (x0 == 0) ? g.nx - 1 : x0 - 1;
@@ -368,12 +372,12 @@ step_rows(StepArgs a, const __grid_constant__ RowMaps<L> maps) {
       }
     });
 
-    bool solid0 = false, solid1 = false;
+    bool solid0 = !lane_ok, solid1 = !lane_ok;
     if (a.flags) {
       const uint16_t fl = *reinterpret_cast<const uint16_t*>(
           a.flags + ((long long)(cur.zi + g.hz) * g.sy + (cur.yi + g.hy)) * g.sx + x0);
-      solid0 = (fl & 0xffu) != 0;
-      solid1 = (fl >> 8) != 0;
+      solid0 = solid0 || (fl & 0xffu) != 0;
+      solid1 = solid1 || (fl >> 8) != 0;
     }
     Macro<V> m;
     if constexpr (OP != 0) {

@@ -172,8 +172,10 @@ def test_streamed_kernel_equals_paired_kernel(cuda_device, storage, lat, shape, 
         c.close()
 
 
+# the last four have a partial last chunk (lanes past nx store nothing)
 ROWS_SHAPES = [(27, (64, 5, 4)), (27, (128, 4, 3)), (27, (192, 3, 3)), (27, (256, 2, 3)),
-               (9, (128, 6, 1))]
+               (9, (128, 6, 1)), (27, (160, 3, 3)), (27, (208, 2, 3)), (27, (96, 4, 3)),
+               (9, (146, 6, 1))]
 
 
 @pytest.mark.parametrize("lat,shape", ROWS_SHAPES)
