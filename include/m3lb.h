@@ -250,7 +250,8 @@ int m3lb_scatter_raw(m3lb_solver* h, const void* in);
 int m3lb_timestep(const m3lb_solver* h, long long* t);
 int m3lb_dims(const m3lb_solver* h, int dims[12]);
 /* populations() (:609): device pointer and byte size of the population array
- * (row-blocked layout: element (x,y,z,q) at ((z*sy+y)*Q+q)*pitch + x). */
+ * (x-chunked layout: with nch = ceil(sx / 64), element (x,y,z,q) of the
+ * padded block at (((z*sy+y)*nch + x/64)*Q + q)*64 + x%64). */
 int m3lb_populations(const m3lb_solver* h, void** ptr, size_t* bytes);
 
 /* Queue the handle's work on `stream` (a cudaStream_t; NULL = legacy default). */
@@ -264,15 +265,19 @@ int m3lb_launch_count(const m3lb_solver* h, long long* n);
  * The reduction of m3lb_reduce for callers that cannot allocate device memory
  * (who therefore cannot create a handle, which allocates): the caller passes
  * the population array and flags it holds (device pointers, the layout of
- * m3lb_populations; flags per padded node, or NULL for an all-fluid interior;
- * any nonzero flag, specular ones included, excludes the node from the sums),
+ * m3lb_populations; flags per padded node, or NULL for an all-fluid interior),
  * the lattice description, the time step (for the parity) and a device array
- * `out` of six doubles receiving the same sums as m3lb_reduce.  Queued on
- * `stream`; returns without waiting.  Allocates nothing: the partial sums use
- * a fixed 768 KiB array inside the library, so at most 4,194,304 interior
- * nodes are accepted (M3LB_ERR_INVALID beyond).  The first call on a device
- * looks that array's address up; make it before any stream capture.  Calls
- * share the array: calls that overlap on the GPU race. */
+ * `out` of six doubles receiving the same sums as m3lb_reduce, bit for bit,
+ * on a lattice without wall nodes.  Wall nodes are not supported: this call
+ * has no wall table, so a node flagged RegWall (3), SpecWall (4) or SpecNode
+ * (5) counts as solid and is left out of the mass, momentum and energy sums,
+ * where m3lb_reduce on a handle with walls counts RegWall and SpecNode nodes.
+ * Queued on `stream`; returns without waiting.  Allocates nothing: the
+ * partial sums use a fixed 768 KiB array inside the library, so at most
+ * 4,194,304 interior nodes are accepted (M3LB_ERR_INVALID beyond).  The
+ * first call in a CUDA context looks that array's address up (again after
+ * cudaDeviceReset or under another context); make it before any stream
+ * capture.  Calls share the array: calls that overlap on the GPU race. */
 int m3lb_reduce_static(int lattice, int nx, int ny, int nz, int px, int py, int pz, int op,
                        int storage, int shifted, int forcing, double fx, double fy, double fz,
                        const void* populations, const uint8_t* flags, long long timestep,

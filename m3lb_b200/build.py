@@ -27,7 +27,7 @@ SLICES = [(lat, st) for lat in ("D2Q9", "D3Q27") for st in ("F32", "F16", "BF16"
 HEADERS = ["lbm_common.cuh", "lbm_collide.cuh", "lbm_kernels.cuh", "lbm_stream.cuh", "lbm_rows.cuh",
            "lbm_bound.cuh",
            "lbm_launch.h",
-           "lbm_host.h", "lbm_walls.h"]
+           "lbm_host.h", "lbm_walls.h", "ctx_cache.h"]
 
 
 def nvcc() -> str:

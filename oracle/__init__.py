@@ -23,6 +23,15 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 ORACLE_LIB = HERE / "liboracle.so"
+# Where the reference tree (M3LB's sources) is mounted: the one place that
+# names it.  Recipes that read the reference (the reference build, the
+# fixture scripts, the facade-driver tests) take it from here.
+REFERENCE_DIR = Path(os.environ.get("M3LB_REFERENCE", "/root/reference"))
+
+
+def reference_present() -> bool:
+    """The reference sources are available to build from."""
+    return (REFERENCE_DIR / "src" / "solver" / "FluidSolver.hpp").exists()
 REF_LIBS = {"f64": HERE / "_ref" / "libm3lb_ref_f64.so", "f32": HERE / "_ref" / "libm3lb_ref_f32.so"}
 
 OPS = {"none": 0, "bgk": 1, "trt": 2, "mrt": 3, "cm": 4}
@@ -410,5 +419,5 @@ def build(ref: bool = True, jobs: int | None = None) -> None:
     import subprocess
     jobs = jobs or os.cpu_count() or 4
     target = "all" if ref else "oracle"
-    subprocess.run(["make", "-C", str(HERE), f"-j{jobs}", target], check=True,
+    subprocess.run(["make", "-C", str(HERE), f"-j{jobs}", target, f"REF={REFERENCE_DIR}"], check=True,
                    stdout=subprocess.DEVNULL)

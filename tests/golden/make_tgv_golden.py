@@ -9,9 +9,13 @@ the GPU test can compare against them without the reference tree.
 
 Run from the repository root:  python tests/golden/make_tgv_golden.py
 """
+import sys
 from pathlib import Path
 
-SRC = Path("/root/reference/results/E_tgv3d/tgv3d_re1600_d3q27_cm.dat")
+sys.path.insert(0, str(Path(__file__).resolve().parents[2]))
+from oracle import REFERENCE_DIR  # noqa: E402
+
+SRC = REFERENCE_DIR / "results" / "E_tgv3d" / "tgv3d_re1600_d3q27_cm.dat"
 DST = Path(__file__).resolve().parent / "tgv3d_re1600_d3q27_cm.txt"
 
 

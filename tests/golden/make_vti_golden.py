@@ -18,7 +18,10 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 ROOT = HERE.parent.parent
-REF_SRC = Path("/root/reference/src")
+sys.path.insert(0, str(ROOT))
+from oracle import REFERENCE_DIR  # noqa: E402
+
+REF_SRC = REFERENCE_DIR / "src"
 OUT = HERE / "vti"
 
 

@@ -114,3 +114,23 @@ def test_scalar_create_checks_extents_before_device_work():
     assert lib.m3lb_scalar_create(7, 4, 4, 4, 1, 1, 1, 2, capi.STORE_F16, C.byref(h)) == \
         capi.ERR_UNSUPPORTED
     assert not h.value
+
+
+def test_noalloc_scratch_address_is_kept_per_context(tmp_path):
+    """m3lb_reduce_static's scratch address is cached per CUDA context, not
+    per device: the cache logic (ctx_cache.h) compiled on the host looks an
+    address up again when the context ID changes (as after cudaDeviceReset)
+    and never keeps one looked up under an unknown context."""
+    import shutil
+    from pathlib import Path
+
+    root = Path(__file__).resolve().parent.parent
+    exe = tmp_path / "ctx_cache_case"
+    cxx = shutil.which("g++") or "g++"
+    r = subprocess.run([cxx, "-std=c++17", "-O1", "-Wall", "-Werror",
+                        f"-I{root / 'm3lb_b200' / 'csrc'}",
+                        str(root / "tests" / "cpp" / "ctx_cache_case.cpp"), "-o", str(exe)],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr[-3000:]
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 0 and r.stdout.strip() == "ok", r.stdout + r.stderr

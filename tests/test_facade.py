@@ -18,6 +18,8 @@ from pathlib import Path
 import numpy as np
 import pytest
 
+from oracle import REFERENCE_DIR
+
 ROOT = Path(__file__).resolve().parent.parent
 FACADE = ROOT / "m3lb_b200" / "facade"
 LIBDIR = ROOT / "m3lb_b200"
@@ -38,13 +40,13 @@ def test_facade_driver_compiles(tmp_path):
     _compile(ROOT / "tests" / "cpp" / "facade_poiseuille.cpp", tmp_path / "fp")
 
 
-@pytest.mark.skipif(not Path("/root/reference/src/app/main.cpp").exists(),
+@pytest.mark.skipif(not (REFERENCE_DIR / "src" / "app" / "main.cpp").exists(),
                     reason="reference sources not present")
 @pytest.mark.parametrize("src", ["src/app/main.cpp", "examples/flow_past_square.cpp"])
 def test_reference_drivers_compile_unmodified(tmp_path, src):
     cxx = shutil.which("g++") or "g++"
     r = subprocess.run([cxx, "-std=c++20", "-O2", "-fsyntax-only", f"-I{FACADE}",
-                        f"-I{ROOT / 'include'}", f"/root/reference/{src}"],
+                        f"-I{ROOT / 'include'}", str(REFERENCE_DIR / src)],
                        capture_output=True, text=True)
     assert r.returncode == 0, r.stderr[-3000:]
 

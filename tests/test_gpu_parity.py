@@ -145,7 +145,7 @@ STREAM_SHAPES = [(27, (64, 5, 4)), (27, (192, 3, 3)), (27, (130, 4, 3)), (27, (2
 
 
 @pytest.mark.parametrize("lat,shape", STREAM_SHAPES)
-@pytest.mark.parametrize("op", [0, 2, 4])
+@pytest.mark.parametrize("op", [0, 1, 2, 4])
 @pytest.mark.parametrize("storage", ["f32", "f16", "bf16", "f64"])
 def test_streamed_kernel_equals_paired_kernel(cuda_device, storage, lat, shape, op):
     """The persistent copy-pipelined kernel and the paired kernel: identical
@@ -179,7 +179,7 @@ ROWS_SHAPES = [(27, (64, 5, 4)), (27, (128, 4, 3)), (27, (192, 3, 3)), (27, (256
 
 
 @pytest.mark.parametrize("lat,shape", ROWS_SHAPES)
-@pytest.mark.parametrize("op", [0, 2, 4])
+@pytest.mark.parametrize("op", [0, 1, 2, 3, 4])
 @pytest.mark.parametrize("storage", ["f32", "f16", "bf16", "f64"])
 def test_row_kernel_equals_paired_kernel(cuda_device, storage, lat, shape, op):
     """The TMA row kernel (whole rows through shared memory) and the paired
@@ -205,6 +205,56 @@ def test_row_kernel_equals_paired_kernel(cuda_device, storage, lat, shape, op):
             np.testing.assert_array_equal(x, y)
     for c in cases:
         c.close()
+
+
+def _kernels_equal(kernels, lat, shape, op, eq, storage, forcing, periodic, steps=7, seed=13):
+    """Run the same lattice under each kernel choice and require identical
+    stored bits and identical stored macroscopic fields."""
+    from m3lb_b200 import capi
+
+    cases = []
+    for kern in kernels:
+        c = Case(lat=lat, op=op, eq=eq, storage=storage, forcing=forcing, shape=shape,
+                 periodic=periodic, omega2=1.1 if op == 2 else -1.0)
+        c.gpu.set_option(capi.OPT_KERNEL, kern)
+        if not all(periodic):
+            c.gpu.set_geometry(_flags(c.shape))
+        rng = np.random.default_rng(seed)
+        c.gpu.initialize_field([1 + 0.01 * rng.standard_normal(c.shape)] +
+                               [0.03 * rng.standard_normal(c.shape) for _ in range(3)])
+        c.gpu.steps(steps, True)
+        c.gpu.sync()
+        cases.append(c)
+    ref = cases[0].gpu.gather_raw()
+    for c in cases[1:]:
+        np.testing.assert_array_equal(ref, c.gpu.gather_raw())
+        if op != 0:
+            for x, y in zip(cases[0].gpu.stored_macroscopic(), c.gpu.stored_macroscopic()):
+                np.testing.assert_array_equal(x, y)
+    for c in cases:
+        c.close()
+
+
+VARIANT_SHAPES = [(27, (128, 4, 3)), (27, (160, 3, 3)), (27, (256, 2, 2)), (9, (128, 6, 1))]
+
+
+@pytest.mark.parametrize("lat,shape", VARIANT_SHAPES)
+@pytest.mark.parametrize("op,eq", OPS)
+@pytest.mark.parametrize("forcing", [False, True])
+@pytest.mark.parametrize("periodic", [(True, True, True), (True, False, True)],
+                         ids=["periodic", "ywalls"])
+@pytest.mark.parametrize("storage", ["f16", "bf16"])
+def test_auto_kernels_equal_paired_kernel(cuda_device, storage, periodic, forcing, op, eq,
+                                          lat, shape):
+    """Every operator instantiation that the automatic choice sends to the row
+    kernel or the streamed kernel (16-bit storage: BGK, TRT, MRT, CM; both
+    equilibria; forced and unforced; a fully periodic lattice, whose rows wrap
+    in y through the row kernel's neighbour-row copies, and one with walls)
+    gives the paired kernel's bits."""
+    from m3lb_b200 import capi
+
+    _kernels_equal([capi.KERNEL_PAIRS, capi.KERNEL_ROWS, capi.KERNEL_STREAM, capi.KERNEL_AUTO],
+                   lat, shape, op, eq, storage, forcing, periodic)
 
 
 @pytest.mark.parametrize("lat,shape", [(9, (6, 70000, 1)), (27, (4, 300, 250))])
