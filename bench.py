@@ -266,6 +266,9 @@ def gpu_arm(args, rank, world, dist):
         out["walls"] = walls_arm(args, stream, omega)
     if rank == 0 and world == 1 and args.thermal_steps > 0:
         out["thermal"] = thermal_arm(args, stream, omega)
+    # the storage-ratio gate last, so it sits in the tail of the printed line
+    for key in ("fp32_storage", "fp16_over_fp32"):
+        out[key] = out.pop(key)
     return out
 
 

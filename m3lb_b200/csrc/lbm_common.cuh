@@ -85,17 +85,47 @@ template <> struct StoreT<kBF16> {
 // ------------------------------------------------------ packed arithmetic
 // Two adjacent nodes are updated together with sm_100's paired FP32 ops
 // (add/mul/fma .f32x2), one instruction for both lanes.  Every operation is
-// an explicitly rounded IEEE op (no contraction left to the compiler), so the
-// paired path and the one-node path give bitwise identical results.
+// an explicitly rounded IEEE op, so the paired path and the one-node path
+// give bitwise identical results.  The paired ops are issued as PTX
+// `mul/add/fma.rn.f32x2`: with the __fmul2_rn / __fadd2_rn intrinsics a
+// paired product feeding a paired sum was fused into one f32x2 FMA (one
+// rounding instead of two), which made the moment operators differ from the
+// one-node kernel by a few ulp; the explicit `.rn` form is never contracted.
 struct f2 { float2 v; };
+
+__device__ __forceinline__ unsigned long long f2_bits(float2 v) {
+  unsigned long long r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(v.x), "f"(v.y));
+  return r;
+}
+__device__ __forceinline__ float2 f2_of_bits(unsigned long long r) {
+  float2 v;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(v.x), "=f"(v.y) : "l"(r));
+  return v;
+}
+__device__ __forceinline__ float2 add2_rn(float2 a, float2 b) {
+  unsigned long long d;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(f2_bits(a)), "l"(f2_bits(b)));
+  return f2_of_bits(d);
+}
+__device__ __forceinline__ float2 mul2_rn(float2 a, float2 b) {
+  unsigned long long d;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(f2_bits(a)), "l"(f2_bits(b)));
+  return f2_of_bits(d);
+}
+__device__ __forceinline__ float2 fma2_rn(float2 a, float2 b, float2 c) {
+  unsigned long long d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(f2_bits(a)), "l"(f2_bits(b)), "l"(f2_bits(c)));
+  return f2_of_bits(d);
+}
 
 __device__ __forceinline__ f2 mk(float a, float b) { return f2{make_float2(a, b)}; }
 __device__ __forceinline__ f2 splat2(float a) { return f2{make_float2(a, a)}; }
-__device__ __forceinline__ f2 add(f2 a, f2 b) { return f2{__fadd2_rn(a.v, b.v)}; }
-__device__ __forceinline__ f2 mul(f2 a, f2 b) { return f2{__fmul2_rn(a.v, b.v)}; }
-__device__ __forceinline__ f2 fma(f2 a, f2 b, f2 c) { return f2{__ffma2_rn(a.v, b.v, c.v)}; }
+__device__ __forceinline__ f2 add(f2 a, f2 b) { return f2{add2_rn(a.v, b.v)}; }
+__device__ __forceinline__ f2 mul(f2 a, f2 b) { return f2{mul2_rn(a.v, b.v)}; }
+__device__ __forceinline__ f2 fma(f2 a, f2 b, f2 c) { return f2{fma2_rn(a.v, b.v, c.v)}; }
 // a - b as a + (-1)*b in one fused op: exactly the IEEE difference.
-__device__ __forceinline__ f2 sub(f2 a, f2 b) { return f2{__ffma2_rn(b.v, make_float2(-1.f, -1.f), a.v)}; }
+__device__ __forceinline__ f2 sub(f2 a, f2 b) { return f2{fma2_rn(b.v, make_float2(-1.f, -1.f), a.v)}; }
 __device__ __forceinline__ f2 neg(f2 a) { return f2{make_float2(-a.v.x, -a.v.y)}; }
 __device__ __forceinline__ f2 rcp(f2 a) { return f2{make_float2(__frcp_rn(a.v.x), __frcp_rn(a.v.y))}; }
 

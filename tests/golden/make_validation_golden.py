@@ -21,7 +21,15 @@ HERE = Path(__file__).resolve().parent
 ROOT = HERE.parent.parent
 OUT = HERE / "validation"
 PROGRAMS = ["specular", "specular_node", "specwall_unsteady", "regularized", "cavity", "thermal",
-            "natural_convection", "scalar_walls", "scalar_specular", "gaussian_plume", "scalar_mass"]
+            "natural_convection", "scalar_walls", "scalar_specular", "gaussian_plume", "scalar_mass",
+            "poiseuille", "galilean", "decaying_flows", "tgv3d_bench_f32_128"]
+# Programs run with arguments: fixture name -> (executable, arguments).  The
+# 3-D Taylor-Green benchmark at the 128^3 workload: FP32 populations, u0 0.05,
+# Re 1600 on L = N / (2 pi), 1000 time steps (t* = 1000 u0 / L; the half step
+# added to tmax only keeps the program's floor(tmax L / u0) at exactly 1000).
+TGV128_TMAX = 1000.5 * 0.05 / (128 / (2 * 3.141592653589793))
+ARGS = {"tgv3d_bench_f32_128": ("tgv3d_bench_f32", ["-d", "128", "-re", "1600", "-u0", "0.05",
+                                                    "-tmax", f"{TGV128_TMAX:.9f}"])}
 
 
 def main(names):
@@ -30,8 +38,9 @@ def main(names):
     OUT.mkdir(exist_ok=True)
     env = dict(os.environ, OMP_NUM_THREADS="4")
     for name in names or PROGRAMS:
-        exe = ROOT / "oracle" / "_ref" / f"{name}_cpu"
-        r = subprocess.run([str(exe)], capture_output=True, text=True, env=env)
+        prog, args = ARGS.get(name, (name, []))
+        exe = ROOT / "oracle" / "_ref" / f"{prog}_cpu"
+        r = subprocess.run([str(exe), *args], capture_output=True, text=True, env=env)
         if r.returncode != 0:
             raise SystemExit(f"{name} failed ({r.returncode}):\n{r.stdout}\n{r.stderr}")
         (OUT / f"{name}.txt").write_text(r.stdout)
