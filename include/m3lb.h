@@ -19,8 +19,9 @@
  *   op      : M3LB_OP_*                              src/collision/{BGK,TRT,MomentCollision}.hpp
  *   eq      : M3LB_EQ_* (BGK and TRT only)           src/equilibrium/Equilibrium.hpp:131-136
  *   storage : M3LB_STORE_* population element type; arithmetic is FP32 for
- *             F32/F16/BF16 and FP64 for F64.  16-bit storage requires shifted
- *             (except for M3LB_OP_NONE, which never reads the convention).
+ *             F32/F16/BF16/F16C and FP64 for F64.  16-bit storage requires
+ *             shifted (except for M3LB_OP_NONE, which never reads the
+ *             convention).
  *   shifted : 1 stores g = f - w (ShiftedPopulations), 0 stores f (Raw)
  *                                                    src/memory/Storage.hpp:27-35
  *   flags   : per interior node, x fastest: 0 Fluid, 1 Solid, 2 Excluded
@@ -55,20 +56,33 @@ extern "C" {
 #define M3LB_STORE_F16 1
 #define M3LB_STORE_BF16 2
 #define M3LB_STORE_F64 3
+/* FP16C: a 16-bit float with IEEE binary16's top exponent bit given to the
+ * mantissa (1 sign, 4 exponent bits with bias 15, 11 mantissa bits,
+ * subnormals; magnitudes up to 2 - 2^-11, larger ones and NaN saturate;
+ * round to nearest, ties away from zero).  The customised 16-bit format of
+ * Lehmann et al. (2022) for shifted populations: the same bytes as FP16,
+ * half the rounding error.  An addition of this library; the reference
+ * stores FP32 or FP64 only. */
+#define M3LB_STORE_F16C 4
 
 #define M3LB_OPT_NODE_KERNEL 1 /* value 1: always use the one-node step kernel */
 #define M3LB_OPT_KERNEL 2      /* value: one of M3LB_KERNEL_* below */
+/* Test only: the row kernel's wait for a row's copies gives up after `value`
+ * clock cycles instead of ~2 s (0 restores the default), so a test can make
+ * the wait run out and see m3lb_sync report it.  The populations of a step
+ * whose wait ran out are not valid. */
+#define M3LB_OPT_WAIT_CYCLES 3
 
 /* Step kernel choice (M3LB_OPT_KERNEL).  The chunk kernels (pairs, stream,
- * rows) need a periodic x axis and even nx, the row kernel also nx up to 256
- * (and FP64 storage up to 128); a choice that does not apply falls back to the
- * paired kernel, and without a periodic x axis to the one-node kernel.  All choices give identical stored bits for BGK/TRT and
- * agree to a few ulp for the moment operators (different FMA contraction). */
+ * rows) need a periodic x axis and even nx, the row kernel also nx up to 512
+ * with 16-bit storage and up to 256 with FP32 / FP64; a choice that does not
+ * apply falls back to the paired kernel, and without a periodic x axis to the
+ * one-node kernel.  All choices give identical stored bits. */
 #define M3LB_KERNEL_AUTO 0   /* the fastest kernel for the lattice */
 #define M3LB_KERNEL_NODES 1  /* one node per thread */
 #define M3LB_KERNEL_PAIRS 2  /* one warp per 64-node chunk, two nodes per lane */
 #define M3LB_KERNEL_STREAM 3 /* persistent chunk kernel, asynchronous copy pipeline */
-#define M3LB_KERNEL_ROWS 4   /* whole rows through shared memory by TMA (nx <= 256) */
+#define M3LB_KERNEL_ROWS 4   /* whole rows through shared memory by TMA (nx <= 512) */
 
 typedef struct m3lb_solver m3lb_solver;
 
@@ -236,6 +250,15 @@ int m3lb_macro_device(m3lb_solver* h, void** rho, void** ux, void** uy, void** u
  * over fluid nodes, out[5] sum of every stored population slot
  * (EsotericPull::storage(), src/memory/EsotericPull.hpp:119-123). */
 int m3lb_reduce(m3lb_solver* h, double out[6]);
+/* The validation campaign's flow diagnostics, diagnostics(s, d, nx, ny, nz)
+ * of validation/Campaign.hpp:99-130, on the device: compute_macroscopic,
+ * then over every interior node out[0] = sum 0.5 |u|^2 (kinetic energy) and
+ * out[1] = sum 0.5 |w|^2 (enstrophy), the vorticity w from central
+ * differences whose neighbours wrap around the interior on every axis (w_z
+ * only when nz == 1), in FP64; out[2] = the number of nodes with a
+ * non-finite velocity, which add nothing (the reference's `finite` is
+ * out[2] == 0).  Waits for the result. */
+int m3lb_diagnostics(m3lb_solver* h, double out[3]);
 
 /* gather_populations() (:620-624): logical populations, n_padded x Q,
  * node-major, as double, or as raw storage elements. */
@@ -381,7 +404,7 @@ typedef struct {
   size_t hbm_budget;  /* bytes the resident lattices may hold */
   int max_resident;   /* most lattices resident at once (0: budget only; at most 1024) */
   int round_steps;    /* most time steps per scheduling round (>= 1) */
-  int storage;        /* M3LB_STORE_F16, _BF16 or _F32, for every request */
+  int storage;        /* M3LB_STORE_F16, _F16C, _BF16 or _F32, for every request */
   int keep_fields;    /* 1: keep rho, u of finished requests for m3lb_serve_fields */
   int mapping;        /* warp-to-node mapping of the batched launches: M3LB_MAP_AUTO (0),
                          _CHUNKS, _DENSE or _TUNE (same results, different speed) */

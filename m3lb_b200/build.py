@@ -23,11 +23,11 @@ LIB = PKG / "libm3lb.so"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2"]
 
-SLICES = [(lat, st) for lat in ("D2Q9", "D3Q27") for st in ("F32", "F16", "BF16", "F64")]
+SLICES = [(lat, st) for lat in ("D2Q9", "D3Q27") for st in ("F32", "F16", "BF16", "F64", "F16C")]
 HEADERS = ["lbm_common.cuh", "lbm_collide.cuh", "lbm_kernels.cuh", "lbm_stream.cuh", "lbm_rows.cuh",
            "lbm_bound.cuh",
            "lbm_launch.h",
-           "lbm_host.h", "lbm_walls.h", "ctx_cache.h"]
+           "lbm_host.h", "lbm_walls.h", "ctx_cache.h", "lbm_diag.cuh"]
 
 
 def nvcc() -> str:

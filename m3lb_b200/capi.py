@@ -19,14 +19,16 @@ ERR_MEMORY = -4
 
 OP_NONE, OP_BGK, OP_TRT, OP_MRT, OP_CM = 0, 1, 2, 3, 4
 EQ_SECOND_ORDER, EQ_PRODUCT_FORM = 0, 1
-STORE_F32, STORE_F16, STORE_BF16, STORE_F64 = 0, 1, 2, 3
+STORE_F32, STORE_F16, STORE_BF16, STORE_F64, STORE_F16C = 0, 1, 2, 3, 4
 OPT_NODE_KERNEL = 1
 OPT_KERNEL = 2
+OPT_WAIT_CYCLES = 3  # test only: shorten the row kernel's wait for its copies
 KERNEL_AUTO, KERNEL_NODES, KERNEL_PAIRS, KERNEL_STREAM, KERNEL_ROWS = 0, 1, 2, 3, 4
 MAP_AUTO, MAP_CHUNKS, MAP_DENSE, MAP_TUNE = 0, 1, 2, 3
 
-STORAGE_NAMES = {"f32": STORE_F32, "f16": STORE_F16, "bf16": STORE_BF16, "f64": STORE_F64}
-STORAGE_BYTES = {STORE_F32: 4, STORE_F16: 2, STORE_BF16: 2, STORE_F64: 8}
+STORAGE_NAMES = {"f32": STORE_F32, "f16": STORE_F16, "bf16": STORE_BF16, "f64": STORE_F64,
+                 "f16c": STORE_F16C}
+STORAGE_BYTES = {STORE_F32: 4, STORE_F16: 2, STORE_BF16: 2, STORE_F64: 8, STORE_F16C: 2}
 
 
 class M3lbError(RuntimeError):
@@ -132,6 +134,7 @@ SIGNATURES = {
     "m3lb_stored_macro_f64": (_i, [_vp] + [_vp] * 4),
     "m3lb_macro_device": (_i, [_vp] + [_pp] * 4),
     "m3lb_reduce": (_i, [_vp, _vp]),
+    "m3lb_diagnostics": (_i, [_vp, _vp]),
     "m3lb_gather": (_i, [_vp, _vp]),
     "m3lb_gather_raw": (_i, [_vp, _vp]),
     "m3lb_scatter": (_i, [_vp, _vp]),

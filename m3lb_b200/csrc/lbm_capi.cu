@@ -10,6 +10,7 @@
 #include <vector>
 
 #include "../../include/m3lb.h"
+#include "lbm_diag.cuh"
 #include "lbm_host.h"
 #include "lbm_walls.h"
 
@@ -62,7 +63,8 @@ int elem_bytes(int storage) {
     case M3LB_STORE_F32: return 4;
     case M3LB_STORE_F64: return 8;
     case M3LB_STORE_F16:
-    case M3LB_STORE_BF16: return 2;
+    case M3LB_STORE_BF16:
+    case M3LB_STORE_F16C: return 2;
     default: return 0;
   }
 }
@@ -97,6 +99,7 @@ const Launchers* table_for(int lattice, int storage) {
       case M3LB_STORE_F16: return launchers_D2Q9_F16();
       case M3LB_STORE_BF16: return launchers_D2Q9_BF16();
       case M3LB_STORE_F64: return launchers_D2Q9_F64();
+      case M3LB_STORE_F16C: return launchers_D2Q9_F16C();
     }
   } else if (lattice == 27) {
     switch (storage) {
@@ -104,11 +107,16 @@ const Launchers* table_for(int lattice, int storage) {
       case M3LB_STORE_F16: return launchers_D3Q27_F16();
       case M3LB_STORE_BF16: return launchers_D3Q27_BF16();
       case M3LB_STORE_F64: return launchers_D3Q27_F64();
+      case M3LB_STORE_F16C: return launchers_D3Q27_F16C();
     }
   }
   return nullptr;
 }
 }  // namespace m3lb
+
+// Shortest rows (in 64-node chunks) the automatic choice sends to the row
+// kernel with 16-bit storage.
+constexpr int kAutoRowsMinChunks = 2;
 
 struct m3lb_solver {
   int lattice = 27, Q = 27, op = 0, eq = 0, storage = 0, shifted = 1, forcing = 0;
@@ -138,6 +146,7 @@ struct m3lb_solver {
   double omega = 1, omega2 = -1, fx = 0, fy = 0, fz = 0;
   bool node_kernel = false;
   int kernel = M3LB_KERNEL_AUTO;     // M3LB_OPT_KERNEL
+  long long wait_cycles = 0;         // M3LB_OPT_WAIT_CYCLES (test only; 0 = default)
   const Launchers* L = nullptr;
 
   long long n_interior() const { return (long long)g.nx * g.ny * g.nz; }
@@ -151,6 +160,7 @@ struct m3lb_solver {
     a.omega = omega; a.omega2 = omega2;
     a.fx = forcing ? fx : 0; a.fy = forcing ? fy : 0; a.fz = forcing ? fz : 0;
     a.err = err;
+    a.wait_cycles = wait_cycles;
     if (forcing && temp) {
       a.temp = temp;
       a.bgx = bg[0]; a.bgy = bg[1]; a.bgz = bg[2];
@@ -165,18 +175,22 @@ struct m3lb_solver {
     if (node_kernel || !chunk_ok() || kernel == M3LB_KERNEL_NODES) return kKernelNodes;
     // the streamed kernel addresses rows with 32-bit element counts
     const bool rows32 = (long long)g.nch * Q * 64 < (1LL << 31);
-    // the row kernel: whole rows of at most 4 chunks (the last may be partial)
-    const bool rows_ok = g.nch <= 4 &&
-                         4LL * Q * 256 * elem_bytes(storage) + 64 <= 227LL * 1024;
+    // the row kernel: whole rows of at most 8 chunks with 16-bit storage, 4
+    // with 32- or 64-bit storage (the last chunk may be partial), in stages
+    // of 2, 4 or 8 chunks that must fit a CTA's shared memory
+    const int lw = g.nch <= 2 ? 2 : (g.nch <= 4 ? 4 : 8);
+    const bool rows_ok = g.nch <= (elem_bytes(storage) == 2 ? 8 : 4) &&
+                         4LL * Q * lw * 64 * elem_bytes(storage) + 80 <= 227LL * 1024;
     if (kernel == M3LB_KERNEL_ROWS && rows_ok) return kKernelRows;
     if (kernel == M3LB_KERNEL_STREAM && rows32) return kKernelStream;
     // auto, from measurements on B200: with 16-bit storage the row kernel
-    // for rows of 3 or 4 chunks (256^3 CM: 0.34 ms against 0.49 ms for
-    // the paired kernel), else the streamed kernel for BGK/TRT and pure
-    // streaming; the paired kernel for everything else (32/64-bit storage
-    // is already near the copy bandwidth with it)
-    const bool narrow = storage == M3LB_STORE_F16 || storage == M3LB_STORE_BF16;
-    if (kernel == M3LB_KERNEL_AUTO && narrow && rows_ok && g.nch >= 3) return kKernelRows;
+    // for rows of at least kAutoRowsMinChunks chunks (256^3 CM: 0.34 ms
+    // against 0.49 ms for the paired kernel), else the streamed kernel for
+    // BGK/TRT and pure streaming; the paired kernel for everything else
+    // (32/64-bit storage is already near the copy bandwidth with it)
+    const bool narrow = elem_bytes(storage) == 2;
+    if (kernel == M3LB_KERNEL_AUTO && narrow && rows_ok && g.nch >= kAutoRowsMinChunks)
+      return kKernelRows;
     if (kernel == M3LB_KERNEL_AUTO && rows32 && narrow && op <= M3LB_OP_TRT) return kKernelStream;
     return kKernelPairs;
   }
@@ -208,7 +222,7 @@ int m3lb_create(int lattice, int nx, int ny, int nz, int px, int py, int pz, int
   if (op < M3LB_OP_NONE || op > M3LB_OP_CM) return fail(M3LB_ERR_INVALID, "create: bad operator %d", op);
   if (eq != 0 && eq != 1) return fail(M3LB_ERR_INVALID, "create: bad equilibrium %d", eq);
   if (!elem_bytes(storage)) return fail(M3LB_ERR_INVALID, "create: bad storage %d", storage);
-  if (!shifted && op != M3LB_OP_NONE && (storage == M3LB_STORE_F16 || storage == M3LB_STORE_BF16))
+  if (!shifted && op != M3LB_OP_NONE && elem_bytes(storage) == 2)
     return fail(M3LB_ERR_UNSUPPORTED, "create: 16-bit storage holds shifted populations only");
   const long long npad = (long long)(nx + 2) * (ny + 2) * (nz + 2);
   if (npad > (1LL << 31)) return fail(M3LB_ERR_INVALID, "create: lattice exceeds 2^31 nodes");
@@ -706,6 +720,33 @@ int m3lb_reduce(m3lb_solver* h, double out[6]) {
   return M3LB_OK;
 }
 
+int m3lb_diagnostics(m3lb_solver* h, double out[3]) {
+  if (!h || !out) return fail(M3LB_ERR_INVALID, "diagnostics: null argument");
+  int rc = m3lb_macro_device(h, nullptr, nullptr, nullptr, nullptr);
+  if (rc) return rc;
+  DeviceGuard dg(h->device);
+  const Geo& g = h->g;
+  // one partial of three values per block fits the reduction scratch
+  // (nblocks partials of kReduceVals = 6)
+  const int nb = h->nblocks;
+  if (h->storage == M3LB_STORE_F64)
+    diag_kernel<double><<<nb, kDiagThreads, 0, h->stream>>>(
+        static_cast<const double*>(h->macro[1]), static_cast<const double*>(h->macro[2]),
+        static_cast<const double*>(h->macro[3]), g.nx, g.ny, g.nz, h->partials);
+  else
+    diag_kernel<float><<<nb, kDiagThreads, 0, h->stream>>>(
+        static_cast<const float*>(h->macro[1]), static_cast<const float*>(h->macro[2]),
+        static_cast<const float*>(h->macro[3]), g.nx, g.ny, g.nz, h->partials);
+  CUDA_TRY(cudaGetLastError());
+  diag_finish<<<1, 32, 0, h->stream>>>(h->partials, nb, h->red_out);
+  CUDA_TRY(cudaGetLastError());
+  h->launches += 2;
+  CUDA_TRY(cudaMemcpyAsync(out, h->red_out, kDiagVals * sizeof(double), cudaMemcpyDeviceToHost,
+                           h->stream));
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return M3LB_OK;
+}
+
 static int gather_impl(m3lb_solver* h, double* out, void* raw) {
   DeviceGuard dg(h->device);
   const size_t n = (size_t)h->g.n_padded * h->Q;
@@ -811,6 +852,11 @@ int m3lb_set_option(m3lb_solver* h, int option, int value) {
     if (value < M3LB_KERNEL_AUTO || value > M3LB_KERNEL_ROWS)
       return fail(M3LB_ERR_INVALID, "set_option: bad kernel %d", value);
     h->kernel = value;
+    return M3LB_OK;
+  }
+  if (option == M3LB_OPT_WAIT_CYCLES) {
+    if (value < 0) return fail(M3LB_ERR_INVALID, "set_option: negative wait %d", value);
+    h->wait_cycles = value;
     return M3LB_OK;
   }
   return fail(M3LB_ERR_INVALID, "set_option: unknown option %d", option);

@@ -366,14 +366,17 @@ __device__ __forceinline__ void collide_moments(V* f, Macro<V>& m, const Collide
 
   // ---- order <= 2 moments in the product basis at u_b
   V K0, K1[3], K2d[3], K2s[3];  // K2s: 110 101 011
-  const V mc = mul(bc<V>(-cs2), N[0]);
+  // the -cs2 rho term enters each diagonal moment through one explicit FMA:
+  // as a separate product followed by an add, the compiler could fuse the
+  // two in the paired kernels only (lbm_common.cuh)
+  const V mcs = bc<V>(-cs2);
   K0 = N[0];
   if constexpr (central) {
 #pragma unroll
     for (int a = 0; a < 3; ++a) K1[a] = fma(neg(u[a]), N[0], N[1 + a]);
 #pragma unroll
     for (int a = 0; a < 3; ++a)
-      K2d[a] = add(fma(neg(u[a]), add(N[1 + a], K1[a]), N[4 + a]), mc);
+      K2d[a] = fma(mcs, N[0], fma(neg(u[a]), add(N[1 + a], K1[a]), N[4 + a]));
     K2s[0] = fma(neg(u[1]), K1[0], fma(neg(u[0]), N[2], N[7]));
     K2s[1] = fma(neg(u[2]), K1[0], fma(neg(u[0]), N[3], N[8]));
     K2s[2] = fma(neg(u[2]), K1[1], fma(neg(u[1]), N[3], N[9]));
@@ -381,7 +384,7 @@ __device__ __forceinline__ void collide_moments(V* f, Macro<V>& m, const Collide
 #pragma unroll
     for (int a = 0; a < 3; ++a) K1[a] = N[1 + a];
 #pragma unroll
-    for (int a = 0; a < 3; ++a) K2d[a] = add(N[4 + a], mc);
+    for (int a = 0; a < 3; ++a) K2d[a] = fma(mcs, N[0], N[4 + a]);
     K2s[0] = N[7];
     K2s[1] = N[8];
     K2s[2] = N[9];

@@ -65,8 +65,13 @@ __host__ __device__ constexpr int dir_of(int x, int y, int z) {
 
 // ---------------------------------------------------------- storage formats
 // Population storage: the element type in HBM.  Arithmetic is FP32 for the
-// 32- and 16-bit formats and FP64 for the 64-bit one.
-enum Store : int { kF32 = 0, kF16 = 1, kBF16 = 2, kF64 = 3 };
+// 32- and 16-bit formats and FP64 for the 64-bit one.  kF16C is the 16-bit
+// float below with one more mantissa bit than IEEE binary16.
+enum Store : int { kF32 = 0, kF16 = 1, kBF16 = 2, kF64 = 3, kF16C = 4 };
+
+// FP16C element: 1 sign bit, 4 exponent bits (bias 15), 11 mantissa bits,
+// subnormals, no infinities or NaN (codec below).
+struct f16c { uint16_t bits; };
 
 template <int S> struct StoreT;
 template <> struct StoreT<kF32> {
@@ -81,16 +86,21 @@ template <> struct StoreT<kF16> {
 template <> struct StoreT<kBF16> {
   using elem = __nv_bfloat16; using word = uint32_t; using real = float; using half_word = uint16_t;
 };
+template <> struct StoreT<kF16C> {
+  using elem = f16c; using word = uint32_t; using real = float; using half_word = uint16_t;
+};
 
 // ------------------------------------------------------ packed arithmetic
 // Two adjacent nodes are updated together with sm_100's paired FP32 ops
 // (add/mul/fma .f32x2), one instruction for both lanes.  Every operation is
 // an explicitly rounded IEEE op, so the paired path and the one-node path
-// give bitwise identical results.  The paired ops are issued as PTX
-// `mul/add/fma.rn.f32x2`: with the __fmul2_rn / __fadd2_rn intrinsics a
-// paired product feeding a paired sum was fused into one f32x2 FMA (one
-// rounding instead of two), which made the moment operators differ from the
-// one-node kernel by a few ulp; the explicit `.rn` form is never contracted.
+// give bitwise identical results.  One exception had to be written around:
+// a paired product whose only use is a paired add can be fused into one
+// f32x2 FMA by the compiler (seen with both the __fmul2_rn / __fadd2_rn
+// intrinsics and the `.rn` PTX below), one rounding instead of two, which the
+// scalar __fmul_rn / __fadd_rn never are.  The one place the operators had
+// that shape (the -cs2 * rho term of the second-order central moments,
+// lbm_collide.cuh) is written as an explicit FMA in both paths.
 struct f2 { float2 v; };
 
 __device__ __forceinline__ unsigned long long f2_bits(float2 v) {
@@ -179,11 +189,65 @@ __device__ __forceinline__ uint32_t pack_bf16(f2 v) {
   return *reinterpret_cast<uint32_t*>(&h);
 }
 
+// FP16C: a 16-bit float for shifted populations that gives IEEE binary16's
+// top exponent bit to the mantissa (the customised 16-bit number format of
+// Lehmann et al. 2022, "Accuracy and performance of the lattice Boltzmann
+// method with 64-bit, 32-bit, and customized 16-bit number formats"):
+// 1 sign bit, 4 exponent bits with bias 15, 11 mantissa bits and subnormals;
+// largest magnitude 2 - 2^-11, smallest normal 2^-14, subnormal step 2^-25;
+// no infinities or NaN.  Shifted populations f - w stay far inside |x| < 2,
+// so the range IEEE binary16 spends above 2 buys nothing here, while the
+// extra mantissa bit halves every stored rounding error.  Encoding rounds to
+// nearest with ties away from zero and saturates larger magnitudes (and NaN)
+// at +-(2 - 2^-11).
+//
+// Codec through the FP32 bit pattern.  Scaled by 2^-112, a value of the
+// format is exactly the FP32 number with bits  sign | code << 12  (the
+// format's exponent bias 15 is FP32's 127 - 112, and its subnormals are FP32
+// subnormals), so decoding is an arithmetic shift, a mask and a multiply by
+// 2^112 (paired for the two values of a word), and encoding a clamp of the
+// magnitude, a multiply by 2^-112, one integer multiply-add that shifts the
+// code into the top half and adds the rounding bit, the sign, and one byte
+// permute that packs the two codes.
+constexpr float kF16CMax = 1.99951171875f;  // 2 - 2^-11
+constexpr float kF16CUp = 0x1p112f;
+constexpr float kF16CDown = 0x1p-112f;
+
+// FP32 bits of the scaled value of the code in bits 31..16 of w
+__device__ __forceinline__ uint32_t f16c_hi_bits(uint32_t w) {
+  return (uint32_t)((int32_t)w >> 4) & 0x87fff000u;
+}
+// The code of the scaled magnitude bits t (FP32 bits of |x| 2^-112), rounded,
+// in bits 30..16, with the sign of x in bit 31; bits 15..0 are rounding
+// residue
+__device__ __forceinline__ uint32_t f16c_code_hi(uint32_t t, float x) {
+  return (t * 16u + 0x8000u) | (__float_as_uint(x) & 0x80000000u);
+}
+__device__ __forceinline__ f2 unpack_f16c(uint32_t w) {
+  const float a = __uint_as_float(f16c_hi_bits(w << 16));
+  const float b = __uint_as_float(f16c_hi_bits(w));
+  return f2{mul2_rn(make_float2(a, b), make_float2(kF16CUp, kF16CUp))};
+}
+__device__ __forceinline__ uint32_t pack_f16c(f2 v) {
+  const float2 m = make_float2(fminf(fabsf(v.v.x), kF16CMax), fminf(fabsf(v.v.y), kF16CMax));
+  const float2 t = mul2_rn(m, make_float2(kF16CDown, kF16CDown));
+  return __byte_perm(f16c_code_hi(__float_as_uint(t.x), v.v.x),
+                     f16c_code_hi(__float_as_uint(t.y), v.v.y), 0x7632);
+}
+__device__ __forceinline__ float f16c_to_float(uint16_t c) {
+  return __fmul_rn(__uint_as_float(f16c_hi_bits((uint32_t)c << 16)), kF16CUp);
+}
+__device__ __forceinline__ uint16_t f16c_from_float(float x) {
+  const float t = __fmul_rn(fminf(fabsf(x), kF16CMax), kF16CDown);
+  return (uint16_t)(f16c_code_hi(__float_as_uint(t), x) >> 16);
+}
+
 // Scalar element <-> arithmetic type.
 __device__ __forceinline__ float to_real(float e) { return e; }
 __device__ __forceinline__ double to_real(double e) { return e; }
 __device__ __forceinline__ float to_real(__half e) { return __half2float(e); }
 __device__ __forceinline__ float to_real(__nv_bfloat16 e) { return __bfloat162float(e); }
+__device__ __forceinline__ float to_real(f16c e) { return f16c_to_float(e.bits); }
 template <class E> __device__ __forceinline__ E from_real(float v);
 template <class E> __device__ __forceinline__ E from_real(double v);
 template <> __device__ __forceinline__ float from_real<float>(float v) { return v; }
@@ -191,6 +255,10 @@ template <> __device__ __forceinline__ double from_real<double>(double v) { retu
 template <> __device__ __forceinline__ __half from_real<__half>(float v) { return __float2half_rn(v); }
 template <> __device__ __forceinline__ __nv_bfloat16 from_real<__nv_bfloat16>(float v) {
   return __float2bfloat16_rn(v);
+}
+template <> __device__ __forceinline__ f16c from_real<f16c>(float v) { return f16c{f16c_from_float(v)}; }
+template <> __device__ __forceinline__ f16c from_real<f16c>(double v) {
+  return f16c{f16c_from_float((float)v)};
 }
 template <> __device__ __forceinline__ double from_real<double>(float v) { return (double)v; }
 template <> __device__ __forceinline__ float from_real<float>(double v) { return (float)v; }
@@ -252,6 +320,8 @@ struct StepArgs {
   double omega, omega2;    // BGK/TRT/MRT/CM rates (TRT: omega_p, omega_m; moments: omega, bulk)
   double fx, fy, fz;       // uniform Guo body force
   int* err;                // device status word: a kernel whose bounded wait ran out sets it
+  long long wait_cycles;   // limit of the row kernel's wait for a row's copies (0: ~2 s);
+                           // shorter only to test the timeout path
   // Boussinesq buoyancy (BoussinesqGuo, src/forcing/Forcing.hpp:93-127): the
   // force at a node is (fx, fy, fz) + g rho0 beta (T - T0) with T per
   // interior node in the arithmetic type; temp == nullptr: (fx, fy, fz) alone

@@ -1,6 +1,6 @@
 // Kernel instantiations and launchers for one (lattice, storage format),
 // selected at compile time:
-//   -DM3LB_LAT=D2Q9|D3Q27 -DM3LB_ST=kF32|kF16|kBF16|kF64 -DM3LB_NAME=launchers_<...>
+//   -DM3LB_LAT=D2Q9|D3Q27 -DM3LB_ST=kF32|kF16|kBF16|kF64|kF16C -DM3LB_NAME=launchers_<...>
 #include "lbm_kernels.cuh"
 #include <cudaTypedefs.h>
 
@@ -99,40 +99,57 @@ cudaError_t rows_maps(const StepArgs& a, RowMaps<L>* maps) {
   return cudaSuccess;
 }
 
-// Persistent row kernel: one CTA of nch warps per row, as many CTAs as are
-// resident (occupancy queried once per device and row width).
+// Persistent row kernel: one CTA of nch update warps and one copy warp per
+// row, stages of LW chunks (the smallest of 2, 4, 8 that holds the row), as
+// many CTAs as are resident (occupancy queried once per device and shape).
+template <int OP, int EQ, bool SH, bool FORCE, int LW>
+cudaError_t launch_rows_lw(const StepArgs& a, cudaStream_t s) {
+  using Cfg = RowsCfg<L, ST, LW>;
+  if constexpr (Cfg::SMEM > kRowsSmemMax) {
+    return cudaErrorInvalidValue;
+  } else {
+    const Geo& g = a.g;
+    auto kern = step_rows<L, ST, OP, EQ, SH, FORCE, LW>;
+    const int threads = (g.nch + 1) * 32;
+    constexpr int kMaxDev = 64;
+    static int cached[kMaxDev][LW + 1];
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= kMaxDev) return cudaErrorInvalidDevice;
+    if (cached[dev][g.nch] == 0) {
+      e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, Cfg::SMEM);
+      if (e != cudaSuccess) return e;
+      int per_sm = 0, nsm = 0;
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, Cfg::SMEM);
+      if (e != cudaSuccess) return e;
+      e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+      if (e != cudaSuccess) return e;
+      if (per_sm < 1) return cudaErrorInvalidConfiguration;
+      cached[dev][g.nch] = per_sm * nsm;
+    }
+    RowMaps<L> maps;
+    e = rows_maps(a, &maps);
+    if (e != cudaSuccess) return e;
+    const long long rows = (long long)g.ny * g.nz;
+    const unsigned grid = (unsigned)(rows < cached[dev][g.nch] ? rows : cached[dev][g.nch]);
+    kern<<<grid, threads, Cfg::SMEM, s>>>(a, maps);
+    return cudaGetLastError();
+  }
+}
 template <int OP, int EQ, bool SH, bool FORCE>
 cudaError_t launch_rows(const StepArgs& a, cudaStream_t s) {
-  using Cfg = RowsCfg<L, ST>;
   const Geo& g = a.g;
-  if (g.nch < 1 || g.nch > kRowsMaxWarps || (g.nx % 2) != 0 || Cfg::SMEM > kRowsSmemMax)
-    return cudaErrorInvalidValue;
-  auto kern = step_rows<L, ST, OP, EQ, SH, FORCE>;
-  const int threads = g.nch * 32;
-  constexpr int kMaxDev = 64;
-  static int cached[kMaxDev][kRowsMaxWarps + 1];
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) return e;
-  if (dev < 0 || dev >= kMaxDev) return cudaErrorInvalidDevice;
-  if (cached[dev][g.nch] == 0) {
-    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, Cfg::SMEM);
-    if (e != cudaSuccess) return e;
-    int per_sm = 0, nsm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, Cfg::SMEM);
-    if (e != cudaSuccess) return e;
-    e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    if (e != cudaSuccess) return e;
-    if (per_sm < 1) return cudaErrorInvalidConfiguration;
-    cached[dev][g.nch] = per_sm * nsm;
+  if (g.nch < 1 || g.nch > kRowsMaxChunks || (g.nx % 2) != 0) return cudaErrorInvalidValue;
+  switch (rows_lw(g.nch)) {
+    case 2: return launch_rows_lw<OP, EQ, SH, FORCE, 2>(a, s);
+    case 4: return launch_rows_lw<OP, EQ, SH, FORCE, 4>(a, s);
+    default:
+      // 8-chunk stages hold 16-bit rows only (FP32 fits one CTA per SM,
+      // FP64 none)
+      if constexpr (sizeof(typename WordOps<ST>::E) == 2) return launch_rows_lw<OP, EQ, SH, FORCE, 8>(a, s);
+      else return cudaErrorInvalidValue;
   }
-  RowMaps<L> maps;
-  e = rows_maps(a, &maps);
-  if (e != cudaSuccess) return e;
-  const long long rows = (long long)g.ny * g.nz;
-  const unsigned grid = (unsigned)(rows < cached[dev][g.nch] ? rows : cached[dev][g.nch]);
-  kern<<<grid, threads, Cfg::SMEM, s>>>(a, maps);
-  return cudaGetLastError();
 }
 
 template <int OP, int EQ, bool SH, bool FORCE>

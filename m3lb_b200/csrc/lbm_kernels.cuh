@@ -96,10 +96,14 @@ __device__ __forceinline__ void store_macro_pair(const StepArgs& a, size_t kk, c
 
 // ------------------------------------------------------------ word traits
 // A word holds one direction of two x-adjacent nodes (lo = even x).
+// unpack(w) decodes the two elements of a word; unpack_join(a, b) decodes
+// the pair (hi element of a, lo element of b), the x-shifted pair that
+// straddles two words, without first joining them.
 template <int ST> struct WordOps;
 template <> struct WordOps<kF32> {
   using W = float2; using H = float; using V = f2; using E = float;
   static __device__ __forceinline__ V unpack(W w) { return f2{w}; }
+  static __device__ __forceinline__ V unpack_join(W a, W b) { return f2{make_float2(a.y, b.x)}; }
   static __device__ __forceinline__ W pack(V v) { return v.v; }
   static __device__ __forceinline__ H lo(W w) { return w.x; }
   static __device__ __forceinline__ H hi(W w) { return w.y; }
@@ -108,6 +112,7 @@ template <> struct WordOps<kF32> {
 template <> struct WordOps<kF64> {
   using W = double2; using H = double; using V = d2; using E = double;
   static __device__ __forceinline__ V unpack(W w) { return {w.x, w.y}; }
+  static __device__ __forceinline__ V unpack_join(W a, W b) { return {a.y, b.x}; }
   static __device__ __forceinline__ W pack(V v) { return make_double2(v.x, v.y); }
   static __device__ __forceinline__ H lo(W w) { return w.x; }
   static __device__ __forceinline__ H hi(W w) { return w.y; }
@@ -116,7 +121,23 @@ template <> struct WordOps<kF64> {
 template <> struct WordOps<kF16> {
   using W = uint32_t; using H = uint16_t; using V = f2; using E = __half;
   static __device__ __forceinline__ V unpack(W w) { return unpack_f16(w); }
+  static __device__ __forceinline__ V unpack_join(W a, W b) {
+    return f2{make_float2(__half2float(__ushort_as_half((unsigned short)(a >> 16))),
+                          __half2float(__ushort_as_half((unsigned short)(b & 0xffffu))))};
+  }
   static __device__ __forceinline__ W pack(V v) { return pack_f16(v); }
+  static __device__ __forceinline__ H lo(W w) { return (H)(w & 0xffffu); }
+  static __device__ __forceinline__ H hi(W w) { return (H)(w >> 16); }
+  static __device__ __forceinline__ W make(H l, H h) { return (W)l | ((W)h << 16); }
+};
+template <> struct WordOps<kF16C> {
+  using W = uint32_t; using H = uint16_t; using V = f2; using E = f16c;
+  static __device__ __forceinline__ V unpack(W w) { return unpack_f16c(w); }
+  static __device__ __forceinline__ V unpack_join(W a, W b) {
+    const float lo = __uint_as_float(f16c_hi_bits(a)), hi = __uint_as_float(f16c_hi_bits(b << 16));
+    return f2{mul2_rn(make_float2(lo, hi), make_float2(kF16CUp, kF16CUp))};
+  }
+  static __device__ __forceinline__ W pack(V v) { return pack_f16c(v); }
   static __device__ __forceinline__ H lo(W w) { return (H)(w & 0xffffu); }
   static __device__ __forceinline__ H hi(W w) { return (H)(w >> 16); }
   static __device__ __forceinline__ W make(H l, H h) { return (W)l | ((W)h << 16); }
@@ -124,6 +145,9 @@ template <> struct WordOps<kF16> {
 template <> struct WordOps<kBF16> {
   using W = uint32_t; using H = uint16_t; using V = f2; using E = __nv_bfloat16;
   static __device__ __forceinline__ V unpack(W w) { return unpack_bf16(w); }
+  static __device__ __forceinline__ V unpack_join(W a, W b) {
+    return f2{make_float2(__uint_as_float(a & 0xffff0000u), __uint_as_float(b << 16))};
+  }
   static __device__ __forceinline__ W pack(V v) { return pack_bf16(v); }
   static __device__ __forceinline__ H lo(W w) { return (H)(w & 0xffffu); }
   static __device__ __forceinline__ H hi(W w) { return (H)(w >> 16); }

@@ -11,8 +11,8 @@ namespace m3lb {
 // Step kernels: one node per thread (any geometry), and, for a periodic x
 // axis with even nx, the paired kernel (one warp per 64-node chunk) or its
 // persistent, copy-pipelined form.
-// The row kernel moves whole rows with the tensor-memory accelerator (nx a
-// multiple of 64, at most 8 chunks per row).
+// The row kernel moves whole rows with the tensor-memory accelerator
+// (16-bit storage; the row widths it takes are in lbm_capi.cu).
 enum StepKernel { kKernelNodes = 1, kKernelPairs = 2, kKernelStream = 3, kKernelRows = 4 };
 
 struct Launchers {
@@ -37,10 +37,12 @@ M3LB_DECLARE_LAUNCHERS(launchers_D2Q9_F32)
 M3LB_DECLARE_LAUNCHERS(launchers_D2Q9_F16)
 M3LB_DECLARE_LAUNCHERS(launchers_D2Q9_BF16)
 M3LB_DECLARE_LAUNCHERS(launchers_D2Q9_F64)
+M3LB_DECLARE_LAUNCHERS(launchers_D2Q9_F16C)
 M3LB_DECLARE_LAUNCHERS(launchers_D3Q27_F32)
 M3LB_DECLARE_LAUNCHERS(launchers_D3Q27_F16)
 M3LB_DECLARE_LAUNCHERS(launchers_D3Q27_BF16)
 M3LB_DECLARE_LAUNCHERS(launchers_D3Q27_F64)
+M3LB_DECLARE_LAUNCHERS(launchers_D3Q27_F16C)
 #undef M3LB_DECLARE_LAUNCHERS
 
 }  // namespace m3lb

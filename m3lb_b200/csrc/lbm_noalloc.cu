@@ -134,7 +134,7 @@ extern "C" int m3lb_reduce_static(int lattice, int nx, int ny, int nz, int px, i
   if (lattice == 9 && nz != 1) return fail(M3LB_ERR_INVALID, "reduce_static: D2Q9 needs nz == 1");
   if (nx < 1 || ny < 1 || nz < 1 || op < M3LB_OP_NONE || op > M3LB_OP_CM)
     return fail(M3LB_ERR_INVALID, "reduce_static: bad extent or operator");
-  if (!shifted && op != M3LB_OP_NONE && (storage == M3LB_STORE_F16 || storage == M3LB_STORE_BF16))
+  if (!shifted && op != M3LB_OP_NONE && elem_bytes(storage) == 2)
     return fail(M3LB_ERR_UNSUPPORTED, "reduce_static: 16-bit storage holds shifted populations only");
   const long long nint = (long long)nx * ny * nz;
   if (nint > kStaticMaxNodes) {

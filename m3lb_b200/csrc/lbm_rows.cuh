@@ -24,13 +24,18 @@
 //     row in the update itself;
 //   * rows are independent: CTAs never exchange data, and a row's global
 //     lines are read and written only by its own CTA within a step.
-// Warp w of a CTA takes chunk w of the row (nch <= 4 warps, nx even,
-// periodic x; lanes past nx in a partial last chunk store nothing).  Rows stream through a kRowsStages-stage ring with the
-// rows ahead of the one being updated in flight.
+// A CTA is nch update warps (warp k takes chunk k of the row; nx even,
+// periodic x; lanes past nx in a partial last chunk store nothing) and one
+// copy warp that moves the rows through a ring of kRowsStages stages: it
+// loads the rows ahead, and once every update warp has marked a row done it
+// stores the row and reloads the stage.  The stage is sized for LW chunks
+// (2, 4 or 8), the smallest that holds the row, so short rows keep more
+// CTAs resident.
 //
-// Waits on the load barriers are bounded: past the limit the CTA records a
-// status in StepArgs::err, lets its copies in flight finish (bounded again)
-// and leaves; the host reports it at the next m3lb_sync.
+// Waits are bounded: past the limit a warp records a status in
+// StepArgs::err and raises the CTA's abort flag, the copy warp lets its
+// copies in flight finish (bounded again) and the CTA leaves; the host
+// reports the status at the next m3lb_sync.
 #pragma once
 #include <cuda.h>
 
@@ -39,9 +44,9 @@
 namespace m3lb {
 
 constexpr int kRowsStages = 4;
-constexpr int kRowsMaxWarps = 4;  // nch <= 4 (nx <= 256)
-constexpr int kRowsLine = kRowsMaxWarps * kChunk;  // shared elements reserved per line
+constexpr int kRowsMaxChunks = 8;  // nch <= 8 (nx <= 512)
 constexpr long long kRowsWaitCycles = 4000000000LL;  // ~2 s at 2 GHz
+constexpr uint32_t kRowsSuspendNs = 20000;            // longest suspension per barrier test
 constexpr int kRowsSmemMax = 227 * 1024;              // dynamic shared memory per CTA
 
 // ---------------------------------------------------------------- plan
@@ -112,11 +117,12 @@ struct RowSlots {
       if (Pl::ops[o].q0 + j * Pl::ops[o].stride == q) return j;
     return -1;
   }
-  // first shared element of a copy's block: blocks in op order, each
-  // count * kRowsLine elements (the row's [nch][count][64] at its start)
-  static __host__ __device__ constexpr int base_of(int o) {
+  // first shared element of a copy's block in a stage of LW-chunk lines:
+  // blocks in op order, each count * LW * 64 elements (the row's
+  // [nch][count][64] at its start)
+  static __host__ __device__ constexpr int base_of(int o, int lw) {
     int b = 0;
-    for (int p = 0; p < o; ++p) b += Pl::ops[p].count * kRowsLine;
+    for (int p = 0; p < o; ++p) b += Pl::ops[p].count * lw * kChunk;
     return b;
   }
   // every value has a copy, every copy of a neighbour row is that value's
@@ -145,13 +151,18 @@ struct RowMaps {
   CUtensorMap m[RowPlan<L>::NMAPS];
 };
 
-template <class L, int ST>
+// Shared memory of a CTA: kRowsStages stages of Q lines of LW chunks, then
+// the barriers (full[s]: the stage's loads landed; empty[s]: every update
+// warp is done with the stage's row) and the abort flag.
+template <class L, int ST, int LW>
 struct RowsCfg {
   using E = typename WordOps<ST>::E;
-  static constexpr int STAGE_BYTES = L::Q * kRowsLine * (int)sizeof(E);
-  static constexpr int SMEM = kRowsStages * STAGE_BYTES + 64;  // + barriers, counters
+  static constexpr int STAGE_BYTES = L::Q * LW * kChunk * (int)sizeof(E);
+  static constexpr int SMEM = kRowsStages * STAGE_BYTES + 2 * kRowsStages * 8 + 16;
   static __host__ __device__ int row_bytes(int nch) { return L::Q * nch * kChunk * (int)sizeof(E); }
 };
+// Line width (chunks per stage line) for a row of nch chunks.
+__host__ __device__ constexpr int rows_lw(int nch) { return nch <= 2 ? 2 : (nch <= 4 ? 4 : 8); }
 
 // ------------------------------------------------------------- primitives
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
@@ -164,22 +175,35 @@ __device__ __forceinline__ void mbar_expect_tx(uint32_t bar, int bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes)
                : "memory");
 }
-__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, int parity) {
+// Whether phase `parity` of a barrier has completed, without waiting.
+__device__ __forceinline__ bool mbar_test(uint32_t bar, int parity) {
   uint32_t ok;
   asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n"
       " selp.u32 %0, 1, 0, p;\n}\n"
       : "=r"(ok) : "r"(bar), "r"(parity) : "memory");
   return ok != 0;
 }
-// Bounded wait for phase `parity` of a barrier; false if the limit passed.
-__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, int parity) {
-  if (mbar_try_wait(bar, parity)) return true;
+// The same test, letting the hardware suspend the warp until the phase
+// completes or kRowsSuspendNs pass, so a waiting warp issues no spin loop.
+__device__ __forceinline__ bool mbar_try_wait_sleep(uint32_t bar, int parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok) : "r"(bar), "r"(parity), "r"(kRowsSuspendNs) : "memory");
+  return ok != 0;
+}
+// Bounded wait for phase `parity` of a barrier: true once the phase has
+// completed, false when `limit` clock cycles passed first (after a first
+// test that never waits).
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, int parity,
+                                                  long long limit = kRowsWaitCycles) {
+  if (mbar_test(bar, parity)) return true;
   const long long t0 = clock64();
-  for (;;) {
-    if (mbar_try_wait(bar, parity)) return true;
-    if (clock64() - t0 > kRowsWaitCycles) return false;
-  }
+  while (clock64() - t0 < limit)
+    if (mbar_try_wait_sleep(bar, parity)) return true;
+  return false;
 }
 // One copy: the box of `map` at (x 0, direction q, chunk c), into dst.
 __device__ __forceinline__ void tma_load_box(uint32_t dst, const CUtensorMap* map, int q, int c,
@@ -230,7 +254,7 @@ struct RowCursor {
 // The copies of one row by the calling thread.  LOAD: global -> stage
 // (completion on `bar`, whose expected bytes the caller has set); else
 // stage -> global, in one bulk group of this thread.
-template <class L, int ST, bool LOAD>
+template <class L, int ST, int LW, bool LOAD>
 __device__ __forceinline__ void rows_copy(const Geo& g, const RowMaps<L>& maps, int P,
                                           const RowCursor& rc, uint32_t stage, uint32_t bar) {
   using Pl = RowPlan<L>;
@@ -247,27 +271,52 @@ __device__ __forceinline__ void rows_copy(const Geo& g, const RowMaps<L>& maps, 
       if (rz < 0) rz += g.nz; else if (rz >= g.sz) rz -= g.nz;
     }
     const int q = op.q0 + op.sgn * P;
-    const uint32_t dst = stage + (uint32_t)(RowSlots<L>::base_of(o) * (int)sizeof(E));
+    const uint32_t dst = stage + (uint32_t)(RowSlots<L>::base_of(o, LW) * (int)sizeof(E));
     if constexpr (LOAD) tma_load_box(dst, &maps.m[op.map], q, row_chunk(g, ry, rz), bar);
     else tma_store_box(&maps.m[op.map], q, row_chunk(g, ry, rz), dst);
   });
   if constexpr (!LOAD) bulk_commit();
 }
 
-// BGK/TRT keep more values live than the moment operators (as in the paired
-// kernel): let them use more registers at fewer resident CTAs.
-template <int OP, int ST>
-constexpr int rows_min_blocks() {
-  return (OP == 1 || OP == 2 || ST == kF64) ? 1 : 4;
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ bool flag_set(const int* f) {
+  return *reinterpret_cast<const volatile int*>(f) != 0;
+}
+// A bounded barrier wait that also gives up once the CTA's abort flag is set.
+__device__ __forceinline__ bool rows_wait(uint32_t bar, int parity, long long limit,
+                                          const int* abort_flag) {
+  if (mbar_test(bar, parity)) return true;
+  const long long t0 = clock64();
+  while (clock64() - t0 < limit) {
+    if (mbar_try_wait_sleep(bar, parity)) return true;
+    if (flag_set(abort_flag)) return false;
+  }
+  return false;
 }
 
-// Rows stream through a ring of kRowsStages stage buffers; stage s holds
-// rows j = s, s + kRowsStages, ... of this CTA.  There is no CTA-wide
-// barrier per row: each warp, when done with row j, counts itself in
-// done[s]; the last warp to finish moves the row (stores it, waits until the
-// stores have read the stage, then loads row j + kRowsStages into it).
-template <class L, int ST, int OP, int EQ, bool SH, bool FORCE>
-__global__ void __launch_bounds__(kRowsMaxWarps * 32, rows_min_blocks<OP, ST>())
+// Resident CTAs per SM the launch bounds ask for: the moment operators fit
+// their registers at the occupancy the stage size allows (16-bit storage,
+// LW 2: 8 CTAs of 27.6 KB fit, registers allow 6; LW 4: 4 CTAs of 55 KB;
+// LW 8: 2 of 110 KB); BGK/TRT keep more values live (as in the paired
+// kernel) and take their registers at fewer resident CTAs.
+template <int OP, int ST, int LW>
+constexpr int rows_min_blocks() {
+  if (ST == kF64) return 1;
+  if (OP == 1 || OP == 2) return LW == 2 ? 4 : (LW == 4 ? 2 : 1);
+  if (ST == kF32) return LW == 2 ? 2 : 1;
+  return LW == 2 ? 6 : (LW == 4 ? 4 : 2);
+}
+
+// One CTA: warps 0 .. nch-1 update chunk k of each of the CTA's rows, warp
+// nch (lane 0) moves them.  Row j of the CTA sits in stage j % kRowsStages;
+// its load completes phase (j / kRowsStages) & 1 of full[s], and the update
+// warps' arrivals on empty[s] (one per warp) complete the same phase there,
+// after which the copy warp stores the row, waits until the stores have
+// read the stage, and loads row j + kRowsStages into it.
+template <class L, int ST, int OP, int EQ, bool SH, bool FORCE, int LW>
+__global__ void __launch_bounds__((LW + 1) * 32, rows_min_blocks<OP, ST, LW>())
 step_rows(StepArgs a, const __grid_constant__ RowMaps<L> maps) {
   using WO = WordOps<ST>;
   using W = typename WO::W;
@@ -275,47 +324,81 @@ step_rows(StepArgs a, const __grid_constant__ RowMaps<L> maps) {
   using E = typename WO::E;
   using V = typename WO::V;
   using S = typename Lanes<V>::S;
-  using Cfg = RowsCfg<L, ST>;
+  using Cfg = RowsCfg<L, ST, LW>;
   using Pl = RowPlan<L>;
   using Sl = RowSlots<L>;
   using XW = XWord<ST>;
   constexpr int Q = L::Q;
+  constexpr int NS = kRowsStages;
   const Geo& g = a.g;
 
   extern __shared__ __align__(128) unsigned char rows_smem[];
   const int lane = threadIdx.x & 31;
-  const int k = threadIdx.x >> 5;  // chunk of the row
-  const int nw = blockDim.x >> 5;  // == nch
+  const int k = threadIdx.x >> 5;  // chunk of the row; == nch for the copy warp
+  const int nch = g.nch;
   const int P = a.parity;
   const long long nrows = (long long)g.ny * g.nz;
-  const int rbytes = Cfg::row_bytes(g.nch);
-  uint64_t* bars = reinterpret_cast<uint64_t*>(rows_smem + kRowsStages * Cfg::STAGE_BYTES);
-  int* done = reinterpret_cast<int*>(bars + kRowsStages);  // warps finished with the stage's row
-  int* issued = done + kRowsStages;                        // loads issued into the stage
+  uint64_t* bars = reinterpret_cast<uint64_t*>(rows_smem + NS * Cfg::STAGE_BYTES);
+  int* abort_flag = reinterpret_cast<int*>(bars + 2 * NS);
   const uint32_t stage0 = smem_addr(rows_smem);
-  const uint32_t bar0 = smem_addr(bars);
+  const uint32_t full0 = smem_addr(bars), empty0 = full0 + 8 * NS;
   const int dyr = (int)(gridDim.x % g.ny), dzr = (int)(gridDim.x / g.ny);
 
-  RowCursor cur;
-  cur.start(blockIdx.x, g.ny);
   if (threadIdx.x == 0) {
-    for (int s = 0; s < kRowsStages; ++s) {
-      mbar_init(bar0 + 8 * s, 1);
-      done[s] = 0;
-      issued[s] = 0;
+    for (int s = 0; s < NS; ++s) {
+      mbar_init(full0 + 8 * s, 1);
+      mbar_init(empty0 + 8 * s, nch);
     }
+    *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
-    // prologue: this CTA's first kRowsStages rows in flight
-    RowCursor c = cur;
-    for (int s = 0; s < kRowsStages && c.r < nrows; ++s) {
-      mbar_expect_tx(bar0 + 8 * s, rbytes);
-      rows_copy<L, ST, true>(g, maps, P, c, stage0 + s * Cfg::STAGE_BYTES, bar0 + 8 * s);
-      issued[s] += 1;
-      c.advance(gridDim.x, dyr, dzr, g.ny);
-    }
   }
   __syncthreads();
 
+  RowCursor cur;
+  cur.start(blockIdx.x, g.ny);
+
+  // ------------------------------------------------------------ copy warp
+  if (k == nch) {
+    if (lane != 0) return;
+    const int rbytes = Cfg::row_bytes(nch);
+    RowCursor ld = cur;  // next row to load
+    int nl = 0, nst = 0;  // rows loaded, rows stored
+    bool failed = false;
+    for (; nl < NS && ld.r < nrows; ++nl) {
+      mbar_expect_tx(full0 + 8 * nl, rbytes);
+      rows_copy<L, ST, LW, true>(g, maps, P, ld, stage0 + nl * Cfg::STAGE_BYTES, full0 + 8 * nl);
+      ld.advance(gridDim.x, dyr, dzr, g.ny);
+    }
+    while (nst < nl) {
+      const int s = nst % NS;
+      if (!rows_wait(empty0 + 8 * s, (nst / NS) & 1, kRowsWaitCycles, abort_flag)) {
+        failed = true;
+        break;
+      }
+      rows_copy<L, ST, LW, false>(g, maps, P, cur, stage0 + s * Cfg::STAGE_BYTES, 0);
+      cur.advance(gridDim.x, dyr, dzr, g.ny);
+      ++nst;
+      if (ld.r < nrows) {
+        bulk_wait_read<0>();  // the stores no longer read the stage
+        mbar_expect_tx(full0 + 8 * s, rbytes);
+        rows_copy<L, ST, LW, true>(g, maps, P, ld, stage0 + s * Cfg::STAGE_BYTES, full0 + 8 * s);
+        ld.advance(gridDim.x, dyr, dzr, g.ny);
+        ++nl;
+      }
+    }
+    bulk_wait_all();  // every store has landed
+    if (failed || flag_set(abort_flag)) {
+      atomicExch(abort_flag, 1);
+      if (a.err) atomicExch(a.err, 1);
+      // loads issued for rows not stored yet land before the CTA's shared
+      // memory is released (bounded; the abort flag is not consulted here)
+      for (int r = nst; r < nl; ++r)
+        mbar_wait_bounded(full0 + 8 * (r % NS), (r / NS) & 1);
+    }
+    return;
+  }
+
+  // ---------------------------------------------------------- update warps
   // Per-lane element offsets of an x position inside a copy's block of
   // `count` lines ([chunk][count][64]): (x >> 6) * count * 64 + (x & 63).
   // The pair's word at x0, the words at x0 + 2 and x0 - 2 and the element
@@ -334,41 +417,42 @@ step_rows(StepArgs a, const __grid_constant__ RowMaps<L> maps) {
   constexpr int COWN = Pl::ops[1].count;
   const int p0_own = posc(x0, COWN);
   const CollideParams<S> prm{(S)a.omega, (S)a.omega2, (S)a.fx, (S)a.fy, (S)a.fz};
+  const long long consume_limit = a.wait_cycles > 0 ? a.wait_cycles : kRowsWaitCycles;
 
-  RowCursor ahead = cur;  // row j + kRowsStages, the next one for this stage
-  for (int t = 0; t < kRowsStages; ++t) ahead.advance(gridDim.x, dyr, dzr, g.ny);
   bool failed = false;
   for (int j = 0; cur.r < nrows; ++j) {
-    const int s = j % kRowsStages;
-    if (!mbar_wait_bounded(bar0 + 8 * s, (j / kRowsStages) & 1)) {
+    const int s = j % NS;
+    if (!rows_wait(full0 + 8 * s, (j / NS) & 1, consume_limit, abort_flag)) {
       failed = true;
       break;
     }
     E* sl = reinterpret_cast<E*>(rows_smem + s * Cfg::STAGE_BYTES);
 
-    // ---- the pair's 27 values from the shared blocks
+    // ---- the pair's 27 values from the shared blocks.  An x-shifted remote
+    // pair straddles two words: the collision operators decode it from both
+    // directly; pure streaming joins the two halves into one word.
     W w[Q];
-    w[0] = *reinterpret_cast<const W*>(sl + Sl::base_of(0) + p0_1);
+    V f[Q];
+    auto rd = [](const E* at) { return *reinterpret_cast<const W*>(at); };
+    w[0] = rd(sl + Sl::base_of(0, LW) + p0_1);
     static_for<1, Q, 2>([&](auto I) {
       constexpr int i = decltype(I)::value;
       constexpr int cx = L::cx[i];
       constexpr int ro = Sl::op_of(i + 1);
       constexpr int rc = Pl::ops[ro].count;
       static_assert(rc == 1 || rc == 2, "remote copies hold one or two lines");
-      const E* ol = sl + Sl::base_of(1) + Sl::j_of(i) * kChunk;
-      const E* rl = sl + Sl::base_of(ro) + Sl::j_of(i + 1) * kChunk;
+      const E* ol = sl + Sl::base_of(1, LW) + Sl::j_of(i) * kChunk;
+      const E* rl = sl + Sl::base_of(ro, LW) + Sl::j_of(i + 1) * kChunk;
       const int r0 = rc == 1 ? p0_1 : p0_2;
-      w[i] = *reinterpret_cast<const W*>(ol + p0_own);
+      w[i] = rd(ol + p0_own);
       if constexpr (cx == 0) {
-        w[i + 1] = *reinterpret_cast<const W*>(rl + r0);
-      } else if constexpr (cx > 0) {
-        // elements (x0 + 1, x0 + 2)
-        const int rn = rc == 1 ? pn_1 : pn_2;
-        w[i + 1] = XW::join(*reinterpret_cast<const W*>(rl + r0), *reinterpret_cast<const W*>(rl + rn));
+        w[i + 1] = rd(rl + r0);
       } else {
-        // elements (x0 - 1, x0)
-        const int rm = rc == 1 ? pm_1 : pm_2;
-        w[i + 1] = XW::join(*reinterpret_cast<const W*>(rl + rm), *reinterpret_cast<const W*>(rl + r0));
+        // elements (x0 + 1, x0 + 2), or (x0 - 1, x0)
+        const W a0 = cx > 0 ? rd(rl + r0) : rd(rl + (rc == 1 ? pm_1 : pm_2));
+        const W b0 = cx > 0 ? rd(rl + (rc == 1 ? pn_1 : pn_2)) : rd(rl + r0);
+        if constexpr (OP == 0) w[i + 1] = XW::join(a0, b0);
+        else f[i + 1] = WO::unpack_join(a0, b0);
       }
     });
 
@@ -381,9 +465,10 @@ step_rows(StepArgs a, const __grid_constant__ RowMaps<L> maps) {
     }
     Macro<V> m;
     if constexpr (OP != 0) {
-      V f[Q];
-#pragma unroll
-      for (int q = 0; q < Q; ++q) f[q] = WO::unpack(w[q]);
+      static_for<0, Q>([&](auto QQ) {
+        constexpr int q = decltype(QQ)::value;
+        if constexpr (q == 0 || (q % 2) == 1 || L::cx[q - 1] == 0) f[q] = WO::unpack(w[q]);
+      });
       if constexpr (FORCE) {  // the force per node of the pair (Boussinesq)
         CollideParams<S, V> pv{prm.omega, prm.omega2, bc<V>(prm.fx), bc<V>(prm.fy), bc<V>(prm.fz)};
         if (a.temp) {
@@ -405,77 +490,60 @@ step_rows(StepArgs a, const __grid_constant__ RowMaps<L> maps) {
     // ---- write back in place: f_{i+1}' to the own slot, f_i' to the
     // remote slot; solid / excluded nodes leave their slots as read
     // (halfway bounce-back, EsotericPull.hpp:27-33).  Each slot belongs to
-    // one lane, so lanes never write what another lane still reads.
-    const bool any_solid = __any_sync(0xffffffffu, solid0 || solid1);
-    auto put = [&](E* at, W v) {  // the pair's word
-      if (!any_solid) {
-        *reinterpret_cast<W*>(at) = v;
-      } else {
-        if (!solid0) *reinterpret_cast<H*>(at) = WO::lo(v);
-        if (!solid1) *reinterpret_cast<H*>(at + 1) = WO::hi(v);
-      }
+    // one lane, so lanes never write what another lane still reads.  A warp
+    // with no solid lane (the common case) stores without per-node tests.
+    auto store_all = [&](auto GUARD) {
+      constexpr bool G = decltype(GUARD)::value;
+      auto put = [&](E* at, W v) {  // the pair's word
+        if constexpr (!G) {
+          *reinterpret_cast<W*>(at) = v;
+        } else {
+          if (!solid0) *reinterpret_cast<H*>(at) = WO::lo(v);
+          if (!solid1) *reinterpret_cast<H*>(at + 1) = WO::hi(v);
+        }
+      };
+      auto put_h = [&](E* at, H v, bool solid) {  // one node's element
+        if (!G || !solid) *reinterpret_cast<H*>(at) = v;
+      };
+      put(sl + Sl::base_of(0, LW) + p0_1, w[0]);
+      static_for<1, Q, 2>([&](auto I) {
+        constexpr int i = decltype(I)::value;
+        constexpr int cx = L::cx[i];
+        constexpr int ro = Sl::op_of(i + 1);
+        constexpr int rc = Pl::ops[ro].count;
+        E* ol = sl + Sl::base_of(1, LW) + Sl::j_of(i) * kChunk;
+        E* rl = sl + Sl::base_of(ro, LW) + Sl::j_of(i + 1) * kChunk;
+        const int r0 = rc == 1 ? p0_1 : p0_2;
+        put(ol + p0_own, w[i + 1]);
+        if constexpr (cx == 0) {
+          put(rl + r0, w[i]);
+        } else if constexpr (cx > 0) {
+          // elements x0 + 1 (inside the pair's word) and x0 + 2
+          put_h(rl + r0 + 1, WO::lo(w[i]), solid0);
+          put_h(rl + (rc == 1 ? pn_1 : pn_2), WO::hi(w[i]), solid1);
+        } else {
+          // elements x0 - 1 and x0
+          put_h(rl + (rc == 1 ? pe_1 : pe_2), WO::lo(w[i]), solid0);
+          put_h(rl + r0, WO::hi(w[i]), solid1);
+        }
+      });
     };
-    put(sl + Sl::base_of(0) + p0_1, w[0]);
-    static_for<1, Q, 2>([&](auto I) {
-      constexpr int i = decltype(I)::value;
-      constexpr int cx = L::cx[i];
-      constexpr int ro = Sl::op_of(i + 1);
-      constexpr int rc = Pl::ops[ro].count;
-      E* ol = sl + Sl::base_of(1) + Sl::j_of(i) * kChunk;
-      E* rl = sl + Sl::base_of(ro) + Sl::j_of(i + 1) * kChunk;
-      const int r0 = rc == 1 ? p0_1 : p0_2;
-      put(ol + p0_own, w[i + 1]);
-      if constexpr (cx == 0) {
-        put(rl + r0, w[i]);
-      } else if constexpr (cx > 0) {
-        // elements x0 + 1 (inside the pair's word) and x0 + 2
-        const int rn = rc == 1 ? pn_1 : pn_2;
-        if (!solid0) *reinterpret_cast<H*>(rl + r0 + 1) = WO::lo(w[i]);
-        if (!solid1) *reinterpret_cast<H*>(rl + rn) = WO::hi(w[i]);
-      } else {
-        // elements x0 - 1 and x0
-        const int re = rc == 1 ? pe_1 : pe_2;
-        if (!solid0) *reinterpret_cast<H*>(rl + re) = WO::lo(w[i]);
-        if (!solid1) *reinterpret_cast<H*>(rl + r0) = WO::hi(w[i]);
-      }
-    });
+    if (__any_sync(0xffffffffu, solid0 || solid1)) store_all(IC<1>{});
+    else store_all(IC<0>{});
 
-    {
-      if (a.rho)
-        store_macro_pair<S>(a, ((size_t)cur.zi * g.ny + cur.yi) * g.nx + x0, m, solid0, solid1);
-    }
+    if (a.rho)
+      store_macro_pair<S>(a, ((size_t)cur.zi * g.ny + cur.yi) * g.nx + x0, m, solid0, solid1);
 
-    // ---- row done for this warp: make its writes visible to the copy
-    // engine, count it; the last warp moves the row
+    // ---- row done for this warp: its shared-memory writes become visible
+    // to the copy engine, then one arrival on the stage's empty barrier
     fence_async_smem();
     __syncwarp();
-    if (lane == 0) {
-      __threadfence_block();
-      const int before = atomicAdd(&done[s], 1);
-      if (before == nw - 1) {
-        atomicExch(&done[s], 0);
-        __threadfence_block();
-        rows_copy<L, ST, false>(g, maps, P, cur, stage0 + s * Cfg::STAGE_BYTES, 0);
-        if (ahead.r < nrows) {
-          bulk_wait_read<0>();  // this thread's stores no longer read the stage
-          mbar_expect_tx(bar0 + 8 * s, rbytes);
-          rows_copy<L, ST, true>(g, maps, P, ahead, stage0 + s * Cfg::STAGE_BYTES, bar0 + 8 * s);
-          issued[s] += 1;
-        }
-      }
-    }
+    if (lane == 0) mbar_arrive(empty0 + 8 * s);
     cur.advance(gridDim.x, dyr, dzr, g.ny);
-    ahead.advance(gridDim.x, dyr, dzr, g.ny);
   }
-
-  if (failed && lane == 0 && a.err) atomicExch(a.err, 1);
-  if (lane == 0) bulk_wait_all();  // this thread's stores have landed
-  // every warp is out of the loop (all waits are bounded); after a failure,
-  // loads that were issued but never consumed land (bounded again) before
-  // the CTA's shared memory is released
-  if (__syncthreads_or(failed) && threadIdx.x == 0) {
-    for (int s = 0; s < kRowsStages; ++s)
-      if (issued[s] > 0) mbar_wait_bounded(bar0 + 8 * s, (issued[s] - 1) & 1);
+  if (failed && lane == 0) {
+    atomicExch(abort_flag, 1);
+    if (a.err) atomicExch(a.err, 1);
   }
 }
 

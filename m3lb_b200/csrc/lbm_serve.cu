@@ -63,7 +63,7 @@ constexpr int kMaxItems = 1024;  // lattices in one launch (shared-memory search
 // (five blocks spill more at 102 registers; six, at 80, lose 15 %).
 template <int OP, int ST>
 constexpr int batch_min_blocks() {
-  return (ST == kF16 || ST == kBF16) ? 4 : pair_min_blocks<OP, ST>();
+  return (ST == kF16 || ST == kBF16 || ST == kF16C) ? 4 : pair_min_blocks<OP, ST>();
 }
 
 template <int ST, int OP, int EQ, bool DENSE>
@@ -116,6 +116,7 @@ BatchFn batch_fn(int storage, int op, bool dense = false) {
   switch (storage) {
     case M3LB_STORE_F16: return dense ? batch_fn_st<kF16, true>(op) : batch_fn_st<kF16, false>(op);
     case M3LB_STORE_BF16: return dense ? batch_fn_st<kBF16, true>(op) : batch_fn_st<kBF16, false>(op);
+    case M3LB_STORE_F16C: return dense ? batch_fn_st<kF16C, true>(op) : batch_fn_st<kF16C, false>(op);
     case M3LB_STORE_F32: return dense ? batch_fn_st<kF32, true>(op) : batch_fn_st<kF32, false>(op);
     default: return nullptr;
   }
@@ -535,7 +536,7 @@ int m3lb_serve_create(const m3lb_serve_config* cfg, m3lb_server** out) {
   if (!cfg || !out) return fail(M3LB_ERR_INVALID, "serve_create: null argument");
   *out = nullptr;
   if (!batch_fn(cfg->storage, M3LB_OP_CM))
-    return fail(M3LB_ERR_UNSUPPORTED, "serve_create: storage %d is not served (F16, BF16, F32)",
+    return fail(M3LB_ERR_UNSUPPORTED, "serve_create: storage %d is not served (F16, F16C, BF16, F32)",
                 cfg->storage);
   if (cfg->round_steps < 1) return fail(M3LB_ERR_INVALID, "serve_create: round_steps must be >= 1");
   if (cfg->mapping < M3LB_MAP_AUTO || cfg->mapping > M3LB_MAP_TUNE)

@@ -8,8 +8,9 @@
 //   * rho()/ux()/uy()/uz()/flags() and gather_populations() return host arrays;
 //   * an optional fourth template argument picks the precision the
 //     populations are stored in on the device (StoreF32, StoreF16, StoreBF16,
-//     StoreF64); by default it follows Real, or -DLBM_B200_STORAGE_F16 /
-//     _BF16 selects 16-bit storage for every solver;
+//     StoreF64, StoreF16C); by default it follows Real, or
+//     -DLBM_B200_STORAGE_F16 / _BF16 / _F16C selects 16-bit storage for
+//     every solver;
 //   * the policies must be ones the device runs: D2Q9 / D3Q27; BGK, TRT,
 //     MomentCollision; NoForcing or Guo; Fluid, Solid and Excluded cells
 //     and the wall cells RegWall, SpecWall and SpecNode.
@@ -46,10 +47,14 @@ struct StoreF32 { static constexpr int code = M3LB_STORE_F32; static constexpr c
 struct StoreF16 { static constexpr int code = M3LB_STORE_F16; static constexpr const char* name = "FP16"; };
 struct StoreBF16 { static constexpr int code = M3LB_STORE_BF16; static constexpr const char* name = "BF16"; };
 struct StoreF64 { static constexpr int code = M3LB_STORE_F64; static constexpr const char* name = "FP64"; };
+// 1 sign, 4 exponent and 11 mantissa bits: FP16's bytes, half its rounding error
+struct StoreF16C { static constexpr int code = M3LB_STORE_F16C; static constexpr const char* name = "FP16C"; };
 #if defined(LBM_B200_STORAGE_F16)
 using DefaultStore = StoreF16;
 #elif defined(LBM_B200_STORAGE_BF16)
 using DefaultStore = StoreBF16;
+#elif defined(LBM_B200_STORAGE_F16C)
+using DefaultStore = StoreF16C;
 #else
 using DefaultStore = std::conditional_t<sizeof(Real) == 4, StoreF32, StoreF64>;
 #endif

@@ -8,8 +8,10 @@ driver reads the same here.  Compile-time policies there become constructor
 arguments here; every time step runs in one fused CUDA kernel on the device.
 
 Added over the reference: the storage precision of the populations
-(``storage="f32" | "f16" | "bf16" | "f64"``; arithmetic is FP32, or FP64 for
-"f64"), and a CUDA stream to queue the work on.
+(``storage="f32" | "f16" | "f16c" | "bf16" | "f64"``; arithmetic is FP32, or
+FP64 for "f64"; "f16c" is a 16-bit float with one more mantissa bit than
+IEEE binary16, include/m3lb.h M3LB_STORE_F16C), and a CUDA stream to queue
+the work on.
 """
 from __future__ import annotations
 
@@ -528,10 +530,27 @@ class FluidSolver:
                                                         (rho, ux, uy, uz)]))
 
     def initialize_field_device(self, rho, ux, uy, uz):
-        """Four device arrays (data pointers) of the arithmetic type."""
-        ptrs = [C.c_void_p(getattr(a, "data_ptr", lambda: a)()) for a in (rho, ux, uy, uz)]
+        """Four device arrays of the arithmetic type: torch tensors, or raw
+        device pointers.  The handle queues its work on its own stream, so
+        for tensors the seed first waits for the work torch has queued on its
+        current stream (which may still be writing them), and the call
+        returns once the seed has read them (torch may reuse their memory as
+        soon as they are freed)."""
+        arrs = (rho, ux, uy, uz)
+        ptrs = [C.c_void_p(getattr(a, "data_ptr", lambda: a)()) for a in arrs]
         self._push_params()
-        capi.check(capi.lib().m3lb_init_field_device(self._h, *ptrs))
+        lib = capi.lib()
+        dev = getattr(rho, "device", None)
+        if dev is not None and getattr(dev, "type", "") == "cuda":
+            import torch
+            mine = C.c_void_p()
+            capi.check(lib.m3lb_get_stream(self._h, C.byref(mine)))
+            theirs = torch.cuda.current_stream(dev).cuda_stream
+            if theirs != (mine.value or 0):
+                capi.check(lib.m3lb_stream_order(C.c_void_p(theirs), mine))
+        capi.check(lib.m3lb_init_field_device(self._h, *ptrs))
+        if dev is not None:
+            self.sync()
 
     def step(self, store_macroscopic=False):
         capi.check(capi.lib().m3lb_step(self._h, 1, int(store_macroscopic)))
@@ -575,6 +594,15 @@ class FluidSolver:
         capi.check(capi.lib().m3lb_reduce(self._h, _ptr(out)))
         return out
 
+    def diagnostics(self):
+        """The validation campaign's flow diagnostics on the device
+        (validation/Campaign.hpp:99-130): (kinetic energy sum 0.5 |u|^2,
+        enstrophy sum 0.5 |w|^2 over the interior, finite) -- the reference's
+        Diag {energy, enstrophy, finite}."""
+        out = np.zeros(3, np.float64)
+        capi.check(capi.lib().m3lb_diagnostics(self._h, _ptr(out)))
+        return float(out[0]), float(out[1]), bool(out[2] == 0)
+
     def total_mass(self):
         return float(self.reduce()[0])
 
@@ -602,7 +630,8 @@ class FluidSolver:
 
     def gather_raw(self):
         dt = {capi.STORE_F32: np.float32, capi.STORE_F64: np.float64,
-              capi.STORE_F16: np.uint16, capi.STORE_BF16: np.uint16}[self.storage]
+              capi.STORE_F16: np.uint16, capi.STORE_BF16: np.uint16,
+              capi.STORE_F16C: np.uint16}[self.storage]
         out = np.empty((self.dom.n_padded, self.Q), dt)
         capi.check(capi.lib().m3lb_gather_raw(self._h, _ptr(out)))
         return out

@@ -35,7 +35,7 @@ def reference_present() -> bool:
 REF_LIBS = {"f64": HERE / "_ref" / "libm3lb_ref_f64.so", "f32": HERE / "_ref" / "libm3lb_ref_f32.so"}
 
 OPS = {"none": 0, "bgk": 1, "trt": 2, "mrt": 3, "cm": 4}
-QUANT = {None: 0, "none": 0, "f16": 1, "bf16": 2}
+QUANT = {None: 0, "none": 0, "f16": 1, "bf16": 2, "f16c": 3}
 
 _dp = C.POINTER(C.c_double)
 _u8p = C.POINTER(C.c_uint8)

@@ -4,6 +4,7 @@
  */
 #include "lbm_oracle.h"
 
+#include <math.h>
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
@@ -83,6 +84,25 @@ static inline float lbmo_bf16_round(float v) {
   u &= 0xffff0000u;
   memcpy(&v, &u, 4);
   return v;
+}
+
+/* float -> FP16C -> float: the 16-bit float of the device's M3LB_STORE_F16C
+ * (1 sign, 4 exponent bits with bias 15, 11 mantissa bits, subnormals),
+ * rounded exactly as the device encodes it: the magnitude is clamped to
+ * 2 - 2^-11 (NaN included), scaled by 2^-112 into FP32's subnormal/low
+ * range where the format's code is the FP32 pattern's bits 26..12, rounded
+ * there by adding half a unit of bit 12 (to nearest, ties away from zero),
+ * and truncated. */
+static inline float lbmo_f16c_round(float v) {
+  const float m = fminf(fabsf(v), 1.99951171875f);
+  const float t = m * 0x1p-112f;
+  uint32_t u;
+  memcpy(&u, &t, 4);
+  u = ((u + 0x800u) >> 12) << 12;
+  float d;
+  memcpy(&d, &u, 4);
+  d = d * 0x1p112f;
+  return signbit(v) ? -d : d;
 }
 
 #define R double

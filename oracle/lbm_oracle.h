@@ -10,7 +10,9 @@
  * Two builds of one body (lbm_oracle_body.h): lbmo_f64_* computes in double,
  * lbmo_f32_* in float.  `quant` emulates narrow population storage with the
  * same arithmetic: every value written into the population array is rounded
- * to IEEE binary16 (1) or bfloat16 (2), round-to-nearest-even, exactly as a
+ * to IEEE binary16 (1) or bfloat16 (2), round-to-nearest-even, or to the
+ * library's FP16C format (3: 1 sign, 4 exponent, 11 mantissa bits, to
+ * nearest with ties away from zero, saturating at 2 - 2^-11), exactly as a
  * GPU store of a 16-bit population does.  0 stores at full precision.
  *
  * The entry points and their argument meanings are those of

@@ -41,6 +41,7 @@ typedef struct {
 static inline R S(q)(const S(solver)* s, R v) {
   if (s->quant == 1) return (R)(_Float16)v;
   if (s->quant == 2) return (R)lbmo_bf16_round((float)v);
+  if (s->quant == 3) return (R)lbmo_f16c_round((float)v);
   return v;
 }
 

@@ -11,7 +11,7 @@ LATS = {9: S.D2Q9, 27: S.D3Q27}
 OPNAMES = {0: "none", 1: "bgk", 2: "trt", 3: "mrt", 4: "cm"}
 # storage -> (oracle precision, oracle storage rounding)
 ORACLE_PREC = {"f32": ("f32", None), "f16": ("f32", "f16"), "bf16": ("f32", "bf16"),
-               "f64": ("f64", None)}
+               "f64": ("f64", None), "f16c": ("f32", "f16c")}
 
 
 def make_collision(lat, op, eq=0, shifted=True, forcing=False, omega=1.3, omega2=-1.0,
@@ -98,4 +98,5 @@ class Case:
 
 
 # Storage unit roundoff, for tolerances.
-EPS = {"f64": 2.0 ** -53, "f32": 2.0 ** -24, "f16": 2.0 ** -11, "bf16": 2.0 ** -8}
+EPS = {"f64": 2.0 ** -53, "f32": 2.0 ** -24, "f16": 2.0 ** -11, "bf16": 2.0 ** -8,
+       "f16c": 2.0 ** -12}

@@ -24,7 +24,7 @@ from tests.helpers import EPS, Case
 pytestmark = pytest.mark.gpu
 
 OPS = [(1, 0), (1, 1), (2, 0), (2, 1), (3, 0), (4, 0)]
-TOL_K = {"f64": 64.0, "f32": 64.0, "f16": 4.0, "bf16": 4.0}
+TOL_K = {"f64": 64.0, "f32": 64.0, "f16": 4.0, "bf16": 4.0, "f16c": 4.0}
 
 
 def _tol(storage, scale):
@@ -34,8 +34,8 @@ def _tol(storage, scale):
 def _cases():
     out = []
     for (op, eq), storage, shifted, forcing in itertools.product(
-            OPS, ["f32", "f16", "bf16", "f64"], [True, False], [False, True]):
-        if storage in ("f16", "bf16") and not shifted:
+            OPS, ["f32", "f16", "bf16", "f64", "f16c"], [True, False], [False, True]):
+        if storage in ("f16", "bf16", "f16c") and not shifted:
             continue
         out.append((op, eq, storage, shifted, forcing))
     return out
@@ -92,13 +92,13 @@ def test_collision_matches_oracle(cuda_device, lat, op, eq, storage, shifted, fo
 
 @pytest.mark.parametrize("lat", [27, 9])
 @pytest.mark.parametrize("op,eq", OPS)
-@pytest.mark.parametrize("storage", ["f32", "f16", "bf16", "f64"])
+@pytest.mark.parametrize("storage", ["f32", "f16", "bf16", "f64", "f16c"])
 def test_pair_kernel_equals_node_kernel(cuda_device, lat, op, eq, storage):
     """The paired kernel (f32x2 arithmetic, warp exchange) and the one-node
-    kernel run the same sequence of rounded operations.  Streaming, BGK and TRT
-    give identical stored bits.  The moment operators agree to a few units in
-    the last place of the arithmetic type (measured: at most 4 ulp of the
-    population scale), bounded here at 8 ulp."""
+    kernel run the same sequence of rounded operations: identical stored bits
+    and stored macroscopic fields for every operator (the moment operators'
+    one product that the compiler could fuse into a sum in the paired kernel
+    only is written as an explicit FMA)."""
     shape = (130, 4, 3) if lat == 27 else (130, 6, 1)
     a = Case(lat=lat, op=op, eq=eq, storage=storage, forcing=True, shape=shape,
              periodic=(True, False, True), omega2=1.1 if op == 2 else -1.0)
@@ -114,15 +114,9 @@ def test_pair_kernel_equals_node_kernel(cuda_device, lat, op, eq, storage):
     b.gpu.initialize_field(fields)
     a.gpu.steps(5, True)
     b.gpu.steps(5, True)
-    if op <= 2:
-        np.testing.assert_array_equal(a.gpu.gather_raw(), b.gpu.gather_raw())
-        for x, y in zip(a.gpu.stored_macroscopic(), b.gpu.stored_macroscopic()):
-            np.testing.assert_array_equal(x, y)
-    else:
-        ga, gb = a.gpu.gather_populations(), b.gpu.gather_populations()
-        ar = EPS["f64"] if storage == "f64" else EPS["f32"]
-        unit = max(ar, EPS[storage])
-        assert float(np.max(np.abs(ga - gb))) <= 8 * unit * float(np.max(np.abs(gb)))
+    np.testing.assert_array_equal(a.gpu.gather_raw(), b.gpu.gather_raw())
+    for x, y in zip(a.gpu.stored_macroscopic(), b.gpu.stored_macroscopic()):
+        np.testing.assert_array_equal(x, y)
     a.close()
     b.close()
 
@@ -146,7 +140,7 @@ STREAM_SHAPES = [(27, (64, 5, 4)), (27, (192, 3, 3)), (27, (130, 4, 3)), (27, (2
 
 @pytest.mark.parametrize("lat,shape", STREAM_SHAPES)
 @pytest.mark.parametrize("op", [0, 1, 2, 4])
-@pytest.mark.parametrize("storage", ["f32", "f16", "bf16", "f64"])
+@pytest.mark.parametrize("storage", ["f32", "f16", "bf16", "f64", "f16c"])
 def test_streamed_kernel_equals_paired_kernel(cuda_device, storage, lat, shape, op):
     """The persistent copy-pipelined kernel and the paired kernel: identical
     stored bits after several steps, on full, multi-chunk, partial-chunk and
@@ -180,7 +174,7 @@ ROWS_SHAPES = [(27, (64, 5, 4)), (27, (128, 4, 3)), (27, (192, 3, 3)), (27, (256
 
 @pytest.mark.parametrize("lat,shape", ROWS_SHAPES)
 @pytest.mark.parametrize("op", [0, 1, 2, 3, 4])
-@pytest.mark.parametrize("storage", ["f32", "f16", "bf16", "f64"])
+@pytest.mark.parametrize("storage", ["f32", "f16", "bf16", "f64", "f16c"])
 def test_row_kernel_equals_paired_kernel(cuda_device, storage, lat, shape, op):
     """The TMA row kernel (whole rows through shared memory) and the paired
     kernel: identical stored bits after several steps, one to four chunks per
@@ -243,7 +237,7 @@ VARIANT_SHAPES = [(27, (128, 4, 3)), (27, (160, 3, 3)), (27, (256, 2, 2)), (9, (
 @pytest.mark.parametrize("forcing", [False, True])
 @pytest.mark.parametrize("periodic", [(True, True, True), (True, False, True)],
                          ids=["periodic", "ywalls"])
-@pytest.mark.parametrize("storage", ["f16", "bf16"])
+@pytest.mark.parametrize("storage", ["f16", "bf16", "f16c"])
 def test_auto_kernels_equal_paired_kernel(cuda_device, storage, periodic, forcing, op, eq,
                                           lat, shape):
     """Every operator instantiation that the automatic choice sends to the row
@@ -281,4 +275,31 @@ def test_rows_beyond_one_grid_dimension(cuda_device, lat, shape):
     nf = float(np.prod(shape))
     assert abs(red[0] - c.cpu.total_mass()) <= nf * lat * tol + 8 * ar * nf * np.sqrt(nf)
     assert abs(red[5] - c.cpu.slot_sum()) <= c.dom.n_padded * lat * tol + 1e-12 * nf * lat
+    c.close()
+
+
+def test_row_kernel_wait_that_runs_out_is_reported(cuda_device):
+    """The row kernel's waits for a row's copies are bounded.  With the
+    consume wait cut to one clock cycle (a test-only option; the drain of the
+    copies still in flight keeps its full limit), CTAs give up on rows whose
+    copies have not landed yet: the kernel records a status instead of
+    hanging, and the next m3lb_sync returns it as an error, once.  The handle
+    stays usable: with the default limit restored and the lattice seeded
+    again, a step is clean."""
+    from m3lb_b200 import capi
+
+    c = Case(lat=27, op=4, storage="f16", shape=(256, 16, 16), periodic=(True, True, True))
+    c.gpu.set_option(capi.OPT_KERNEL, capi.KERNEL_ROWS)
+    c.gpu.initialize(1.0, 0.01, 0.0, 0.0)
+    c.gpu.sync()
+    c.gpu.set_option(capi.OPT_WAIT_CYCLES, 1)
+    c.gpu.steps(2)
+    with pytest.raises(capi.M3lbError, match="gave up waiting"):
+        c.gpu.sync()
+    c.gpu.sync()  # reported once
+    c.gpu.set_option(capi.OPT_WAIT_CYCLES, 0)
+    c.gpu.initialize(1.0, 0.01, 0.0, 0.0)
+    c.gpu.steps(2)
+    c.gpu.sync()
+    assert np.isfinite(c.gpu.reduce()).all()
     c.close()

@@ -66,7 +66,7 @@ RAGGED = [SV.Request(10, 0.0, 6, capi.OP_CM, 11, 0.05),
           SV.Request(14, 0.0, 64, capi.OP_CM, 9, 0.05)]
 
 
-@pytest.mark.parametrize("storage", ["f16", "bf16", "f32"])
+@pytest.mark.parametrize("storage", ["f16", "f16c", "bf16", "f32"])
 def test_dense_mapping_equals_chunks(cuda_device, storage):
     reqs = MIX + RAGGED
     ch, ch_f, st_c = _serve(reqs, storage, mapping="chunks")

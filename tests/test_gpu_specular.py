@@ -20,7 +20,7 @@ from tests.helpers import EPS, Case, make_collision
 
 pytestmark = pytest.mark.gpu
 
-TOL_K = {"f64": 64.0, "f32": 64.0, "f16": 4.0, "bf16": 4.0}
+TOL_K = {"f64": 64.0, "f32": 64.0, "f16": 4.0, "bf16": 4.0, "f16c": 4.0}
 OPS = [(0, 0, -1.0), (1, 0, -1.0), (1, 1, -1.0), (2, 0, 1.1), (3, 0, 1.5), (4, 0, -1.0)]
 
 
@@ -37,8 +37,8 @@ def _case(lat, op, eq, om2, storage, shifted, forcing, kind, shape=None):
 def _cases():
     out = []
     for (op, eq, om2), storage, shifted, forcing in itertools.product(
-            OPS, ["f32", "f16", "bf16", "f64"], [True, False], [False, True]):
-        if storage in ("f16", "bf16") and not shifted:
+            OPS, ["f32", "f16", "bf16", "f64", "f16c"], [True, False], [False, True]):
+        if storage in ("f16", "bf16", "f16c") and not shifted:
             continue
         if op == 0 and (forcing or not shifted):
             continue

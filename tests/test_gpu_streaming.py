@@ -18,7 +18,7 @@ pytestmark = pytest.mark.gpu
 
 def _tags(dom, Q, storage):
     n = dom.n_padded * Q
-    if storage in ("f16", "bf16"):
+    if storage in ("f16", "bf16", "f16c"):
         # unique finite 16-bit patterns (exponent field not all ones)
         pats = np.arange(1, 0x7000, dtype=np.uint16)
         assert n <= len(pats)
@@ -34,7 +34,7 @@ def _permutation(lat, shape, steps, storage, node_kernel):
     if node_kernel:
         s.set_option(capi.OPT_NODE_KERNEL, 1)
     tags = _tags(dom, L.Q, storage)
-    raw = storage in ("f16", "bf16")
+    raw = storage in ("f16", "bf16", "f16c")
     if raw:
         s.seed_raw(tags)
     else:
@@ -68,7 +68,7 @@ CASES = [
 
 
 @pytest.mark.parametrize("lat,shape,steps", CASES)
-@pytest.mark.parametrize("storage", ["f32", "f16", "bf16", "f64"])
+@pytest.mark.parametrize("storage", ["f32", "f16", "bf16", "f64", "f16c"])
 def test_permutation(cuda_device, lat, shape, steps, storage):
     assert _permutation(lat, shape, steps, storage, node_kernel=False) == 0
 

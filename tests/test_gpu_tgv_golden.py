@@ -10,7 +10,8 @@ vorticity, validation/Campaign.hpp:96-131) every 1600 steps, normalised by
 their initial values.  The same run through FluidSolver:
   * FP64 storage matches every printed value (nine digits) to 2e-8;
   * FP32 storage with FP32 arithmetic stays within 2e-4, FP16 storage
-    within 1e-2: precision changes the storage, not the scheme.
+    within 1e-2, FP16C storage (one more mantissa bit) within 5e-3:
+    precision changes the storage, not the scheme.
 (BF16 storage leaves the trajectory at this amplitude: its 8-bit mantissa is
 coarser than the shifted populations' variation, and the decay stalls.)
 """
@@ -68,7 +69,8 @@ def _trajectory(storage):
     return np.array(rows)
 
 
-@pytest.mark.parametrize("storage,rtol", [("f64", 2e-8), ("f32", 2e-4), ("f16", 1e-2)])
+@pytest.mark.parametrize("storage,rtol", [("f64", 2e-8), ("f32", 2e-4), ("f16", 1e-2),
+                                          ("f16c", 5e-3)])
 def test_taylor_green_matches_reference_trajectory(cuda_device, storage, rtol):
     gold = np.loadtxt(GOLD)
     got = _trajectory(storage)

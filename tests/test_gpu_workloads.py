@@ -159,3 +159,48 @@ def test_tgv128_energy_and_enstrophy_match_reference_build(cuda_device):
         assert abs(g[3] - w[3]) <= 1e-5 * w[3] + 1e-6, (g, w)
         if not math.isnan(w[2]):
             assert abs(g[2] - w[2]) <= 1e-3, (g, w)
+
+
+def test_tgv256_16bit_storage_accuracy(cuda_device):
+    """Config 3 (the headline workload): the 256^3 Taylor-Green vortex after
+    500 steps with 16-bit shifted populations, against FP64 populations from
+    the same initial field.  FP16C (1 sign, 4 exponent, 11 mantissa bits)
+    keeps the velocity error under the 1e-3 bound (measured ~6e-4); IEEE
+    binary16 does not (~2.0e-3); FP32 storage is ~4e-7."""
+    import torch
+    from m3lb_b200 import solver as S
+
+    n, u0, steps = 256, 0.05, 500
+    nu = u0 * (n / (2 * math.pi)) / 1600.0
+    omega = 1.0 / (3 * nu + 0.5)
+    k = 2 * math.pi / n
+    i = torch.arange(n, dtype=torch.float64, device=cuda_device) * k
+    z, y, x = torch.meshgrid(i, i, i, indexing="ij")
+    dr = 3.0 * u0 * u0 / 16.0
+    f64 = [1 + dr * (torch.cos(2 * x) + torch.cos(2 * y)) * (torch.cos(2 * z) + 2),
+           u0 * torch.sin(x) * torch.cos(y) * torch.cos(z),
+           -u0 * torch.cos(x) * torch.sin(y) * torch.cos(z)]
+    f64.append(torch.zeros_like(f64[0]))
+    del x, y, z
+
+    def run(storage):
+        dom = S.Domain(n, n, n, True, True, True)
+        coll = S.CentralMoments(S.D3Q27, S.NoForcing(), S.ShiftedPopulations, omega=omega)
+        s = S.FluidSolver(dom, coll, storage=storage)
+        dt = torch.float64 if storage == "f64" else torch.float32
+        s.initialize_field_device(*[t.to(dt).contiguous() for t in f64])
+        s.steps(steps)
+        rho, ux, uy, uz = s.compute_macroscopic()
+        s.close()
+        return rho, np.stack([ux, uy, uz])
+
+    r_ref, u_ref = run("f64")
+    du = float(np.sqrt(np.sum(u_ref * u_ref)))
+    err = {}
+    for st in ("f16c", "f16", "f32"):
+        _, u = run(st)
+        err[st] = float(np.sqrt(np.sum((u - u_ref) ** 2)) / du)
+        del u
+    assert err["f32"] < 2e-6, err
+    assert err["f16c"] < 1e-3, err
+    assert err["f16c"] < 0.5 * err["f16"], err

@@ -484,3 +484,43 @@ def test_oracle_scalar_diffusion_rate():
         k = 2 * np.pi / N
         assert abs(amp / 0.01 / np.exp(-D * k * k * steps) - 1) < 1e-3
         s.close()
+
+
+def _f16c_reference(v):
+    """The FP16C format from its definition (1 sign, 4 exponent bits with bias
+    15, 11 mantissa bits, subnormals below 2^-14 with step 2^-25, largest
+    magnitude 2 - 2^-11): nearest value, ties away from zero, magnitudes
+    beyond the largest (and NaN) saturated."""
+    v = np.asarray(v, np.float64)
+    top = 2.0 - 2.0 ** -11
+    m = np.where(np.isnan(v), top, np.minimum(np.abs(v), top))
+    _, k = np.frexp(np.where(m > 0, m, 1.0))
+    e = np.maximum(k - 1, -14)               # binade exponent, subnormals share -14
+    ulp = np.ldexp(1.0, e - 11)
+    q = np.floor(m / ulp + 0.5) * ulp
+    return np.where(np.signbit(v), -q, q)
+
+
+def test_oracle_f16c_storage_rounds_as_the_format_defines():
+    """The oracle's FP16C storage emulation (what the device's encoder must
+    match bit for bit) against the format's definition: exact values stay,
+    halfway values go away from zero, subnormals keep a 2^-25 step, large
+    magnitudes saturate, and random shifted-population-sized values land on
+    the nearest representable value."""
+    c = O.CpuSolver("oracle", lattice=27, op="none", shifted=True, nx=4, ny=3, nz=2,
+                    px=True, py=True, pz=True, precision="f32", quant="f16c")
+    n = c.n_padded * c.Q
+    special = [1.0, -1.0, 1 + 2 ** -11, 1 + 2 ** -12, 1 + 3 * 2 ** -12, -(1 + 2 ** -12),
+               2 ** -14, 2 ** -25, 2 ** -26, 3 * 2 ** -26, 2 ** -27, 0.0, -0.0,
+               1.99951171875, 1.9998, 3.0, -70000.0, 2 ** -14 - 2 ** -26, 0.1, -0.01]
+    rng = np.random.default_rng(0)
+    rand = (rng.standard_normal(n - len(special)) * 10.0 ** rng.uniform(-7, 0, n - len(special)))
+    vals = np.concatenate([special, rand]).astype(np.float32).astype(np.float64)
+    c.seed(vals.reshape(c.n_padded, c.Q))
+    got = c.gather().reshape(-1)
+    c.close()
+    want = _f16c_reference(vals)
+    assert np.array_equal(got, want), np.flatnonzero(got != want)[:10]
+    assert got[3] == 1 + 2 ** -11 and got[5] == -(1 + 2 ** -11)   # ties away from zero
+    assert got[8] == 2 ** -25 and got[10] == 0.0                 # subnormal step 2^-25
+    assert got[13] == got[14] == got[15] == 1.99951171875 and got[16] == -1.99951171875
