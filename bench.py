@@ -281,6 +281,9 @@ def gpu_arm(args, rank, world, dist):
         out["accuracy"] = accuracy_arm(args, dev, stream, omega)
     if rank == 0 and world == 1 and args.serve_requests > 0:
         out["serving"] = serving_arm(args)
+        # the serving target: aggregate within 25 % of the single large lattice
+        out["serving"]["aggregate_over_single"] = round(
+            out["serving"]["aggregate_mlups"] / out["value"], 3)
     if rank == 0 and world == 1 and args.walls_steps > 0:
         out["walls"] = walls_arm(args, stream, omega)
     if rank == 0 and world == 1 and args.thermal_steps > 0:
@@ -440,10 +443,13 @@ def serving_arm(args):
                  "graph_captures": st.graph_captures, "graph_launches": st.graph_launches,
                  "hbm_budget_gib": args.serve_budget_gb, "max_resident": args.serve_resident,
                  "round_steps": args.serve_round},
-        "mapping_tuner": {"chosen": {1: "chunks", 2: "dense"}.get(st.tuned_mapping, "none"),
+        "mapping_tuner": {"chosen": {1: "chunks", 2: "dense", 4: "rows"}.get(st.tuned_mapping,
+                                                                              "none"),
                           "chunks_mlups": round(st.tuned_chunks_mlups, 1),
                           "dense_mlups": round(st.tuned_dense_mlups, 1),
-                          "dense_launches": st.dense_launches},
+                          "rows_mlups": round(st.tuned_rows_mlups, 1),
+                          "dense_launches": st.dense_launches,
+                          "rows_launches": st.rows_launches},
         "workload": "seed 0, Poisson 50/s, N in {32..160 step 16}, op in {BGK, TRT, CM}, "
                     "u0 ~ U[0.02, 0.08], steps ~ U[200, 2000], FP16, tau 0.6",
     }

@@ -393,8 +393,8 @@ int m3lb_couple_thermal(m3lb_solver* fluid, m3lb_scalar* scalar, double gx, doub
  * arrival order while their footprint (populations plus 16 B per node of
  * seed/readout fields) fits hbm_budget; every admitted lattice stays resident
  * until its last step.  Each time step of a round is one batched launch per
- * operator over all resident lattices, replayed from a CUDA graph while the
- * resident set repeats.  Results are FP64 mass, momentum and energy of
+ * operator (and, through the row kernel, row width) over all resident
+ * lattices, replayed from a CUDA graph (see M3LB_MAP_ROWS).  Results are FP64 mass, momentum and energy of
  * the final state (and rho, u with keep_fields); a request's result is
  * bit-identical alone, in any mix, and through m3lb_step with
  * M3LB_KERNEL_PAIRS. */
@@ -406,23 +406,31 @@ typedef struct {
   int round_steps;    /* most time steps per scheduling round (>= 1) */
   int storage;        /* M3LB_STORE_F16, _F16C, _BF16 or _F32, for every request */
   int keep_fields;    /* 1: keep rho, u of finished requests for m3lb_serve_fields */
-  int mapping;        /* warp-to-node mapping of the batched launches: M3LB_MAP_AUTO (0),
-                         _CHUNKS, _DENSE or _TUNE (same results, different speed) */
+  int mapping;        /* how the batched launches map lattices to warps: M3LB_MAP_AUTO (0),
+                         _CHUNKS, _DENSE, _TUNE or _ROWS (same results, different speed) */
 } m3lb_serve_config;
 
 /* M3LB_MAP_CHUNKS: a warp updates one 64-slot chunk of a row (lanes past the
  * row's end idle when N is not a multiple of 64).  M3LB_MAP_DENSE: a warp
  * updates 64 consecutive nodes in x-fastest order, rows packed back to back,
- * so no lane idles.  M3LB_MAP_AUTO: dense for an operator's launch when one
- * of its lattices has N not a multiple of 64, chunks otherwise.
- * M3LB_MAP_TUNE: an autotuner on the live stream: the first rounds alternate
- * the two mappings, each timed on the device (CUDA events around the round's
- * launches) for 6 rounds, and the one with more lattice updates per second
- * serves every later round (reported in m3lb_serve_stats). */
+ * so no lane idles.  M3LB_MAP_ROWS (16-bit storage): the row kernel, a CTA
+ * moving whole x-rows of any lattice of its group through shared memory by
+ * TMA, one persistent launch per step and (operator, row width) group;
+ * rounds run their full length, a lattice that finishes inside a round sits
+ * the rest of it out, and each (groups present, length) is captured into a
+ * CUDA graph once and replayed whatever lattices come and go.
+ * M3LB_MAP_AUTO: rows with 16-bit storage; otherwise dense for an operator's
+ * launch when one of its lattices has N not a multiple of 64, chunks
+ * otherwise.  M3LB_MAP_TUNE: an autotuner on the live stream: the first
+ * rounds alternate the three (two without 16-bit storage), each timed on the
+ * device (CUDA events around the round's launches) for 6 rounds, and the one
+ * with the most lattice updates per second serves every later round
+ * (reported in m3lb_serve_stats). */
 #define M3LB_MAP_AUTO 0
 #define M3LB_MAP_CHUNKS 1
 #define M3LB_MAP_DENSE 2
 #define M3LB_MAP_TUNE 3
+#define M3LB_MAP_ROWS 4
 
 typedef struct {
   long long id;         /* caller's tag */
@@ -451,9 +459,11 @@ typedef struct {
   long long node_steps;     /* sum of n^3 * steps over completed requests */
   double makespan;          /* seconds from the start of the last run to its end */
   long long dense_launches; /* batched launches with the dense mapping */
-  int tuned_mapping;         /* M3LB_MAP_TUNE: the mapping chosen (_CHUNKS or _DENSE), 0 before */
-  double tuned_chunks_mlups; /* the tuner's measured rates of both mappings (MLUPS) */
+  int tuned_mapping;         /* M3LB_MAP_TUNE: the mapping chosen (_CHUNKS, _DENSE or _ROWS), 0 before */
+  double tuned_chunks_mlups; /* the tuner's measured rates of its candidates (MLUPS) */
   double tuned_dense_mlups;
+  long long rows_launches;   /* batched launches through the row kernel */
+  double tuned_rows_mlups;
 } m3lb_serve_stats;
 
 int m3lb_serve_create(const m3lb_serve_config* cfg, m3lb_server** out);

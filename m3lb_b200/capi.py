@@ -24,7 +24,7 @@ OPT_NODE_KERNEL = 1
 OPT_KERNEL = 2
 OPT_WAIT_CYCLES = 3  # test only: shorten the row kernel's wait for its copies
 KERNEL_AUTO, KERNEL_NODES, KERNEL_PAIRS, KERNEL_STREAM, KERNEL_ROWS = 0, 1, 2, 3, 4
-MAP_AUTO, MAP_CHUNKS, MAP_DENSE, MAP_TUNE = 0, 1, 2, 3
+MAP_AUTO, MAP_CHUNKS, MAP_DENSE, MAP_TUNE, MAP_ROWS = 0, 1, 2, 3, 4
 
 STORAGE_NAMES = {"f32": STORE_F32, "f16": STORE_F16, "bf16": STORE_BF16, "f64": STORE_F64,
                  "f16c": STORE_F16C}
@@ -66,7 +66,8 @@ class ServeStats(C.Structure):
                 ("finished", C.c_longlong), ("node_steps", C.c_longlong),
                 ("makespan", C.c_double), ("dense_launches", C.c_longlong),
                 ("tuned_mapping", C.c_int), ("tuned_chunks_mlups", C.c_double),
-                ("tuned_dense_mlups", C.c_double)]
+                ("tuned_dense_mlups", C.c_double), ("rows_launches", C.c_longlong),
+                ("tuned_rows_mlups", C.c_double)]
 
 
 _vp = C.c_void_p

@@ -180,7 +180,7 @@ struct m3lb_solver {
     // of 2, 4 or 8 chunks that must fit a CTA's shared memory
     const int lw = g.nch <= 2 ? 2 : (g.nch <= 4 ? 4 : 8);
     const bool rows_ok = g.nch <= (elem_bytes(storage) == 2 ? 8 : 4) &&
-                         4LL * Q * lw * 64 * elem_bytes(storage) + 80 <= 227LL * 1024;
+                         4LL * Q * lw * 64 * elem_bytes(storage) + 84 <= 227LL * 1024;
     if (kernel == M3LB_KERNEL_ROWS && rows_ok) return kKernelRows;
     if (kernel == M3LB_KERNEL_STREAM && rows32) return kKernelStream;
     // auto, from measurements on B200: with 16-bit storage the row kernel

@@ -303,7 +303,71 @@ cudaError_t bound(const StepArgs& a, const BoundArgs& b, int phase, int op, int 
     default: return cudaErrorInvalidValue;
   }
 }
-const Launchers kTable = {step, seed, gather, macro, reduce, bound};
+cudaError_t row_maps(const StepArgs& a, void* maps, size_t bytes) {
+  if (bytes != sizeof(RowMaps<L>)) return cudaErrorInvalidValue;
+  return rows_maps(a, static_cast<RowMaps<L>*>(maps));
+}
+
+// Batched row launches (the serving loop): 16-bit storage, shifted
+// populations, no force.  A persistent grid of the resident CTAs of the
+// shape, which does not depend on the batch's size, so the launch can be
+// captured once and serve any resident set of its (operator, row width).
+template <int OP, int LW>
+cudaError_t launch_batch_rows(const void* items, const void* desc, int nch, int step,
+                              cudaStream_t s) {
+  using Cfg = RowsCfg<L, ST, LW>;
+  if constexpr (Cfg::SMEM > kRowsSmemMax || sizeof(typename WordOps<ST>::E) != 2) {
+    return cudaErrorNotSupported;
+  } else {
+    auto kern = batch_rows<L, ST, OP, 0, LW>;
+    const int threads = (nch + 1) * 32;
+    constexpr int kMaxDev = 64;
+    static int cached[kMaxDev][LW + 1];
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= kMaxDev) return cudaErrorInvalidDevice;
+    if (cached[dev][nch] == 0) {
+      e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, Cfg::SMEM);
+      if (e != cudaSuccess) return e;
+      int per_sm = 0, nsm = 0;
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, Cfg::SMEM);
+      if (e != cudaSuccess) return e;
+      e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+      if (e != cudaSuccess) return e;
+      if (per_sm < 1) return cudaErrorInvalidConfiguration;
+      cached[dev][nch] = per_sm * nsm;
+    }
+    kern<<<cached[dev][nch], threads, Cfg::SMEM, s>>>(static_cast<const RowItem<L>*>(items),
+                                                      static_cast<const RowBatch*>(desc), step);
+    return cudaGetLastError();
+  }
+}
+template <int OP>
+cudaError_t batch_rows_op(const void* items, const void* desc, int nch, int step, cudaStream_t s) {
+  if (nch < 1 || nch > kRowsMaxChunks) return cudaErrorInvalidValue;
+  switch (rows_lw(nch)) {
+    case 2: return launch_batch_rows<OP, 2>(items, desc, nch, step, s);
+    case 4: return launch_batch_rows<OP, 4>(items, desc, nch, step, s);
+    default: return launch_batch_rows<OP, 8>(items, desc, nch, step, s);
+  }
+}
+cudaError_t batch_rows_launch(const void* items, const void* desc, int op, int nch, int step,
+                              cudaStream_t s) {
+  if constexpr (sizeof(typename WordOps<ST>::E) != 2 || L::Q != 27) {
+    return cudaErrorNotSupported;
+  } else {
+    switch (op) {
+      case 1: return batch_rows_op<1>(items, desc, nch, step, s);
+      case 2: return batch_rows_op<2>(items, desc, nch, step, s);
+      case 3: return batch_rows_op<3>(items, desc, nch, step, s);
+      case 4: return batch_rows_op<4>(items, desc, nch, step, s);
+      default: return cudaErrorInvalidValue;
+    }
+  }
+}
+
+const Launchers kTable = {step, seed, gather, macro, reduce, bound, row_maps, batch_rows_launch};
 
 }  // namespace
 

@@ -28,6 +28,14 @@ struct Launchers {
   // boundary pass over the wall-node list b.begin..b.end (lbm_bound.cuh)
   cudaError_t (*bound)(const StepArgs& a, const BoundArgs& b, int phase, int op, int eq, bool sh,
                        bool force, cudaStream_t s);
+  // the row kernel's tensor maps of a lattice (RowMaps of lbm_rows.cuh,
+  // `bytes` long), for the items of batched row launches
+  cudaError_t (*row_maps)(const StepArgs& a, void* maps, size_t bytes);
+  // one time step of a batch of lattices through the row kernel: `items` a
+  // device table of RowItem, `desc` the device RowBatch of this launch (all
+  // its lattices with operator op, shifted, no force, rows of nch chunks)
+  cudaError_t (*batch_rows)(const void* items, const void* desc, int op, int nch, int step,
+                            cudaStream_t s);
 };
 // phases of the boundary pass
 enum BoundPhase { kBndSnapshot = 0, kBndCornerRho = 1, kBndUpdate = 2, kBndMacro = 3 };

@@ -151,14 +151,33 @@ struct RowMaps {
   CUtensorMap m[RowPlan<L>::NMAPS];
 };
 
+// One lattice of a batched launch (the serving loop): its tensor maps, step
+// arguments, first row in the launch's numbering and time at the start of
+// the round.
+template <class L>
+struct RowItem {
+  RowMaps<L> maps;
+  StepArgs a;
+  long long first_row;
+  long long t0;     // the lattice's time at step 0 of the launch
+  long long t_end;  // its last time: steps from t_end on leave its rows alone
+};
+// A batched launch: items first_item .. first_item + n_items of the table
+// (one operator, one row width), n_rows rows in all.
+struct RowBatch {
+  int first_item, n_items;
+  long long n_rows;
+};
+
 // Shared memory of a CTA: kRowsStages stages of Q lines of LW chunks, then
 // the barriers (full[s]: the stage's loads landed; empty[s]: every update
-// warp is done with the stage's row) and the abort flag.
+// warp is done with the stage's row), the abort flag and, for batched
+// launches, the item of each stage's row.
 template <class L, int ST, int LW>
 struct RowsCfg {
   using E = typename WordOps<ST>::E;
   static constexpr int STAGE_BYTES = L::Q * LW * kChunk * (int)sizeof(E);
-  static constexpr int SMEM = kRowsStages * STAGE_BYTES + 2 * kRowsStages * 8 + 16;
+  static constexpr int SMEM = kRowsStages * STAGE_BYTES + 2 * kRowsStages * 8 + 4 + 4 * kRowsStages;
   static __host__ __device__ int row_bytes(int nch) { return L::Q * nch * kChunk * (int)sizeof(E); }
 };
 // Line width (chunks per stage line) for a row of nch chunks.
@@ -315,9 +334,19 @@ constexpr int rows_min_blocks() {
 // warps' arrivals on empty[s] (one per warp) complete the same phase there,
 // after which the copy warp stores the row, waits until the stores have
 // read the stage, and loads row j + kRowsStages into it.
-template <class L, int ST, int OP, int EQ, bool SH, bool FORCE, int LW>
-__global__ void __launch_bounds__((LW + 1) * 32, rows_min_blocks<OP, ST, LW>())
-step_rows(StepArgs a, const __grid_constant__ RowMaps<L> maps) {
+//
+// BATCH: the rows of many lattices of one operator and one row width (the
+// serving loop): global row r belongs to the item whose range holds it
+// (items sorted by first_row), each item carrying its own step arguments,
+// tensor maps and time.  The copy warp finds the item of each row it moves
+// and records it in the stage's slot of `meta`; the update warps read it
+// there and take the lattice's x extent and rates when it changes.  Batched
+// lattices are periodic boxes with no cell flags, buoyancy or macroscopic
+// output.
+template <class L, int ST, int OP, int EQ, bool SH, bool FORCE, int LW, bool BATCH>
+__device__ __forceinline__ void rows_body(const StepArgs& a, const RowMaps<L>& maps,
+                                          const RowItem<L>* __restrict__ items, int n_items,
+                                          long long batch_rows, int step) {
   using WO = WordOps<ST>;
   using W = typename WO::W;
   using H = typename WO::H;
@@ -335,11 +364,11 @@ step_rows(StepArgs a, const __grid_constant__ RowMaps<L> maps) {
   extern __shared__ __align__(128) unsigned char rows_smem[];
   const int lane = threadIdx.x & 31;
   const int k = threadIdx.x >> 5;  // chunk of the row; == nch for the copy warp
-  const int nch = g.nch;
-  const int P = a.parity;
-  const long long nrows = (long long)g.ny * g.nz;
+  const int nch = BATCH ? items[0].a.g.nch : g.nch;
+  const long long nrows = BATCH ? batch_rows : (long long)g.ny * g.nz;
   uint64_t* bars = reinterpret_cast<uint64_t*>(rows_smem + NS * Cfg::STAGE_BYTES);
   int* abort_flag = reinterpret_cast<int*>(bars + 2 * NS);
+  int* meta = abort_flag + 1;  // BATCH: the item of each stage's row
   const uint32_t stage0 = smem_addr(rows_smem);
   const uint32_t full0 = smem_addr(bars), empty0 = full0 + 8 * NS;
   const int dyr = (int)(gridDim.x % g.ny), dzr = (int)(gridDim.x / g.ny);
@@ -355,35 +384,81 @@ step_rows(StepArgs a, const __grid_constant__ RowMaps<L> maps) {
   __syncthreads();
 
   RowCursor cur;
-  cur.start(blockIdx.x, g.ny);
+  if constexpr (BATCH) cur.r = blockIdx.x;
+  else cur.start(blockIdx.x, g.ny);
 
   // ------------------------------------------------------------ copy warp
   if (k == nch) {
     if (lane != 0) return;
     const int rbytes = Cfg::row_bytes(nch);
-    RowCursor ld = cur;  // next row to load
-    int nl = 0, nst = 0;  // rows loaded, rows stored
+    // one row's copies: the lattice's geometry, maps and parity, the row
+    auto copy_row = [&](auto LOAD, const RowCursor& rc, int item, int s) {
+      const uint32_t st = stage0 + s * Cfg::STAGE_BYTES;
+      const uint32_t bar = decltype(LOAD)::value ? full0 + 8 * s : 0;
+      if constexpr (BATCH) {
+        const RowItem<L>& it = items[item];
+        rows_copy<L, ST, LW, decltype(LOAD)::value>(it.a.g, it.maps, (int)((it.t0 + step) & 1),
+                                                     rc, st, bar);
+      } else {
+        rows_copy<L, ST, LW, decltype(LOAD)::value>(g, maps, a.parity, rc, st, bar);
+      }
+    };
+    // the item of global row r and its (y, z) there (BATCH), from a search
+    // of the items' first rows
+    auto locate = [&](long long r, RowCursor& rc) {
+      int lo = 0, hi = n_items - 1;
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (items[mid].first_row <= r) lo = mid; else hi = mid - 1;
+      }
+      const long long local = r - items[lo].first_row;
+      const int ny = items[lo].a.g.ny;
+      rc.r = r;
+      rc.yi = (int)(local % ny);
+      rc.zi = (int)(local / ny);
+      return lo;
+    };
+    RowCursor ld = cur;       // next row to load
+    RowCursor held[NS];       // the rows in the stages (BATCH: with their items)
+    int held_item[NS];
+    int nl = 0, nst = 0;      // rows loaded, rows stored
     bool failed = false;
-    for (; nl < NS && ld.r < nrows; ++nl) {
-      mbar_expect_tx(full0 + 8 * nl, rbytes);
-      rows_copy<L, ST, LW, true>(g, maps, P, ld, stage0 + nl * Cfg::STAGE_BYTES, full0 + 8 * nl);
-      ld.advance(gridDim.x, dyr, dzr, g.ny);
-    }
+    auto load_next = [&](int s) {
+      int item = 0;
+      bool live = true;
+      if constexpr (BATCH) {
+        item = locate(ld.r, held[s]);
+        // a lattice that has done its steps sits this step out: its row is
+        // neither loaded nor stored, the update warps see item -1
+        live = items[item].t0 + step < items[item].t_end;
+        if (!live) item = -1;
+        meta[s] = item;  // published to the update warps by the arrival below
+      } else {
+        held[s] = ld;
+      }
+      held_item[s] = item;
+      if (live) {
+        mbar_expect_tx(full0 + 8 * s, rbytes);
+        copy_row(IC<1>{}, held[s], item, s);
+      } else {
+        mbar_arrive(full0 + 8 * s);
+      }
+      if constexpr (BATCH) ld.r += gridDim.x;
+      else ld.advance(gridDim.x, dyr, dzr, g.ny);
+      ++nl;
+    };
+    while (nl < NS && ld.r < nrows) load_next(nl);
     while (nst < nl) {
       const int s = nst % NS;
       if (!rows_wait(empty0 + 8 * s, (nst / NS) & 1, kRowsWaitCycles, abort_flag)) {
         failed = true;
         break;
       }
-      rows_copy<L, ST, LW, false>(g, maps, P, cur, stage0 + s * Cfg::STAGE_BYTES, 0);
-      cur.advance(gridDim.x, dyr, dzr, g.ny);
+      if (held_item[s] >= 0) copy_row(IC<0>{}, held[s], held_item[s], s);
       ++nst;
       if (ld.r < nrows) {
         bulk_wait_read<0>();  // the stores no longer read the stage
-        mbar_expect_tx(full0 + 8 * s, rbytes);
-        rows_copy<L, ST, LW, true>(g, maps, P, ld, stage0 + s * Cfg::STAGE_BYTES, full0 + 8 * s);
-        ld.advance(gridDim.x, dyr, dzr, g.ny);
-        ++nl;
+        load_next(s);
       }
     }
     bulk_wait_all();  // every store has landed
@@ -406,18 +481,27 @@ step_rows(StepArgs a, const __grid_constant__ RowMaps<L> maps) {
   // A lane past the end of a partial last chunk (x0 >= nx) takes lane 0's
   // positions, so its shared-memory reads stay inside the row, and counts as
   // solid, so it stores nothing.
-  const bool lane_ok = k * kChunk + 2 * lane < g.nx;
-  const int x0 = lane_ok ? k * kChunk + 2 * lane : 0;
-  const int xn = (x0 + 2 == g.nx) ? 0 : x0 + 2;
-  const int xm = (x0 == 0) ? g.nx - 2 : x0 - 2;
-  const int xe = (x0 == 0) ? g.nx - 1 : x0 - 1;
   auto posc = [](int x, int c) { return (x >> 6) * c * kChunk + (x & 63); };
-  const int p0_1 = x0, pn_1 = xn, pm_1 = xm, pe_1 = xe;
-  const int p0_2 = posc(x0, 2), pn_2 = posc(xn, 2), pm_2 = posc(xm, 2), pe_2 = posc(xe, 2);
   constexpr int COWN = Pl::ops[1].count;
-  const int p0_own = posc(x0, COWN);
-  const CollideParams<S> prm{(S)a.omega, (S)a.omega2, (S)a.fx, (S)a.fy, (S)a.fz};
-  const long long consume_limit = a.wait_cycles > 0 ? a.wait_cycles : kRowsWaitCycles;
+  bool lane_ok;
+  int x0, p0_1, pn_1, pm_1, pe_1, p0_2, pn_2, pm_2, pe_2, p0_own;
+  CollideParams<S> prm;
+  auto set_lattice = [&](const StepArgs& la) {
+    const int nx = la.g.nx;
+    lane_ok = k * kChunk + 2 * lane < nx;
+    x0 = lane_ok ? k * kChunk + 2 * lane : 0;
+    const int xn = (x0 + 2 == nx) ? 0 : x0 + 2;
+    const int xm = (x0 == 0) ? nx - 2 : x0 - 2;
+    const int xe = (x0 == 0) ? nx - 1 : x0 - 1;
+    p0_1 = x0; pn_1 = xn; pm_1 = xm; pe_1 = xe;
+    p0_2 = posc(x0, 2); pn_2 = posc(xn, 2); pm_2 = posc(xm, 2); pe_2 = posc(xe, 2);
+    p0_own = posc(x0, COWN);
+    prm = CollideParams<S>{(S)la.omega, (S)la.omega2, (S)la.fx, (S)la.fy, (S)la.fz};
+  };
+  int cur_item = -1;
+  if constexpr (!BATCH) set_lattice(a);
+  const long long consume_limit = BATCH ? kRowsWaitCycles
+                                        : (a.wait_cycles > 0 ? a.wait_cycles : kRowsWaitCycles);
 
   bool failed = false;
   for (int j = 0; cur.r < nrows; ++j) {
@@ -427,6 +511,19 @@ step_rows(StepArgs a, const __grid_constant__ RowMaps<L> maps) {
       break;
     }
     E* sl = reinterpret_cast<E*>(rows_smem + s * Cfg::STAGE_BYTES);
+    if constexpr (BATCH) {
+      const int item = meta[s];
+      if (item < 0) {  // a finished lattice's row: nothing to update
+        __syncwarp();
+        if (lane == 0) mbar_arrive(empty0 + 8 * s);
+        cur.r += gridDim.x;
+        continue;
+      }
+      if (item != cur_item) {
+        cur_item = item;
+        set_lattice(items[item].a);
+      }
+    }
 
     // ---- the pair's 27 values from the shared blocks.  An x-shifted remote
     // pair straddles two words: the collision operators decode it from both
@@ -457,7 +554,7 @@ step_rows(StepArgs a, const __grid_constant__ RowMaps<L> maps) {
     });
 
     bool solid0 = !lane_ok, solid1 = !lane_ok;
-    if (a.flags) {
+    if (!BATCH && a.flags) {
       const uint16_t fl = *reinterpret_cast<const uint16_t*>(
           a.flags + ((long long)(cur.zi + g.hz) * g.sy + (cur.yi + g.hy)) * g.sx + x0);
       solid0 = solid0 || (fl & 0xffu) != 0;
@@ -471,7 +568,7 @@ step_rows(StepArgs a, const __grid_constant__ RowMaps<L> maps) {
       });
       if constexpr (FORCE) {  // the force per node of the pair (Boussinesq)
         CollideParams<S, V> pv{prm.omega, prm.omega2, bc<V>(prm.fx), bc<V>(prm.fy), bc<V>(prm.fz)};
-        if (a.temp) {
+        if (!BATCH && a.temp) {
           const S* T = reinterpret_cast<const S*>(a.temp);
           const size_t kk = ((size_t)cur.zi * g.ny + cur.yi) * g.nx + x0;
           buoyant_force<V>(a, pack2v(load_pair2(T, kk)), pv.fx, pv.fy, pv.fz);
@@ -531,7 +628,7 @@ step_rows(StepArgs a, const __grid_constant__ RowMaps<L> maps) {
     if (__any_sync(0xffffffffu, solid0 || solid1)) store_all(IC<1>{});
     else store_all(IC<0>{});
 
-    if (a.rho)
+    if (!BATCH && a.rho)
       store_macro_pair<S>(a, ((size_t)cur.zi * g.ny + cur.yi) * g.nx + x0, m, solid0, solid1);
 
     // ---- row done for this warp: its shared-memory writes become visible
@@ -539,12 +636,31 @@ step_rows(StepArgs a, const __grid_constant__ RowMaps<L> maps) {
     fence_async_smem();
     __syncwarp();
     if (lane == 0) mbar_arrive(empty0 + 8 * s);
-    cur.advance(gridDim.x, dyr, dzr, g.ny);
+    if constexpr (BATCH) cur.r += gridDim.x;
+    else cur.advance(gridDim.x, dyr, dzr, g.ny);
   }
   if (failed && lane == 0) {
     atomicExch(abort_flag, 1);
     if (a.err) atomicExch(a.err, 1);
   }
+}
+
+template <class L, int ST, int OP, int EQ, bool SH, bool FORCE, int LW>
+__global__ void __launch_bounds__((LW + 1) * 32, rows_min_blocks<OP, ST, LW>())
+step_rows(StepArgs a, const __grid_constant__ RowMaps<L> maps) {
+  rows_body<L, ST, OP, EQ, SH, FORCE, LW, false>(a, maps, nullptr, 0, 0, 0);
+}
+
+// One time step of the rows of a batch (launch descriptor read from device
+// memory, so a captured launch serves any resident set of its group).
+template <class L, int ST, int OP, int EQ, int LW>
+__global__ void __launch_bounds__((LW + 1) * 32, rows_min_blocks<OP, ST, LW>())
+batch_rows(const RowItem<L>* __restrict__ items, const RowBatch* __restrict__ desc, int step) {
+  const RowBatch d = *desc;
+  if (d.n_items <= 0 || d.n_rows <= 0) return;
+  const RowItem<L>* it = items + d.first_item;
+  rows_body<L, ST, OP, EQ, true, false, LW, true>(it[0].a, it[0].maps, it, d.n_items, d.n_rows,
+                                                 step);
 }
 
 }  // namespace m3lb

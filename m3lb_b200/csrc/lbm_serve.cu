@@ -18,6 +18,18 @@
 // what else is resident: it is bit-identical alone, in any mix, and through
 // the single-lattice C ABI with the same kernel.
 //
+// With 16-bit storage the lattices can instead go through the row kernel
+// (lbm_rows.cuh, batch_rows): one persistent launch per time step and per
+// (operator, row width in chunks) group, each CTA moving whole rows of
+// whichever lattice of its group they belong to through shared memory by
+// TMA.  The launch reads its group's row count and item table from device
+// memory, and a lattice that has done its steps sits the rest of a round
+// out inside the kernel, so every round runs the configured length and a
+// round's launches are captured once per (groups present, length) and
+// replayed from then on, whatever lattices come and go.  The row kernel's
+// per-node arithmetic is the paired kernel's, so results stay bit-identical
+// across the two paths.
+//
 // The reference has no serving loop; this file has no counterpart there.
 #include <cuda_runtime.h>
 
@@ -36,6 +48,7 @@
 #include "../../include/m3lb.h"
 #include "lbm_host.h"
 #include "lbm_kernels.cuh"
+#include "lbm_rows.cuh"
 
 using namespace m3lb;
 
@@ -50,6 +63,9 @@ struct BatchItem {
 
 constexpr int kBatchThreads = 128;
 constexpr int kMaxItems = 1024;  // lattices in one launch (shared-memory search table)
+// Batched row launches: one group per (operator, row width in chunks).
+constexpr int kRowGroups = 4 * kRowsMaxChunks;
+using RowItem27 = RowItem<D3Q27>;
 
 // One time step of every lattice in `items` (all with operator OP): warp u
 // of the grid updates unit u - first_unit of the item whose range holds u,
@@ -144,6 +160,7 @@ int fail(int code, const char* fmt, ...) {
 using Clock = std::chrono::steady_clock;
 
 struct Lattice {
+  RowMaps<D3Q27> maps{};    // the row kernel's tensor maps of its populations
   m3lb_request req;
   Geo g{};
   const Launchers* L = nullptr;
@@ -173,8 +190,21 @@ struct Inflight {
   double lups = 0;
 };
 
-// Rounds the tuner measures with each mapping before it fixes the faster.
+// Rounds the tuner measures with each mapping before it fixes the fastest,
+// and its candidates: 64-slot chunks, dense 64-node strips, whole rows.
 constexpr int kTuneRounds = 6;
+constexpr int kCands = 3;
+constexpr int kCandRows = 2;
+
+// A captured round of batched row launches: the groups it launches and its
+// length.
+struct RowGraph {
+  unsigned mask = 0;
+  int R = 0;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+};
+constexpr int kRowGraphs = 8;
 
 }  // namespace
 
@@ -210,9 +240,19 @@ struct m3lb_server {
   // M3LB_MAP_TUNE: rounds launched / measured with each mapping, their time
   // and lattice updates, the mapping of the round being built (-1: the
   // automatic rule), and the choice once made (-1 until then)
-  int tune_launched[2] = {0, 0}, tune_measured[2] = {0, 0};
-  double tune_ms[2] = {0, 0}, tune_lups[2] = {0, 0};
+  int tune_launched[kCands] = {0, 0, 0}, tune_measured[kCands] = {0, 0, 0};
+  double tune_ms[kCands] = {0, 0, 0}, tune_lups[kCands] = {0, 0, 0};
   int tune_cand = -1, tuned = -1;
+  // batched row launches: device item table and per-group launch
+  // descriptors, their pinned host copies (two of each, as for items_host),
+  // the groups of the round being built, the captured rounds
+  RowItem27* ritems_dev = nullptr;
+  RowItem27* ritems_host = nullptr;
+  RowBatch* rdesc_dev = nullptr;
+  RowBatch* rdesc_host = nullptr;
+  unsigned row_mask = 0, prev_row_mask = ~0u;
+  int prev_row_R = -1;
+  std::vector<RowGraph> rgraphs;
   std::vector<cudaEvent_t> free_timing;
   double* red_slots = nullptr;      // pinned, kReduceVals per request of a run
   int red_cap = 0;
@@ -242,6 +282,22 @@ struct SrvGuard {
 size_t footprint(const m3lb_serve_config& c, int n) {
   const Geo g = make_geo(n, n, n, 1, 1, 1);
   return pop_elems(g, 27) * (size_t)elem_bytes(c.storage) + 16 * (size_t)n * n * n;
+}
+
+// Whole-row launches need 16-bit storage (their stage of 4 rows of up to 8
+// chunks fits a CTA) and rows of at most 8 chunks (N <= 512, as admitted).
+bool rows_eligible(const m3lb_server* s) { return elem_bytes(s->cfg.storage) == 2; }
+
+// Whether the round being built goes through the row kernel: as configured;
+// automatic: whenever eligible; tuner: its candidate or its choice.
+bool use_rows(const m3lb_server* s) {
+  if (!rows_eligible(s)) return false;
+  if (s->cfg.mapping == M3LB_MAP_ROWS || s->cfg.mapping == M3LB_MAP_AUTO) return true;
+  if (s->cfg.mapping == M3LB_MAP_TUNE) {
+    const int m = s->tuned >= 0 ? s->tuned : s->tune_cand;
+    return m == kCandRows;
+  }
+  return false;
 }
 
 double now_s(Clock::time_point t0) {
@@ -314,6 +370,8 @@ int admit(m3lb_server* s, const m3lb_request& r, double t_now) {
   sa.rho = fld; sa.ux = fld + nn; sa.uy = fld + 2 * nn; sa.uz = fld + 3 * nn;
   SRV_TRY(l.L->seed(sa, r.op, 0, true, s->stream));
   SRV_TRY(cudaFreeAsync(fld, s->stream));
+  if (elem_bytes(s->cfg.storage) == 2)
+    SRV_TRY(l.L->row_maps(lattice_args(s, l), &l.maps, sizeof l.maps));
   s->resident += l.bytes;
   s->active.push_back(l);
   ++s->set_version;
@@ -376,14 +434,22 @@ int retire_oldest(m3lb_server* s, Clock::time_point t0) {
     s->tune_measured[f.cand] += 1;
     s->free_timing.push_back(f.t0);
     s->free_timing.push_back(f.t1);
-    if (s->tuned < 0 && s->tune_measured[0] >= kTuneRounds && s->tune_measured[1] >= kTuneRounds) {
-      // the higher rate of lattice updates per second of GPU time
-      const double r0 = s->tune_lups[0] / std::max(s->tune_ms[0], 1e-9);
-      const double r1 = s->tune_lups[1] / std::max(s->tune_ms[1], 1e-9);
-      s->tuned = r1 > r0 ? 1 : 0;
-      s->stats.tuned_mapping = s->tuned ? M3LB_MAP_DENSE : M3LB_MAP_CHUNKS;
-      s->stats.tuned_chunks_mlups = r0 * 1e-3;
-      s->stats.tuned_dense_mlups = r1 * 1e-3;
+    const int ncand = rows_eligible(s) ? kCands : 2;
+    bool all = true;
+    for (int c = 0; c < ncand; ++c) all = all && s->tune_measured[c] >= kTuneRounds;
+    if (s->tuned < 0 && all) {
+      // the highest rate of lattice updates per second of GPU time
+      double best = -1;
+      for (int c = 0; c < ncand; ++c) {
+        const double r = s->tune_lups[c] / std::max(s->tune_ms[c], 1e-9);
+        if (r > best) { best = r; s->tuned = c; }
+      }
+      static const int kMap[kCands] = {M3LB_MAP_CHUNKS, M3LB_MAP_DENSE, M3LB_MAP_ROWS};
+      s->stats.tuned_mapping = kMap[s->tuned];
+      s->stats.tuned_chunks_mlups = s->tune_lups[0] / std::max(s->tune_ms[0], 1e-9) * 1e-3;
+      s->stats.tuned_dense_mlups = s->tune_lups[1] / std::max(s->tune_ms[1], 1e-9) * 1e-3;
+      if (ncand > kCandRows)
+        s->stats.tuned_rows_mlups = s->tune_lups[2] / std::max(s->tune_ms[2], 1e-9) * 1e-3;
     }
   }
   for (size_t i : f.finishing) {
@@ -411,7 +477,7 @@ BatchItem* host_table(m3lb_server* s) { return s->items_host + (size_t)s->flip *
 void choose_mapping(m3lb_server* s) {
   if (s->cfg.mapping == M3LB_MAP_TUNE) {
     const int m = s->tuned >= 0 ? s->tuned : s->tune_cand;
-    if (m >= 0) {
+    if (m == 0 || m == 1) {
       for (int o = 0; o < 4; ++o) s->dense[o] = m == 1;
       return;
     }
@@ -522,6 +588,103 @@ int run_round(m3lb_server* s, int R) {
   return M3LB_OK;
 }
 
+// The batched row tables of the resident set for a round: items grouped by
+// (operator, row width), each group's rows numbered in item order; the
+// groups present in s->row_mask.
+void build_row_items(m3lb_server* s) {
+  RowItem27* tab = s->ritems_host + (size_t)s->flip * kMaxItems;
+  RowBatch* desc = s->rdesc_host + (size_t)s->flip * kRowGroups;
+  int count[kRowGroups] = {};
+  for (const Lattice& l : s->active) {
+    int o = 0;
+    while (kOps[o] != l.req.op) ++o;
+    ++count[o * kRowsMaxChunks + l.g.nch - 1];
+  }
+  int first = 0;
+  s->row_mask = 0;
+  for (int g = 0; g < kRowGroups; ++g) {
+    desc[g].first_item = first;
+    desc[g].n_items = 0;
+    desc[g].n_rows = 0;
+    first += count[g];
+    if (count[g]) s->row_mask |= 1u << g;
+  }
+  for (const Lattice& l : s->active) {
+    int o = 0;
+    while (kOps[o] != l.req.op) ++o;
+    RowBatch& d = desc[o * kRowsMaxChunks + l.g.nch - 1];
+    RowItem27& it = tab[d.first_item + d.n_items++];
+    it.maps = l.maps;
+    it.a = lattice_args(s, l);
+    it.first_row = d.n_rows;
+    it.t0 = l.t;
+    it.t_end = l.req.steps;
+    d.n_rows += (long long)l.g.ny * l.g.nz;
+  }
+}
+
+int launch_rows_round(m3lb_server* s, int R) {
+  const Launchers* T = table_for(27, s->cfg.storage);
+  for (int step = 0; step < R; ++step)
+    for (int g = 0; g < kRowGroups; ++g) {
+      if (!(s->row_mask >> g & 1u)) continue;
+      SRV_TRY(T->batch_rows(s->ritems_dev, s->rdesc_dev + g, kOps[g / kRowsMaxChunks],
+                            g % kRowsMaxChunks + 1, step, s->stream));
+    }
+  return M3LB_OK;
+}
+
+// A round of batched row launches: the tables go to the device ahead of the
+// launches; a round whose groups and length match a captured one replays it,
+// a round repeating the previous round's groups and length is captured, and
+// any other launches directly.
+int run_round_rows(m3lb_server* s, int R) {
+  s->flip ^= 1;
+  build_row_items(s);
+  const size_t n = s->active.size();
+  if (n)
+    SRV_TRY(cudaMemcpyAsync(s->ritems_dev, s->ritems_host + (size_t)s->flip * kMaxItems,
+                            n * sizeof(RowItem27), cudaMemcpyHostToDevice, s->stream));
+  SRV_TRY(cudaMemcpyAsync(s->rdesc_dev, s->rdesc_host + (size_t)s->flip * kRowGroups,
+                          kRowGroups * sizeof(RowBatch), cudaMemcpyHostToDevice, s->stream));
+  RowGraph* hit = nullptr;
+  for (RowGraph& g : s->rgraphs)
+    if (g.mask == s->row_mask && g.R == R) hit = &g;
+  const bool repeat = s->prev_row_mask == s->row_mask && s->prev_row_R == R;
+  s->prev_row_mask = s->row_mask;
+  s->prev_row_R = R;
+  if (!hit && repeat && (int)s->rgraphs.size() < kRowGraphs) {
+    RowGraph g;
+    g.mask = s->row_mask;
+    g.R = R;
+    SRV_TRY(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+    const int rc = launch_rows_round(s, R);
+    const cudaError_t e = cudaStreamEndCapture(s->stream, &g.graph);
+    if (rc) {
+      if (g.graph) cudaGraphDestroy(g.graph);
+      return rc;
+    }
+    SRV_TRY(e);
+    SRV_TRY(cudaGraphInstantiate(&g.exec, g.graph, 0));
+    s->rgraphs.push_back(g);
+    hit = &s->rgraphs.back();
+    s->stats.graph_captures += 1;
+  }
+  if (hit) {
+    SRV_TRY(cudaGraphLaunch(hit->exec, s->stream));
+    s->stats.graph_launches += 1;
+  } else {
+    const int rc = launch_rows_round(s, R);
+    if (rc) return rc;
+  }
+  for (Lattice& l : s->active) l.t = std::min<long long>(l.t + R, l.req.steps);
+  s->stats.rounds += 1;
+  const long long groups = __builtin_popcount(s->row_mask);
+  s->stats.launches += (long long)R * groups;
+  s->stats.rows_launches += (long long)R * groups;
+  return M3LB_OK;
+}
+
 bool fits(const m3lb_server* s, const m3lb_request& r) {
   if (s->cfg.max_resident > 0 && (int)s->active.size() >= s->cfg.max_resident) return false;
   if ((int)s->active.size() >= kMaxItems) return false;
@@ -539,9 +702,11 @@ int m3lb_serve_create(const m3lb_serve_config* cfg, m3lb_server** out) {
     return fail(M3LB_ERR_UNSUPPORTED, "serve_create: storage %d is not served (F16, F16C, BF16, F32)",
                 cfg->storage);
   if (cfg->round_steps < 1) return fail(M3LB_ERR_INVALID, "serve_create: round_steps must be >= 1");
-  if (cfg->mapping < M3LB_MAP_AUTO || cfg->mapping > M3LB_MAP_TUNE)
+  if (cfg->mapping < M3LB_MAP_AUTO || cfg->mapping > M3LB_MAP_ROWS)
     return fail(M3LB_ERR_INVALID,
-                "serve_create: mapping must be M3LB_MAP_AUTO, _CHUNKS, _DENSE or _TUNE");
+                "serve_create: mapping must be M3LB_MAP_AUTO, _CHUNKS, _DENSE, _TUNE or _ROWS");
+  if (cfg->mapping == M3LB_MAP_ROWS && elem_bytes(cfg->storage) != 2)
+    return fail(M3LB_ERR_UNSUPPORTED, "serve_create: M3LB_MAP_ROWS needs 16-bit storage");
   auto* s = new m3lb_server();
   s->cfg = *cfg;
   cudaGetDevice(&s->device);
@@ -557,6 +722,11 @@ int m3lb_serve_create(const m3lb_serve_config* cfg, m3lb_server** out) {
       cudaMallocHost((void**)&s->items_host, 2 * 4 * kMaxItems * sizeof(BatchItem)) != cudaSuccess)
     return bail(fail(M3LB_ERR_MEMORY, "serve_create: cannot allocate the item tables"));
   std::memset(s->items_host, 0, 2 * 4 * kMaxItems * sizeof(BatchItem));
+  if (cudaMalloc((void**)&s->ritems_dev, kMaxItems * sizeof(RowItem27)) != cudaSuccess ||
+      cudaMallocHost((void**)&s->ritems_host, 2 * kMaxItems * sizeof(RowItem27)) != cudaSuccess ||
+      cudaMalloc((void**)&s->rdesc_dev, kRowGroups * sizeof(RowBatch)) != cudaSuccess ||
+      cudaMallocHost((void**)&s->rdesc_host, 2 * kRowGroups * sizeof(RowBatch)) != cudaSuccess)
+    return bail(fail(M3LB_ERR_MEMORY, "serve_create: cannot allocate the row tables"));
   *out = s;
   return M3LB_OK;
 }
@@ -618,16 +788,27 @@ int m3lb_serve_run(m3lb_server* s, double time_limit) {
       }
       continue;
     }
-    long long R = s->cfg.round_steps;
-    for (const Lattice& l : s->active) R = std::min<long long>(R, l.req.steps - l.t);
+    // the mapping tuner alternates its candidates over its first rounds
+    s->tune_cand = -1;
+    if (s->cfg.mapping == M3LB_MAP_TUNE && s->tuned < 0) {
+      const int ncand = rows_eligible(s) ? kCands : 2;
+      int c = 0;
+      for (int k = 1; k < ncand; ++k)
+        if (s->tune_launched[k] < s->tune_launched[c]) c = k;
+      if (s->tune_launched[c] < kTuneRounds) s->tune_cand = c;
+    }
+    // whole-row rounds run the configured length (a lattice that finishes
+    // inside the round sits the rest out); chunk rounds end with the first
+    // lattice to finish
+    const bool rows = use_rows(s);
+    long long R = rows ? 0 : s->cfg.round_steps;
+    for (const Lattice& l : s->active) {
+      if (rows) R = std::max<long long>(R, l.req.steps - l.t);
+      else R = std::min<long long>(R, l.req.steps - l.t);
+    }
+    if (rows) R = std::min<long long>(R, s->cfg.round_steps);
     Inflight f;
     if (R > 0) {
-      // the mapping tuner alternates the two mappings over its first rounds
-      s->tune_cand = -1;
-      if (s->cfg.mapping == M3LB_MAP_TUNE && s->tuned < 0) {
-        const int c = s->tune_launched[0] <= s->tune_launched[1] ? 0 : 1;
-        if (s->tune_launched[c] < kTuneRounds) s->tune_cand = c;
-      }
       if (s->tune_cand >= 0) {
         for (int k = 0; k < 2; ++k) {
           if (s->free_timing.empty()) {
@@ -639,11 +820,13 @@ int m3lb_serve_run(m3lb_server* s, double time_limit) {
           s->free_timing.pop_back();
         }
         f.cand = s->tune_cand;
-        for (const Lattice& l : s->active) f.lups += (double)l.req.n * l.req.n * l.req.n * (double)R;
+        for (const Lattice& l : s->active)
+          f.lups += (double)l.req.n * l.req.n * l.req.n *
+                    (double)std::min<long long>(R, l.req.steps - l.t);
         s->tune_launched[f.cand] += 1;
         SRV_TRY(cudaEventRecord(f.t0, s->stream));
       }
-      const int rc = run_round(s, (int)R);
+      const int rc = rows ? run_round_rows(s, (int)R) : run_round(s, (int)R);
       if (rc) return rc;
       if (f.cand >= 0) SRV_TRY(cudaEventRecord(f.t1, s->stream));
     }
@@ -724,6 +907,14 @@ int m3lb_serve_destroy(m3lb_server* s) {
   if (s->partials) cudaFree(s->partials);
   if (s->items_dev) cudaFree(s->items_dev);
   if (s->items_host) cudaFreeHost(s->items_host);
+  for (RowGraph& g : s->rgraphs) {
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+    if (g.graph) cudaGraphDestroy(g.graph);
+  }
+  if (s->ritems_dev) cudaFree(s->ritems_dev);
+  if (s->ritems_host) cudaFreeHost(s->ritems_host);
+  if (s->rdesc_dev) cudaFree(s->rdesc_dev);
+  if (s->rdesc_host) cudaFreeHost(s->rdesc_host);
   if (s->red_slots) cudaFreeHost(s->red_slots);
   for (Inflight& f : s->inflight) {
     cudaEventDestroy(f.end);

@@ -76,7 +76,7 @@ class Server:
     """One serving loop on the current CUDA device."""
 
     MAPPINGS = {"auto": capi.MAP_AUTO, "chunks": capi.MAP_CHUNKS, "dense": capi.MAP_DENSE,
-                "tune": capi.MAP_TUNE}
+                "tune": capi.MAP_TUNE, "rows": capi.MAP_ROWS}
 
     def __init__(self, hbm_budget: int = 4 << 30, max_resident: int = 32, round_steps: int = 50,
                  storage: str = "f16", keep_fields: bool = False, mapping: str = "auto"):

@@ -1,10 +1,11 @@
 """Serving loop on the GPU (m3lb_serve_*).
 
 A request's result must not depend on what else is resident: the batched
-kernel runs the paired kernel's per-unit code for every lattice, so results
-are bit-identical alone, in a mix, under a one-lattice admission limit, with
-either warp-to-node mapping (chunks or dense), and through the single-lattice
-C ABI with the paired kernel.
+kernels run the paired kernel's per-node arithmetic for every lattice (the
+chunk and dense mappings its per-unit code, the row mapping the row kernel,
+bit-identical to it), so results are bit-identical alone, in a mix, under a
+one-lattice admission limit, with every mapping (chunks, dense strips, whole
+rows), and through the single-lattice C ABI with the paired kernel.
 """
 import ctypes as C
 
@@ -79,26 +80,60 @@ def test_dense_mapping_equals_chunks(cuda_device, storage):
 
 
 def test_auto_mapping_rule(cuda_device):
-    # every N a multiple of 64: chunks; one ragged lattice: dense for its operator
+    # 16-bit storage: whole rows, one launch per (operator, row width) group
+    # and step; FP32: every N a multiple of 64 takes chunks, one ragged
+    # lattice dense strips for its operator
     _, _, st = _serve([SV.Request(0, 0.0, 64, capi.OP_CM, 5, 0.05),
                        SV.Request(1, 0.0, 128, capi.OP_BGK, 5, 0.05)])
-    assert st.dense_launches == 0
+    assert st.rows_launches == st.launches == 10 and st.dense_launches == 0
     _, _, st = _serve([SV.Request(0, 0.0, 64, capi.OP_CM, 5, 0.05),
-                       SV.Request(1, 0.0, 96, capi.OP_BGK, 5, 0.05)])
+                       SV.Request(1, 0.0, 128, capi.OP_BGK, 5, 0.05)], "f32")
+    assert st.dense_launches == 0 and st.rows_launches == 0
+    _, _, st = _serve([SV.Request(0, 0.0, 64, capi.OP_CM, 5, 0.05),
+                       SV.Request(1, 0.0, 96, capi.OP_BGK, 5, 0.05)], "f32")
     assert st.dense_launches == 5 and st.launches == 10
 
 
-def test_tuned_mapping_measures_both_and_keeps_results(cuda_device):
-    # 200 steps in rounds of 10: 20 rounds, the first 12 alternate the mappings
-    reqs = [SV.Request(i, 0.0, n, op, 200, 0.05)
+@pytest.mark.parametrize("storage", ["f16", "f16c", "bf16"])
+def test_rows_mapping_equals_chunks(cuda_device, storage):
+    """Whole-row launches (one per operator and row width, lattices finishing
+    inside a round) give the chunk mapping's bits, ragged boxes included."""
+    reqs = MIX + RAGGED
+    ch, ch_f, _ = _serve(reqs, storage, mapping="chunks")
+    ro, ro_f, st = _serve(reqs, storage, mapping="rows", round_steps=8)
+    assert st.rows_launches == st.launches > 0
+    for r in reqs:
+        assert ro[r.id].status == 0
+        _same((ch[r.id], ch_f[r.id]), (ro[r.id], ro_f[r.id]))
+
+
+def test_rows_rounds_replay_captured_graphs(cuda_device):
+    """Lattices arriving and finishing at different times: row rounds keep
+    their length, so after the first two rounds of a group set every round
+    replays a captured graph, and the results equal the chunk mapping's."""
+    reqs = [SV.Request(i, 0.02 * i, n, op, steps, 0.05)
+            for i, (n, op, steps) in enumerate([(48, capi.OP_CM, 130), (80, capi.OP_BGK, 70),
+                                                (32, capi.OP_TRT, 210), (64, capi.OP_CM, 95),
+                                                (96, capi.OP_CM, 160), (48, capi.OP_BGK, 40)])]
+    ro, ro_f, st = _serve(reqs, mapping="rows", round_steps=10)
+    ch, ch_f, _ = _serve(reqs, mapping="chunks", round_steps=10)
+    assert st.graph_launches >= 0.5 * st.rounds, (st.graph_launches, st.rounds)
+    for r in reqs:
+        _same((ro[r.id], ro_f[r.id]), (ch[r.id], ch_f[r.id]))
+
+
+def test_tuned_mapping_measures_all_and_keeps_results(cuda_device):
+    # 300 steps in rounds of 10: 30 rounds, the first 18 alternate the three
+    # mappings (whole rows, chunks, dense strips), 6 timed rounds each
+    reqs = [SV.Request(i, 0.0, n, op, 300, 0.05)
             for i, (n, op) in enumerate([(48, capi.OP_CM), (80, capi.OP_BGK), (32, capi.OP_TRT)])]
     tu, tu_f, st = _serve(reqs, round_steps=10, mapping="tune")
     ch, ch_f, _ = _serve(reqs, round_steps=10, mapping="chunks")
-    assert st.tuned_mapping in (capi.MAP_CHUNKS, capi.MAP_DENSE)
-    assert st.tuned_chunks_mlups > 0 and st.tuned_dense_mlups > 0
-    faster = capi.MAP_DENSE if st.tuned_dense_mlups > st.tuned_chunks_mlups else capi.MAP_CHUNKS
-    assert st.tuned_mapping == faster
-    assert 0 < st.dense_launches < st.launches
+    rates = {capi.MAP_CHUNKS: st.tuned_chunks_mlups, capi.MAP_DENSE: st.tuned_dense_mlups,
+             capi.MAP_ROWS: st.tuned_rows_mlups}
+    assert all(v > 0 for v in rates.values()), rates
+    assert st.tuned_mapping == max(rates, key=rates.get)
+    assert 0 < st.dense_launches < st.launches and 0 < st.rows_launches < st.launches
     for r in reqs:
         _same((tu[r.id], tu_f[r.id]), (ch[r.id], ch_f[r.id]))
 

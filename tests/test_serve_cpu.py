@@ -55,9 +55,12 @@ def test_serve_config_is_checked_before_any_device_work():
     import ctypes as C
     lib = capi.lib()
     h = C.c_void_p()
-    bad_mapping = capi.ServeConfig(1 << 30, 8, 50, capi.STORE_F16, 0, 4)
+    bad_mapping = capi.ServeConfig(1 << 30, 8, 50, capi.STORE_F16, 0, 5)
     assert lib.m3lb_serve_create(C.byref(bad_mapping), C.byref(h)) == capi.ERR_INVALID
     assert b"mapping" in lib.m3lb_last_error()
+    rows_f32 = capi.ServeConfig(1 << 30, 8, 50, capi.STORE_F32, 0, capi.MAP_ROWS)
+    assert lib.m3lb_serve_create(C.byref(rows_f32), C.byref(h)) == capi.ERR_UNSUPPORTED
+    assert b"16-bit" in lib.m3lb_last_error()
     bad_round = capi.ServeConfig(1 << 30, 8, 0, capi.STORE_F16, 0, capi.MAP_DENSE)
     assert lib.m3lb_serve_create(C.byref(bad_round), C.byref(h)) == capi.ERR_INVALID
     f64 = capi.ServeConfig(1 << 30, 8, 50, capi.STORE_F64, 0, capi.MAP_AUTO)
