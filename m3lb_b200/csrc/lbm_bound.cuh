@@ -27,7 +27,17 @@
 namespace m3lb {
 
 // ------------------------------------------------------------ node access
+// Coordinates of a padded node index (32-bit division when the block has
+// fewer than 2^31 nodes, as every lattice up to ~1290^3 does).
 __device__ __forceinline__ void padded_coords(const Geo& g, long long n, int& x, int& y, int& z) {
+  if (g.n_padded < (1LL << 31)) {
+    const unsigned u = (unsigned)n, sx = (unsigned)g.sx, sy = (unsigned)g.sy;
+    const unsigned r = u / sx;
+    x = (int)(u - r * sx);
+    y = (int)(r % sy);
+    z = (int)(r / sy);
+    return;
+  }
   x = (int)(n % g.sx);
   y = (int)((n / g.sx) % g.sy);
   z = (int)(n / ((long long)g.sx * g.sy));
@@ -40,24 +50,27 @@ __device__ __forceinline__ size_t interior_index(const Geo& g, long long n) {
   return ((size_t)(z - g.hz) * g.ny + (y - g.hy)) * g.nx + (x - g.hx);
 }
 
-// The Q populations about to arrive at node n (Access::load_pair, parity P).
+// The Q populations about to arrive at node n (Access::load_pair, parity P):
+// the node's own slot of direction 0 plus, per direction, a compile-time
+// direction offset and the neighbour's per-axis offsets (AxisSteps, the wrap
+// or clamp folded in), as the one-node step kernel addresses them.
 template <class L, int ST, class R>
 __device__ __forceinline__ void load_pops(const StepArgs& a, long long n, R* f) {
   using E = typename StoreT<ST>::elem;
   const Geo& g = a.g;
   int x, y, z;
   padded_coords(g, n, x, y, z);
-  NodeNb<L> nb;
-  node_neighbours<L>(g, x, y, z, nb);
-  const E* A = reinterpret_cast<const E*>(a.f);
+  const E* own = reinterpret_cast<const E*>(a.f) + slot<L::Q>(g, x, y, z, 0);
+  const AxisSteps<L::Q> st = axis_steps<L::Q>(g, x, y, z);
   const int P = a.parity;
-  f[0] = to_real(A[slot<L::Q>(g, x, y, z, 0)]);
-#pragma unroll
-  for (int i = 1; i < L::Q; i += 2) {
-    const int* m = nb.nb[i];
-    f[i] = to_real(A[slot<L::Q>(g, x, y, z, i + P)]);
-    f[i + 1] = to_real(A[slot<L::Q>(g, m[0], m[1], m[2], i + 1 - P)]);
-  }
+  const E* up = own + P * kChunk;        // slot i + P of the node
+  const E* dn = own + (1 - P) * kChunk;  // slot i + 1 - P, before the neighbour offset
+  f[0] = to_real(own[0]);
+  static_for<1, L::Q, 2>([&](auto I) {
+    constexpr int i = decltype(I)::value;
+    f[i] = to_real(up[i * kChunk]);
+    f[i + 1] = to_real(dn[nb_offset<L, i>(st) + i * kChunk]);
+  });
 }
 template <class L, int ST, class R>
 __device__ __forceinline__ void store_pops(const StepArgs& a, long long n, const R* f) {
@@ -65,17 +78,17 @@ __device__ __forceinline__ void store_pops(const StepArgs& a, long long n, const
   const Geo& g = a.g;
   int x, y, z;
   padded_coords(g, n, x, y, z);
-  NodeNb<L> nb;
-  node_neighbours<L>(g, x, y, z, nb);
-  E* A = reinterpret_cast<E*>(a.f);
+  E* own = reinterpret_cast<E*>(a.f) + slot<L::Q>(g, x, y, z, 0);
+  const AxisSteps<L::Q> st = axis_steps<L::Q>(g, x, y, z);
   const int P = a.parity;
-  A[slot<L::Q>(g, x, y, z, 0)] = from_real<E>(f[0]);
-#pragma unroll
-  for (int i = 1; i < L::Q; i += 2) {
-    const int* m = nb.nb[i];
-    A[slot<L::Q>(g, m[0], m[1], m[2], i + 1 - P)] = from_real<E>(f[i]);
-    A[slot<L::Q>(g, x, y, z, i + P)] = from_real<E>(f[i + 1]);
-  }
+  E* up = own + P * kChunk;
+  E* dn = own + (1 - P) * kChunk;
+  own[0] = from_real<E>(f[0]);
+  static_for<1, L::Q, 2>([&](auto I) {
+    constexpr int i = decltype(I)::value;
+    dn[nb_offset<L, i>(st) + i * kChunk] = from_real<E>(f[i]);
+    up[i * kChunk] = from_real<E>(f[i + 1]);
+  });
 }
 // Populations of the k-th node a list node reads, unshifted when USH; from
 // the snapshot inside a step (SNAP), from the array outside one.
