@@ -245,9 +245,17 @@ __device__ __forceinline__ R moments(const R* g, R* m) {
   return sm;
 }
 
-// Wall velocity of a list node: the per-node field when set, else its state.
+// Wall velocity of list node idx: the per-node field when set, else its
+// state.  A node whose velocities are all +0 (not `moving`) gets the same
+// products with +0 without reading its BNode.
 template <class R>
-__device__ __forceinline__ void wall_velocity(const BoundArgs& b, const BNode& nd, R* uw) {
+__device__ __forceinline__ void wall_velocity(const BoundArgs& b, const BHead& h, int idx, R* uw) {
+  if (!h.moving) {
+    const R z = b.field_on ? R(b.field_scale) * R(0) : R(0) * R(b.scale);
+    uw[0] = uw[1] = uw[2] = z;
+    return;
+  }
+  const BNode& nd = b.nodes[idx];
 #pragma unroll
   for (int a = 0; a < 3; ++a)
     uw[a] = b.field_on ? R(b.field_scale) * R(nd.un[a]) : R(nd.u[a]) * R(b.scale);
@@ -268,21 +276,22 @@ __device__ __forceinline__ void up_velocity(const StepArgs& a, const BoundArgs& 
 // populations f.  Returns true when the node is finished (the outflow codes
 // that overwrite it), false when it goes on to collide.
 template <class L, int ST, int OP, int EQ, bool SH, bool FORCE, class R>
-__device__ __forceinline__ bool regwall(const StepArgs& a, const BoundArgs& b, int idx, R* f) {
-  const BNode& nd = b.nodes[idx];
+__device__ __forceinline__ bool regwall(const StepArgs& a, const BoundArgs& b, const BHead& h,
+                                        int idx, R* f) {
+  const BNode& nd = b.nodes[idx];  // read only by the outflow and corner-stencil branches
   constexpr int Q = L::Q;
   constexpr bool USH = SH && OP != 0;                    // the no-collision mock runs raw
   constexpr int BEQ = OP >= 3 ? 1 : (OP == 0 ? 0 : EQ);  // EquilibriumOf (Regularized.hpp:47-57)
   shift_pops<L, USH>(f, R(1));
-  const unsigned code = nd.code;
+  const unsigned code = h.code;
   int nrm[3];
   normal_of_code(code, nrm);
   R uw[3];
-  wall_velocity(b, nd, uw);
+  wall_velocity(b, h, idx, uw);
   // has_forcing looks for a ForcingPolicy member type, which only BGK declares
   R Fv[3] = {0, 0, 0};
   if constexpr (FORCE && OP == 1) {
-    const CollideParams<R> fp = node_params<FORCE, R>(a, interior_index(a.g, nd.n));
+    const CollideParams<R> fp = node_params<FORCE, R>(a, interior_index(a.g, h.n));
     Fv[0] = fp.fx; Fv[1] = fp.fy; Fv[2] = fp.fz;
   }
   R ur[3] = {uw[0], uw[1], uw[2]};
@@ -299,7 +308,7 @@ __device__ __forceinline__ bool regwall(const StepArgs& a, const BoundArgs& b, i
       for (int i = 0; i < Q; ++i) f[i] = g[i] * sc;
     }
     shift_pops<L, USH>(f, R(-1));
-    store_pops<L, ST>(a, nd.n, f);
+    store_pops<L, ST>(a, h.n, f);
     return true;
   }
   if (code == kNrmOutEq) {                               // equilibrium at the upstream velocity
@@ -313,7 +322,7 @@ __device__ __forceinline__ bool regwall(const StepArgs& a, const BoundArgs& b, i
       f[decltype(I)::value] = bc_feq<L, BEQ, decltype(I)::value>(rw2, mu[0], mu[1], mu[2]);
     });
     shift_pops<L, USH>(f, R(-1));
-    store_pops<L, ST>(a, nd.n, f);
+    store_pops<L, ST>(a, h.n, f);
     return true;
   }
   if (code == kNrmOutXp) {                               // imposed density, closure normal velocity
@@ -371,7 +380,7 @@ __device__ __forceinline__ bool regwall(const StepArgs& a, const BoundArgs& b, i
                      kk * R(0.5) * (grad[1][2] + grad[2][1])};
     bc_apply_with_stress<L, BEQ>(f, rw, ur, Pi);
   } else {
-    bc_apply<L, BEQ>(f, rw, ur, nd.unk, b.force_bc ? Fv : (const R*)nullptr);
+    bc_apply<L, BEQ>(f, rw, ur, h.unk, b.force_bc ? Fv : (const R*)nullptr);
   }
   shift_pops<L, USH>(f, R(-1));
   return false;
@@ -403,25 +412,26 @@ __global__ void __launch_bounds__(kBndThreads) bnd_wall_rho(StepArgs a, BoundArg
   using R = typename StoreT<ST>::real;
   const int i = b.begin + (int)(blockIdx.x * blockDim.x + threadIdx.x);
   if (i >= b.end) return;
-  const BNode& nd = b.nodes[i];
-  if (nd.type != kRegWall || nd.code == kNrmCorner || nd.code == 0) return;
+  const BHead h = b.heads[i];
+  if (h.type != kRegWall || h.code == kNrmCorner || h.code == 0) return;
   R f[L::Q], uw[3];
-  load_pops<L, ST>(a, nd.n, f);
+  load_pops<L, ST>(a, h.n, f);
   shift_pops<L, USH>(f, R(1));
   int nrm[3];
-  normal_of_code(nd.code, nrm);
-  wall_velocity(b, nd, uw);
+  normal_of_code(h.code, nrm);
+  wall_velocity(b, h, i, uw);
   R* rho = reinterpret_cast<R*>(b.wall_rho);
-  rho[i] = (nd.code == kNrmOutXp || nd.code == kNrmOutEq) ? R(nd.u[3])
-         : (nd.code == kNrmOutFree) ? R(b.out_rho) : bc_density<L>(f, nrm, uw);
+  rho[i] = (h.code == kNrmOutXp || h.code == kNrmOutEq) ? R(b.nodes[i].u[3])
+         : (h.code == kNrmOutFree) ? R(b.out_rho) : bc_density<L>(f, nrm, uw);
 }
 // pass 2 (:696-711): corners extrapolated along a wall, 1 without a stencil.
 template <class R>
 __global__ void __launch_bounds__(kBndThreads) bnd_corner_rho(BoundArgs b) {
   const int i = b.begin + (int)(blockIdx.x * blockDim.x + threadIdx.x);
   if (i >= b.end) return;
+  const BHead h = b.heads[i];
+  if (h.type != kRegWall || h.code != kNrmCorner) return;
   const BNode& nd = b.nodes[i];
-  if (nd.type != kRegWall || nd.code != kNrmCorner) return;
   R* rho = reinterpret_cast<R*>(b.wall_rho);
   rho[i] = nd.c1 < 0 ? R(1) : R(2) * rho[nd.c1] - rho[nd.c2];
 }
@@ -433,19 +443,19 @@ __global__ void __launch_bounds__(kBndThreads) bnd_step(StepArgs a, BoundArgs b)
   using R = typename StoreT<ST>::real;
   const int i = b.begin + (int)(blockIdx.x * blockDim.x + threadIdx.x);
   if (i >= b.end) return;
-  const BNode& nd = b.nodes[i];
+  const BHead h = b.heads[i];
   R f[L::Q];
-  load_pops<L, ST>(a, nd.n, f);
-  if (nd.type == kSpecWall) {
-    spec_wall_permute<L>(f, spec_axis(nd.code));
-    store_pops<L, ST>(a, nd.n, f);
+  load_pops<L, ST>(a, h.n, f);
+  if (h.type == kSpecWall) {
+    spec_wall_permute<L>(f, spec_axis(h.code));
+    store_pops<L, ST>(a, h.n, f);
     return;
   }
-  if (nd.type == kSpecNode) spec_node_mirror<L>(f, nd.code);
-  else if (regwall<L, ST, OP, EQ, SH, FORCE>(a, b, i, f)) return;
-  const size_t k = interior_index(a.g, nd.n);
+  if (h.type == kSpecNode) spec_node_mirror<L>(f, h.code);
+  else if (regwall<L, ST, OP, EQ, SH, FORCE>(a, b, h, i, f)) return;
+  const size_t k = interior_index(a.g, h.n);
   const Macro<R> mc = collide<L, OP, EQ, SH, FORCE>(f, node_params<FORCE, R>(a, k));
-  store_pops<L, ST>(a, nd.n, f);
+  store_pops<L, ST>(a, h.n, f);
   if (a.rho) {
     reinterpret_cast<R*>(a.rho)[k] = mc.rho;
     reinterpret_cast<R*>(a.ux)[k] = mc.ux;
@@ -462,16 +472,17 @@ __global__ void __launch_bounds__(kBndThreads) bnd_macro(StepArgs a, BoundArgs b
   constexpr int Q = L::Q;
   const int i = b.begin + (int)(blockIdx.x * blockDim.x + threadIdx.x);
   if (i >= b.end) return;
+  const BHead h = b.heads[i];
+  if (h.type != kRegWall) return;
   const BNode& nd = b.nodes[i];
-  if (nd.type != kRegWall) return;
   R fw[Q];
-  load_pops<L, ST>(a, nd.n, fw);
+  load_pops<L, ST>(a, h.n, fw);
   shift_pops<L, USH>(fw, R(1));
-  const unsigned code = nd.code;
+  const unsigned code = h.code;
   int nrm[3];
   normal_of_code(code, nrm);
   R uw[3];
-  wall_velocity(b, nd, uw);
+  wall_velocity(b, h, i, uw);
   R rw;
   if (code == kNrmOutFree) {
     rw = R(b.out_rho);
@@ -516,7 +527,7 @@ __global__ void __launch_bounds__(kBndThreads) bnd_macro(StepArgs a, BoundArgs b
   }
   const Geo& g = a.g;
   int x, y, z;
-  padded_coords(g, nd.n, x, y, z);
+  padded_coords(g, h.n, x, y, z);
   const size_t k = ((size_t)(z - g.hz) * g.ny + (y - g.hy)) * g.nx + (x - g.hx);
   reinterpret_cast<R*>(a.rho)[k] = rw;
   reinterpret_cast<R*>(a.ux)[k] = uw[0];

@@ -354,8 +354,22 @@ struct BNode {
   double un[3];                // per-node wall velocity field
 };
 
+// The fields of a list node that every update reads, in a separate array of
+// 16-byte entries, so a warp reads those of its 32 consecutive nodes in one
+// coalesced request (a BNode is 184 bytes; reading single fields of 32 of
+// them touches a sector per node and field).
+struct alignas(16) BHead {
+  long long n;       // padded index (BNode::n)
+  uint32_t unk;      // BNode::unk
+  uint8_t type;      // BNode::type
+  uint8_t code;      // BNode::code
+  uint8_t moving;    // a bit of u[0..2] or un[0..2] is set: the wall velocity is read
+  uint8_t pad;
+};
+
 struct BoundArgs {
   const BNode* nodes;
+  const BHead* heads;          // one per list node, same order
   int begin, end;              // list positions of this launch
   void* wall_rho;              // arithmetic type, one per list node (corner densities)
   void* snap;                  // arithmetic type, Q per snapshot slot

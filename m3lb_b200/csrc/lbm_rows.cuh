@@ -248,11 +248,6 @@ __device__ __forceinline__ void fence_async_smem() {
   asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
 }
 
-// First chunk index (tensor coordinate) of padded row (py, pz).
-__device__ __forceinline__ int row_chunk(const Geo& g, int py, int pz) {
-  return (pz * g.sy + py) * g.nch;
-}
-
 // Interior row cursor: row r = (yi, zi), advanced by the grid's CTA count.
 struct RowCursor {
   long long r;
@@ -270,15 +265,25 @@ struct RowCursor {
   }
 };
 
-// The copies of one row by the calling thread.  LOAD: global -> stage
-// (completion on `bar`, whose expected bytes the caller has set); else
-// stage -> global, in one bulk group of this thread.
+// What the copies of a row need of its lattice, held in registers (read
+// through a pointer into global memory, the fields would be reloaded after
+// every copy, each of which clobbers memory).
+struct RowGeo {
+  int ny, nz, sy, sz, hy, hz, nch;
+  __device__ __forceinline__ static RowGeo of(const Geo& g) {
+    return RowGeo{g.ny, g.nz, g.sy, g.sz, g.hy, g.hz, g.nch};
+  }
+};
+
+// The copies of one row (interior row yi, zi) by the calling thread.  LOAD:
+// global -> stage (completion on `bar`, whose expected bytes the caller has
+// set); else stage -> global, in one bulk group of this thread.
 template <class L, int ST, int LW, bool LOAD>
-__device__ __forceinline__ void rows_copy(const Geo& g, const RowMaps<L>& maps, int P,
-                                          const RowCursor& rc, uint32_t stage, uint32_t bar) {
+__device__ __forceinline__ void rows_copy(const RowGeo g, const RowMaps<L>* maps, int P, int yi,
+                                          int zi, uint32_t stage, uint32_t bar) {
   using Pl = RowPlan<L>;
   using E = typename WordOps<ST>::E;
-  const int py = rc.yi + g.hy, pz = rc.zi + g.hz;
+  const int py = yi + g.hy, pz = zi + g.hz;
   static_for<0, Pl::NOPS>([&](auto O) {
     constexpr int o = decltype(O)::value;
     constexpr RowOp op = Pl::ops[o];
@@ -290,9 +295,10 @@ __device__ __forceinline__ void rows_copy(const Geo& g, const RowMaps<L>& maps, 
       if (rz < 0) rz += g.nz; else if (rz >= g.sz) rz -= g.nz;
     }
     const int q = op.q0 + op.sgn * P;
+    const int chunk = (rz * g.sy + ry) * g.nch;
     const uint32_t dst = stage + (uint32_t)(RowSlots<L>::base_of(o, LW) * (int)sizeof(E));
-    if constexpr (LOAD) tma_load_box(dst, &maps.m[op.map], q, row_chunk(g, ry, rz), bar);
-    else tma_store_box(&maps.m[op.map], q, row_chunk(g, ry, rz), dst);
+    if constexpr (LOAD) tma_load_box(dst, &maps->m[op.map], q, chunk, bar);
+    else tma_store_box(&maps->m[op.map], q, chunk, dst);
   });
   if constexpr (!LOAD) bulk_commit();
 }
@@ -391,60 +397,70 @@ __device__ __forceinline__ void rows_body(const StepArgs& a, const RowMaps<L>& m
   if (k == nch) {
     if (lane != 0) return;
     const int rbytes = Cfg::row_bytes(nch);
-    // one row's copies: the lattice's geometry, maps and parity, the row
-    auto copy_row = [&](auto LOAD, const RowCursor& rc, int item, int s) {
-      const uint32_t st = stage0 + s * Cfg::STAGE_BYTES;
-      const uint32_t bar = decltype(LOAD)::value ? full0 + 8 * s : 0;
-      if constexpr (BATCH) {
-        const RowItem<L>& it = items[item];
-        rows_copy<L, ST, LW, decltype(LOAD)::value>(it.a.g, it.maps, (int)((it.t0 + step) & 1),
-                                                     rc, st, bar);
-      } else {
-        rows_copy<L, ST, LW, decltype(LOAD)::value>(g, maps, a.parity, rc, st, bar);
-      }
+    // A row in a stage: its lattice's copy geometry, maps and parity, its
+    // (y, z) there, and (BATCH) its item, -1 for a lattice sitting out.
+    struct Held {
+      RowGeo g;
+      const RowMaps<L>* maps;
+      int parity, yi, zi, item;
     };
-    // the item of global row r and its (y, z) there (BATCH), from a search
-    // of the items' first rows
-    auto locate = [&](long long r, RowCursor& rc) {
-      int lo = 0, hi = n_items - 1;
-      while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (items[mid].first_row <= r) lo = mid; else hi = mid - 1;
-      }
-      const long long local = r - items[lo].first_row;
-      const int ny = items[lo].a.g.ny;
-      rc.r = r;
-      rc.yi = (int)(local % ny);
-      rc.zi = (int)(local / ny);
-      return lo;
-    };
-    RowCursor ld = cur;       // next row to load
-    RowCursor held[NS];       // the rows in the stages (BATCH: with their items)
-    int held_item[NS];
-    int nl = 0, nst = 0;      // rows loaded, rows stored
+    Held held[NS];
+    // BATCH: the lattice the load cursor is in, cached while consecutive rows
+    // of this CTA (gridDim.x apart) stay in it: its rows [c_first, c_end),
+    // copy geometry, parity, whether it steps, and the cursor's (y, z) with
+    // the grid stride's (y, z) parts for an incremental advance
+    int c_item = -1, c_yi = 0, c_zi = 0, c_dy = 0, c_dz = 0, c_par = 0;
+    long long c_first = 0, c_end = 0;
+    bool c_live = true;
+    RowGeo c_g = RowGeo::of(g);
+    RowCursor ld = cur;  // next row to load
+    int nl = 0, nst = 0;  // rows loaded, rows stored
     bool failed = false;
     auto load_next = [&](int s) {
-      int item = 0;
+      Held& h = held[s];
       bool live = true;
       if constexpr (BATCH) {
-        item = locate(ld.r, held[s]);
+        const long long r = ld.r;
+        if (c_item >= 0 && r >= c_first && r < c_end) {
+          c_yi += c_dy;
+          if (c_yi >= c_g.ny) { c_yi -= c_g.ny; ++c_zi; }
+          c_zi += c_dz;
+        } else {
+          int lo = 0, hi = n_items - 1;  // last item with first_row <= r
+          while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (items[mid].first_row <= r) lo = mid; else hi = mid - 1;
+          }
+          const RowItem<L>& it = items[lo];
+          c_item = lo;
+          c_g = RowGeo::of(it.a.g);
+          c_first = it.first_row;
+          c_end = c_first + (long long)c_g.ny * c_g.nz;
+          c_par = (int)((it.t0 + step) & 1);
+          c_live = it.t0 + step < it.t_end;
+          const long long local = r - c_first;
+          c_yi = (int)(local % c_g.ny);
+          c_zi = (int)(local / c_g.ny);
+          c_dy = (int)(gridDim.x % (unsigned)c_g.ny);
+          c_dz = (int)(gridDim.x / (unsigned)c_g.ny);
+        }
         // a lattice that has done its steps sits this step out: its row is
         // neither loaded nor stored, the update warps see item -1
-        live = items[item].t0 + step < items[item].t_end;
-        if (!live) item = -1;
-        meta[s] = item;  // published to the update warps by the arrival below
+        live = c_live;
+        h = Held{c_g, &items[c_item].maps, c_par, c_yi, c_zi, live ? c_item : -1};
+        meta[s] = h.item;  // published to the update warps by the arrival below
+        ld.r += gridDim.x;
       } else {
-        held[s] = ld;
+        h = Held{RowGeo::of(g), &maps, a.parity, ld.yi, ld.zi, 0};
+        ld.advance(gridDim.x, dyr, dzr, g.ny);
       }
-      held_item[s] = item;
       if (live) {
         mbar_expect_tx(full0 + 8 * s, rbytes);
-        copy_row(IC<1>{}, held[s], item, s);
+        rows_copy<L, ST, LW, true>(h.g, h.maps, h.parity, h.yi, h.zi,
+                                   stage0 + s * Cfg::STAGE_BYTES, full0 + 8 * s);
       } else {
         mbar_arrive(full0 + 8 * s);
       }
-      if constexpr (BATCH) ld.r += gridDim.x;
-      else ld.advance(gridDim.x, dyr, dzr, g.ny);
       ++nl;
     };
     while (nl < NS && ld.r < nrows) load_next(nl);
@@ -454,7 +470,10 @@ __device__ __forceinline__ void rows_body(const StepArgs& a, const RowMaps<L>& m
         failed = true;
         break;
       }
-      if (held_item[s] >= 0) copy_row(IC<0>{}, held[s], held_item[s], s);
+      const Held& h = held[s];
+      if (h.item >= 0)
+        rows_copy<L, ST, LW, false>(h.g, h.maps, h.parity, h.yi, h.zi,
+                                    stage0 + s * Cfg::STAGE_BYTES, 0);
       ++nst;
       if (ld.r < nrows) {
         bulk_wait_read<0>();  // the stores no longer read the stage

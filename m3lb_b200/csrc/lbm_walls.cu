@@ -4,6 +4,7 @@
 
 #include <algorithm>
 #include <cstdio>
+#include <cstring>
 #include <numeric>
 
 #include "../../include/m3lb.h"
@@ -36,10 +37,11 @@ inline bool is_wall(uint8_t f) { return f == kRegWall || f == kSpecWall || f == 
 
 void WallSet::release() {
   cudaFree(nodes);
+  cudaFree(heads);
   cudaFree(wall_rho);
   cudaFree(snap);
   cudaFree(spec);
-  nodes = nullptr; wall_rho = nullptr; snap = nullptr; spec = nullptr;
+  nodes = nullptr; heads = nullptr; wall_rho = nullptr; snap = nullptr; spec = nullptr;
   count = 0; nsnap = 0;
 }
 
@@ -153,6 +155,7 @@ int WallSet::set_regularized(const Geo& g, int lattice, std::vector<uint8_t>& fl
 BoundArgs WallSet::args(int begin, int end) const {
   BoundArgs b{};
   b.nodes = nodes;
+  b.heads = heads;
   b.begin = begin;
   b.end = end;
   b.wall_rho = wall_rho;
@@ -303,7 +306,25 @@ int WallSet::build(const Geo& g, int lattice, int op, int storage, const std::ve
     if (flags[n] == kSpecWall && !spec_nrm.empty()) sp[n] = spec_nrm[n];
     if (flags[n] == kSpecNode && !spec_faces.empty()) sp[n] = spec_faces[n];
   }
+  std::vector<BHead> hd(sorted.size());
+  for (size_t p = 0; p < sorted.size(); ++p) {
+    const BNode& b = sorted[p];
+    BHead& h = hd[p];
+    h.n = b.n;
+    h.unk = b.unk;
+    h.type = b.type;
+    h.code = b.code;
+    h.moving = 0;
+    h.pad = 0;
+    for (int a = 0; a < 3; ++a) {
+      uint64_t u, v;
+      std::memcpy(&u, &b.u[a], 8);
+      std::memcpy(&v, &b.un[a], 8);
+      if (u | v) h.moving = 1;
+    }
+  }
   if (cudaMalloc((void**)&nodes, sizeof(BNode) * count) != cudaSuccess ||
+      cudaMalloc((void**)&heads, sizeof(BHead) * count) != cudaSuccess ||
       cudaMalloc(&wall_rho, rb * count) != cudaSuccess ||
       (nsnap && cudaMalloc(&snap, rb * (size_t)nsnap * (lattice == 9 ? 9 : 27)) != cudaSuccess) ||
       cudaMalloc((void**)&spec, (size_t)g.n_padded) != cudaSuccess) {
@@ -311,6 +332,8 @@ int WallSet::build(const Geo& g, int lattice, int op, int storage, const std::ve
     return werr(M3LB_ERR_MEMORY, "walls: cannot allocate the wall-node list");
   }
   cudaError_t e = cudaMemcpyAsync(nodes, sorted.data(), sizeof(BNode) * count, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(heads, hd.data(), sizeof(BHead) * count, cudaMemcpyHostToDevice, s);
   if (e == cudaSuccess) e = cudaMemsetAsync(wall_rho, 0, rb * count, s);
   if (e == cudaSuccess) e = cudaMemcpyAsync(spec, sp.data(), sp.size(), cudaMemcpyHostToDevice, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);

@@ -36,6 +36,7 @@ class WallSet {
 
   // ---- device list (rebuilt by build())
   BNode* nodes = nullptr;
+  BHead* heads = nullptr;     // the hot fields of `nodes`, one per list node
   void* wall_rho = nullptr;   // arithmetic type, one per list node
   void* snap = nullptr;       // arithmetic type, Q per snapshot slot
   uint8_t* spec = nullptr;    // per padded node: SpecWall code / SpecNode mask
