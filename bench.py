@@ -264,6 +264,10 @@ def gpu_arm(args, rank, world, dist):
         "clocks": clocks,
         "state_finite": finite,
     }
+    if isinstance(clocks, dict) and clocks.get("sm_mhz"):
+        # the step time in clock cycles (ms x MHz): constant across boxes
+        # and power states when the kernel is bound by instruction issue
+        clocks["ms_x_sm_mhz"] = round(t16 / args.steps * 1e3 * clocks["sm_mhz"], 1)
     if mass_drift is not None:
         out["mass_drift"] = mass_drift
     if other16:

@@ -127,6 +127,7 @@ struct m3lb_solver {
   void* f = nullptr;                 // populations
   size_t f_bytes = 0;
   uint8_t* flags = nullptr;          // per padded node
+  uint8_t* row_flags = nullptr;      // per padded row: any interior node not fluid
   std::vector<uint8_t> flags_host;   // per padded node
   bool has_geometry = false;
   // wall nodes (regularised and free-slip) and their device list
@@ -155,6 +156,7 @@ struct m3lb_solver {
     a.g = g;
     a.f = f;
     a.flags = has_geometry ? flags : nullptr;
+    a.row_flags = has_geometry ? row_flags : nullptr;
     a.spec = walls.count ? walls.spec : nullptr;
     a.parity = (int)(t & 1);
     a.omega = omega; a.omega2 = omega2;
@@ -238,7 +240,8 @@ int m3lb_create(int lattice, int nx, int ny, int nz, int px, int py, int pz, int
   h->f_bytes = pop_elems(h->g, lattice) * elem_bytes(storage);
   if (cudaMalloc(&h->f, h->f_bytes) != cudaSuccess)
     return cleanup(fail(M3LB_ERR_MEMORY, "create: cannot allocate %zu bytes of populations", h->f_bytes));
-  if (cudaMalloc((void**)&h->flags, (size_t)h->g.n_padded) != cudaSuccess)
+  if (cudaMalloc((void**)&h->flags, (size_t)h->g.n_padded) != cudaSuccess ||
+      cudaMalloc((void**)&h->row_flags, (size_t)h->g.sy * h->g.sz) != cudaSuccess)
     return cleanup(fail(M3LB_ERR_MEMORY, "create: cannot allocate flags"));
   const size_t mb = (size_t)h->n_interior() * real_bytes(storage);
   for (int i = 0; i < 4; ++i)
@@ -286,6 +289,7 @@ int m3lb_destroy(m3lb_solver* h) {
   cudaDeviceSynchronize();
   cudaFree(h->f);
   cudaFree(h->flags);
+  cudaFree(h->row_flags);
   cudaFree(h->temp_own);
   h->walls.release();
   for (void* p : h->macro) cudaFree(p);
@@ -304,17 +308,26 @@ int m3lb_set_params(m3lb_solver* h, double omega, double omega2, double fx, doub
 
 }  // extern "C"
 
-// Upload the host flags and rebuild the wall-node list.
+// Upload the host flags, with the per-row summary the row kernel reads to
+// skip the flag loads of rows that are all fluid, and rebuild the wall-node
+// list.
 static int upload_geometry(m3lb_solver* h) {
   const Geo& g = h->g;
   bool any = false;
+  std::vector<uint8_t> rows((size_t)g.sy * g.sz, 0);
   for (int z = 0; z < g.nz; ++z)
-    for (int y = 0; y < g.ny; ++y)
-      for (int x = 0; x < g.nx; ++x)
-        any |= h->flags_host[((size_t)(z + g.hz) * g.sy + (y + g.hy)) * g.sx + (x + g.hx)] != 0;
+    for (int y = 0; y < g.ny; ++y) {
+      const size_t r = (size_t)(z + g.hz) * g.sy + (y + g.hy);
+      bool row = false;
+      for (int x = 0; x < g.nx; ++x) row |= h->flags_host[r * g.sx + (x + g.hx)] != 0;
+      rows[r] = row ? 1 : 0;
+      any |= row;
+    }
   DeviceGuard dg(h->device);
   CUDA_TRY(cudaMemcpyAsync(h->flags, h->flags_host.data(), (size_t)g.n_padded,
                            cudaMemcpyHostToDevice, h->stream));
+  CUDA_TRY(cudaMemcpyAsync(h->row_flags, rows.data(), rows.size(), cudaMemcpyHostToDevice,
+                           h->stream));
   CUDA_TRY(cudaStreamSynchronize(h->stream));
   h->has_geometry = any;
   return h->walls.build(g, h->lattice, h->op, h->storage, h->flags_host, h->stream);

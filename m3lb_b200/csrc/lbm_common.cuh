@@ -310,6 +310,8 @@ struct StepArgs {
   Geo g;
   void* f;                 // populations
   const uint8_t* flags;    // per padded node (0 fluid); nullptr: all interior fluid
+  const uint8_t* row_flags;  // per padded row (pz * sy + py): 1 when a node of the row
+                             // is not fluid; nullptr: test every row's flags
   const uint8_t* spec;     // per padded node: SpecWall normal code / SpecNode face mask;
                            // nullptr: no wall nodes (flags 3, 4 and 5 then act as solid)
   void* rho;               // macroscopic outputs, per padded node, or nullptr

@@ -341,6 +341,10 @@ constexpr int rows_min_blocks() {
 // after which the copy warp stores the row, waits until the stores have
 // read the stage, and loads row j + kRowsStages into it.
 //
+// A lattice with cell flags: the copy warp also records in the stage's slot
+// of `meta` whether the row has a non-fluid node (the per-row summary
+// row_flags), and the update warps load the flags of those rows only.
+//
 // BATCH: the rows of many lattices of one operator and one row width (the
 // serving loop): global row r belongs to the item whose range holds it
 // (items sorted by first_row), each item carrying its own step arguments,
@@ -374,7 +378,7 @@ __device__ __forceinline__ void rows_body(const StepArgs& a, const RowMaps<L>& m
   const long long nrows = BATCH ? batch_rows : (long long)g.ny * g.nz;
   uint64_t* bars = reinterpret_cast<uint64_t*>(rows_smem + NS * Cfg::STAGE_BYTES);
   int* abort_flag = reinterpret_cast<int*>(bars + 2 * NS);
-  int* meta = abort_flag + 1;  // BATCH: the item of each stage's row
+  int* meta = abort_flag + 1;  // per stage: BATCH the row's item, else whether it has flags
   const uint32_t stage0 = smem_addr(rows_smem);
   const uint32_t full0 = smem_addr(bars), empty0 = full0 + 8 * NS;
   const int dyr = (int)(gridDim.x % g.ny), dzr = (int)(gridDim.x / g.ny);
@@ -415,6 +419,13 @@ __device__ __forceinline__ void rows_body(const StepArgs& a, const RowMaps<L>& m
     RowGeo c_g = RowGeo::of(g);
     RowCursor ld = cur;  // next row to load
     int nl = 0, nst = 0;  // rows loaded, rows stored
+    // with cell flags: the flag summary of row `ld`, read one row ahead so
+    // the global load's latency passes while the copy thread waits
+    auto row_flag = [&]() -> int {
+      if (BATCH || !a.flags || ld.r >= nrows) return 0;
+      return a.row_flags ? a.row_flags[(ld.zi + g.hz) * g.sy + (ld.yi + g.hy)] : 1;
+    };
+    int ld_flag = row_flag();
     bool failed = false;
     auto load_next = [&](int s) {
       Held& h = held[s];
@@ -452,7 +463,11 @@ __device__ __forceinline__ void rows_body(const StepArgs& a, const RowMaps<L>& m
         ld.r += gridDim.x;
       } else {
         h = Held{RowGeo::of(g), &maps, a.parity, ld.yi, ld.zi, 0};
+        // whether the update warps load the row's flags (published, as in a
+        // batch, by the barrier arrival below)
+        meta[s] = ld_flag;
         ld.advance(gridDim.x, dyr, dzr, g.ny);
+        ld_flag = row_flag();
       }
       if (live) {
         mbar_expect_tx(full0 + 8 * s, rbytes);
@@ -573,7 +588,7 @@ __device__ __forceinline__ void rows_body(const StepArgs& a, const RowMaps<L>& m
     });
 
     bool solid0 = !lane_ok, solid1 = !lane_ok;
-    if (!BATCH && a.flags) {
+    if (!BATCH && a.flags && meta[s]) {
       const uint16_t fl = *reinterpret_cast<const uint16_t*>(
           a.flags + ((long long)(cur.zi + g.hz) * g.sy + (cur.yi + g.hy)) * g.sx + x0);
       solid0 = solid0 || (fl & 0xffu) != 0;

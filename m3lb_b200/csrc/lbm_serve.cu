@@ -253,6 +253,11 @@ struct m3lb_server {
   unsigned row_mask = 0, prev_row_mask = ~0u;
   int prev_row_R = -1;
   std::vector<RowGraph> rgraphs;
+  // one stream per group of a round (its steps depend only on each other),
+  // forked from and joined back to `stream`
+  std::vector<cudaStream_t> row_streams;
+  std::vector<cudaEvent_t> row_joins;
+  cudaEvent_t row_fork = nullptr;
   std::vector<cudaEvent_t> free_timing;
   double* red_slots = nullptr;      // pinned, kReduceVals per request of a run
   int red_cap = 0;
@@ -623,14 +628,43 @@ void build_row_items(m3lb_server* s) {
   }
 }
 
+// The groups' lattices are disjoint, so a group's R steps depend only on
+// each other: with several groups each runs on its own stream (forked from
+// the server stream after the tables' upload, joined back before the
+// round's readouts), so one group's launch tail overlaps the others' work.
+int ensure_row_streams(m3lb_server* s, int groups) {
+  if (groups < 2) return M3LB_OK;
+  if (!s->row_fork) SRV_TRY(cudaEventCreateWithFlags(&s->row_fork, cudaEventDisableTiming));
+  while ((int)s->row_streams.size() < groups) {
+    cudaStream_t st = nullptr;
+    cudaEvent_t e = nullptr;
+    SRV_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    s->row_streams.push_back(st);
+    SRV_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    s->row_joins.push_back(e);
+  }
+  return M3LB_OK;
+}
+
+// (the streams and events exist: ensure_row_streams ran before any capture)
 int launch_rows_round(m3lb_server* s, int R) {
   const Launchers* T = table_for(27, s->cfg.storage);
-  for (int step = 0; step < R; ++step)
-    for (int g = 0; g < kRowGroups; ++g) {
-      if (!(s->row_mask >> g & 1u)) continue;
+  const int groups = __builtin_popcount(s->row_mask);
+  if (groups > 1) SRV_TRY(cudaEventRecord(s->row_fork, s->stream));
+  int lane = 0;
+  for (int g = 0; g < kRowGroups; ++g) {
+    if (!(s->row_mask >> g & 1u)) continue;
+    cudaStream_t st = groups > 1 ? s->row_streams[lane] : s->stream;
+    if (groups > 1) SRV_TRY(cudaStreamWaitEvent(st, s->row_fork, 0));
+    for (int step = 0; step < R; ++step)
       SRV_TRY(T->batch_rows(s->ritems_dev, s->rdesc_dev + g, kOps[g / kRowsMaxChunks],
-                            g % kRowsMaxChunks + 1, step, s->stream));
+                            g % kRowsMaxChunks + 1, step, st));
+    if (groups > 1) {
+      SRV_TRY(cudaEventRecord(s->row_joins[lane], st));
+      SRV_TRY(cudaStreamWaitEvent(s->stream, s->row_joins[lane], 0));
     }
+    ++lane;
+  }
   return M3LB_OK;
 }
 
@@ -647,6 +681,10 @@ int run_round_rows(m3lb_server* s, int R) {
                             n * sizeof(RowItem27), cudaMemcpyHostToDevice, s->stream));
   SRV_TRY(cudaMemcpyAsync(s->rdesc_dev, s->rdesc_host + (size_t)s->flip * kRowGroups,
                           kRowGroups * sizeof(RowBatch), cudaMemcpyHostToDevice, s->stream));
+  {
+    const int rc = ensure_row_streams(s, __builtin_popcount(s->row_mask));
+    if (rc) return rc;
+  }
   RowGraph* hit = nullptr;
   for (RowGraph& g : s->rgraphs)
     if (g.mask == s->row_mask && g.R == R) hit = &g;
@@ -923,6 +961,12 @@ int m3lb_serve_destroy(m3lb_server* s) {
   }
   for (cudaEvent_t e : s->free_events) cudaEventDestroy(e);
   for (cudaEvent_t e : s->free_timing) cudaEventDestroy(e);
+  for (cudaStream_t st : s->row_streams) {
+    cudaStreamSynchronize(st);
+    cudaStreamDestroy(st);
+  }
+  for (cudaEvent_t e : s->row_joins) cudaEventDestroy(e);
+  if (s->row_fork) cudaEventDestroy(s->row_fork);
   if (s->stream) cudaStreamDestroy(s->stream);
   delete s;
   return M3LB_OK;
