@@ -179,8 +179,8 @@ struct m3lb_solver {
     const bool rows32 = (long long)g.nch * Q * 64 < (1LL << 31);
     // the row kernel: whole rows of at most 8 chunks with 16-bit storage, 4
     // with 32- or 64-bit storage (the last chunk may be partial), in stages
-    // of 2, 4 or 8 chunks that must fit a CTA's shared memory
-    const int lw = g.nch <= 2 ? 2 : (g.nch <= 4 ? 4 : 8);
+    // of 2, 3, 4 or 8 chunks that must fit a CTA's shared memory
+    const int lw = g.nch <= 2 ? 2 : (g.nch == 3 ? 3 : (g.nch <= 4 ? 4 : 8));
     const bool rows_ok = g.nch <= (elem_bytes(storage) == 2 ? 8 : 4) &&
                          4LL * Q * lw * 64 * elem_bytes(storage) + 84 <= 227LL * 1024;
     if (kernel == M3LB_KERNEL_ROWS && rows_ok) return kKernelRows;

@@ -99,18 +99,20 @@ cudaError_t rows_maps(const StepArgs& a, RowMaps<L>* maps) {
   return cudaSuccess;
 }
 
-// Persistent row kernel: one CTA of nch update warps and one copy warp per
-// row, stages of LW chunks (the smallest of 2, 4, 8 that holds the row), as
-// many CTAs as are resident (occupancy queried once per device and shape).
+// Persistent row kernel: one CTA of nch update warps per row (and, for rows
+// of 3 chunks or more, one copy warp), stages of LW chunks (the smallest of
+// 2, 3, 4, 8 that holds the row), as many CTAs as are resident (occupancy
+// queried once per device and shape).
 template <int OP, int EQ, bool SH, bool FORCE, int LW>
 cudaError_t launch_rows_lw(const StepArgs& a, cudaStream_t s) {
-  using Cfg = RowsCfg<L, ST, LW>;
+  constexpr bool CW = LW != 2;
+  using Cfg = RowsCfg<L, ST, LW, rows_stages<CW>()>;
   if constexpr (Cfg::SMEM > kRowsSmemMax) {
     return cudaErrorInvalidValue;
   } else {
     const Geo& g = a.g;
-    auto kern = step_rows<L, ST, OP, EQ, SH, FORCE, LW>;
-    const int threads = (g.nch + 1) * 32;
+    auto kern = step_rows<L, ST, OP, EQ, SH, FORCE, LW, CW>;
+    const int threads = (g.nch + (CW ? 1 : 0)) * 32;
     constexpr int kMaxDev = 64;
     static int cached[kMaxDev][LW + 1];
     int dev = 0;
@@ -143,6 +145,7 @@ cudaError_t launch_rows(const StepArgs& a, cudaStream_t s) {
   if (g.nch < 1 || g.nch > kRowsMaxChunks || (g.nx % 2) != 0) return cudaErrorInvalidValue;
   switch (rows_lw(g.nch)) {
     case 2: return launch_rows_lw<OP, EQ, SH, FORCE, 2>(a, s);
+    case 3: return launch_rows_lw<OP, EQ, SH, FORCE, 3>(a, s);
     case 4: return launch_rows_lw<OP, EQ, SH, FORCE, 4>(a, s);
     default:
       // 8-chunk stages hold 16-bit rows only (FP32 fits one CTA per SM,
@@ -315,12 +318,13 @@ cudaError_t row_maps(const StepArgs& a, void* maps, size_t bytes) {
 template <int OP, int LW>
 cudaError_t launch_batch_rows(const void* items, const void* desc, int nch, int step,
                               cudaStream_t s) {
-  using Cfg = RowsCfg<L, ST, LW>;
+  constexpr bool CW = LW != 2;
+  using Cfg = RowsCfg<L, ST, LW, rows_stages<CW>()>;
   if constexpr (Cfg::SMEM > kRowsSmemMax || sizeof(typename WordOps<ST>::E) != 2) {
     return cudaErrorNotSupported;
   } else {
     auto kern = batch_rows<L, ST, OP, 0, LW>;
-    const int threads = (nch + 1) * 32;
+    const int threads = (nch + (CW ? 1 : 0)) * 32;
     constexpr int kMaxDev = 64;
     static int cached[kMaxDev][LW + 1];
     int dev = 0;
@@ -348,6 +352,7 @@ cudaError_t batch_rows_op(const void* items, const void* desc, int nch, int step
   if (nch < 1 || nch > kRowsMaxChunks) return cudaErrorInvalidValue;
   switch (rows_lw(nch)) {
     case 2: return launch_batch_rows<OP, 2>(items, desc, nch, step, s);
+    case 3: return launch_batch_rows<OP, 3>(items, desc, nch, step, s);
     case 4: return launch_batch_rows<OP, 4>(items, desc, nch, step, s);
     default: return launch_batch_rows<OP, 8>(items, desc, nch, step, s);
   }

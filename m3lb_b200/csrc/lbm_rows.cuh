@@ -169,19 +169,61 @@ struct RowBatch {
   long long n_rows;
 };
 
-// Shared memory of a CTA: kRowsStages stages of Q lines of LW chunks, then
-// the barriers (full[s]: the stage's loads landed; empty[s]: every update
-// warp is done with the stage's row), the abort flag and, for batched
-// launches, the item of each stage's row.
-template <class L, int ST, int LW>
+// Interior row cursor: row r = (yi, zi), advanced by the grid's CTA count.
+struct RowCursor {
+  long long r;
+  int yi, zi;
+  __device__ __forceinline__ void start(long long r0, int ny) {
+    r = r0;
+    yi = (int)(r0 % ny);
+    zi = (int)(r0 / ny);
+  }
+  __device__ __forceinline__ void advance(long long dr, int dy, int dz, int ny) {
+    r += dr;
+    yi += dy;
+    if (yi >= ny) { yi -= ny; ++zi; }
+    zi += dz;
+  }
+};
+
+// What the copies of a row need of its lattice, held in registers (read
+// through a pointer into global memory, the fields would be reloaded after
+// every copy, each of which clobbers memory).
+struct RowGeo {
+  int ny, nz, sy, sz, hy, hz, nch;
+  __device__ __forceinline__ static RowGeo of(const Geo& g) {
+    return RowGeo{g.ny, g.nz, g.sy, g.sz, g.hy, g.hz, g.nch};
+  }
+};
+
+// A row in a stage: its lattice's copy geometry, maps and parity, its (y, z)
+// there, and (batched launches) its item, -1 for a lattice sitting out.
+template <class L>
+struct RowHeld {
+  RowGeo g;
+  const RowMaps<L>* maps;
+  int parity, yi, zi, item;
+};
+
+// Shared memory of a CTA: NS stages of Q lines of LW chunks, then the
+// barriers (full[s]: the stage's loads landed; empty[s]: every update warp
+// is done with the stage's row), the abort flag, per stage the row's item
+// (batched launches) or whether it has a non-fluid node, and per stage the
+// RowHeld of its row.  Without a copy warp the empty barriers' words hold,
+// per stage, the count of update warps done with the row and the count of
+// loads issued into it.
+template <class L, int ST, int LW, int NS = kRowsStages>
 struct RowsCfg {
   using E = typename WordOps<ST>::E;
   static constexpr int STAGE_BYTES = L::Q * LW * kChunk * (int)sizeof(E);
-  static constexpr int SMEM = kRowsStages * STAGE_BYTES + 2 * kRowsStages * 8 + 4 + 4 * kRowsStages;
+  static constexpr int HELD_OFF = (NS * STAGE_BYTES + 2 * NS * 8 + 4 + 4 * NS + 15) / 16 * 16;
+  static constexpr int SMEM = HELD_OFF + NS * (int)sizeof(RowHeld<L>);
   static __host__ __device__ int row_bytes(int nch) { return L::Q * nch * kChunk * (int)sizeof(E); }
 };
-// Line width (chunks per stage line) for a row of nch chunks.
-__host__ __device__ constexpr int rows_lw(int nch) { return nch <= 2 ? 2 : (nch <= 4 ? 4 : 8); }
+// Line width (chunks per stage line) for a row of nch chunks: 2, 3, 4 or 8.
+__host__ __device__ constexpr int rows_lw(int nch) {
+  return nch <= 2 ? 2 : (nch == 3 ? 3 : (nch <= 4 ? 4 : 8));
+}
 
 // ------------------------------------------------------------- primitives
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
@@ -248,33 +290,6 @@ __device__ __forceinline__ void fence_async_smem() {
   asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
 }
 
-// Interior row cursor: row r = (yi, zi), advanced by the grid's CTA count.
-struct RowCursor {
-  long long r;
-  int yi, zi;
-  __device__ __forceinline__ void start(long long r0, int ny) {
-    r = r0;
-    yi = (int)(r0 % ny);
-    zi = (int)(r0 / ny);
-  }
-  __device__ __forceinline__ void advance(long long dr, int dy, int dz, int ny) {
-    r += dr;
-    yi += dy;
-    if (yi >= ny) { yi -= ny; ++zi; }
-    zi += dz;
-  }
-};
-
-// What the copies of a row need of its lattice, held in registers (read
-// through a pointer into global memory, the fields would be reloaded after
-// every copy, each of which clobbers memory).
-struct RowGeo {
-  int ny, nz, sy, sz, hy, hz, nch;
-  __device__ __forceinline__ static RowGeo of(const Geo& g) {
-    return RowGeo{g.ny, g.nz, g.sy, g.sz, g.hy, g.hz, g.nch};
-  }
-};
-
 // The copies of one row (interior row yi, zi) by the calling thread.  LOAD:
 // global -> stage (completion on `bar`, whose expected bytes the caller has
 // set); else stage -> global, in one bulk group of this thread.
@@ -321,39 +336,142 @@ __device__ __forceinline__ bool rows_wait(uint32_t bar, int parity, long long li
   return false;
 }
 
-// Resident CTAs per SM the launch bounds ask for: the moment operators fit
-// their registers at the occupancy the stage size allows (16-bit storage,
-// LW 2: 8 CTAs of 27.6 KB fit, registers allow 6; LW 4: 4 CTAs of 55 KB;
-// LW 8: 2 of 110 KB); BGK/TRT keep more values live (as in the paired
-// kernel) and take their registers at fewer resident CTAs.
-template <int OP, int ST, int LW>
+// Resident CTAs per SM the launch bounds ask for.  With a copy warp (rows of
+// 3 to 8 chunks, and the batched kernel): the moment operators fit their
+// registers at the occupancy the stage size allows (16-bit storage, LW 2: 8
+// CTAs of 27.6 KB fit, registers allow 6; LW 3: 5 CTAs of 41.5 KB; LW 4: 4
+// CTAs of 55 KB; LW 8: 2 of 110 KB); BGK/TRT keep more values live (as in
+// the paired kernel) and take their registers at fewer resident CTAs.  Without a copy warp (the
+// single-lattice kernel's rows of up to 4 chunks, 3 stages): 16-bit LW 4
+// stages of 41.5 KB fit 5 CTAs of 4 warps, LW 2 stages of 20.8 KB 10 CTAs of
+// 2 warps, both at up to 96 registers.
+template <int OP, int ST, int LW, bool CW = true>
 constexpr int rows_min_blocks() {
   if (ST == kF64) return 1;
-  if (OP == 1 || OP == 2) return LW == 2 ? 4 : (LW == 4 ? 2 : 1);
-  if (ST == kF32) return LW == 2 ? 2 : 1;
-  return LW == 2 ? 6 : (LW == 4 ? 4 : 2);
+  if (!CW) {
+    if (ST == kF32) return LW == 2 ? 5 : 2;
+    if (OP == 1 || OP == 2) return LW == 2 ? 6 : 3;
+    return LW == 2 ? 10 : 5;
+  }
+  if (OP == 1 || OP == 2) return LW == 2 ? 4 : (LW == 3 ? 3 : (LW == 4 ? 2 : 1));
+  if (ST == kF32) return LW <= 3 ? 2 : 1;
+  return LW == 2 ? 6 : (LW == 3 ? 5 : (LW == 4 ? 4 : 2));
 }
+// Stages of the ring: 4 with a copy warp, 3 without (the warp that finishes
+// a row last moves it, so a stage is busy only while its row is stored and
+// the next one loads).
+template <bool CW>
+__host__ __device__ constexpr int rows_stages() { return CW ? kRowsStages : 3; }
 
-// One CTA: warps 0 .. nch-1 update chunk k of each of the CTA's rows, warp
-// nch (lane 0) moves them.  Row j of the CTA sits in stage j % kRowsStages;
-// its load completes phase (j / kRowsStages) & 1 of full[s], and the update
-// warps' arrivals on empty[s] (one per warp) complete the same phase there,
-// after which the copy warp stores the row, waits until the stores have
-// read the stage, and loads row j + kRowsStages into it.
+// The rows a CTA loads, in order (row j of the CTA at its j-th call of
+// next()).  BATCH: global row r belongs to the item whose row range holds
+// it; the lattice the cursor is in is cached while consecutive rows of the
+// CTA (gridDim.x apart) stay in it: its rows [c_first, c_end), copy
+// geometry, parity, whether it steps, and the cursor's (y, z) with the grid
+// stride's (y, z) parts for an incremental advance.  The item table is
+// searched only when the cursor leaves the lattice.
+template <class L, bool BATCH>
+struct RowLoader {
+  RowCursor ld;  // next row to load
+  int c_item, c_yi, c_zi, c_dy, c_dz, c_par;
+  long long c_first, c_end;
+  bool c_live;
+  RowGeo c_g;
+  int flag;  // with cell flags: the summary of row ld, read one row ahead
+  __device__ __forceinline__ static int row_flag(const StepArgs& a, const RowCursor& c,
+                                                 long long nrows) {
+    if (BATCH || !a.flags || c.r >= nrows) return 0;
+    const Geo& g = a.g;
+    return a.row_flags ? a.row_flags[(c.zi + g.hz) * g.sy + (c.yi + g.hy)] : 1;
+  }
+  __device__ __forceinline__ void init(const RowCursor& start, const StepArgs& a, long long nrows) {
+    const Geo& g = a.g;
+    ld = start;
+    flag = row_flag(a, ld, nrows);
+    c_item = -1;
+    c_yi = c_zi = c_dy = c_dz = c_par = 0;
+    c_first = c_end = 0;
+    c_live = true;
+    c_g = RowGeo::of(g);
+  }
+  // The RowHeld of row ld (which the caller has checked is < nrows); ld
+  // moves to the CTA's next row.
+  __device__ __forceinline__ RowHeld<L> next(const StepArgs& a, const RowMaps<L>& maps,
+                                             const RowItem<L>* __restrict__ items, int n_items,
+                                             int step, int dyr, int dzr, long long nrows) {
+    if constexpr (BATCH) {
+      const long long r = ld.r;
+      if (c_item >= 0 && r >= c_first && r < c_end) {
+        c_yi += c_dy;
+        if (c_yi >= c_g.ny) { c_yi -= c_g.ny; ++c_zi; }
+        c_zi += c_dz;
+      } else {
+        int lo = 0, hi = n_items - 1;  // last item with first_row <= r
+        while (lo < hi) {
+          const int mid = (lo + hi + 1) >> 1;
+          if (items[mid].first_row <= r) lo = mid; else hi = mid - 1;
+        }
+        const RowItem<L>& it = items[lo];
+        c_item = lo;
+        c_g = RowGeo::of(it.a.g);
+        c_first = it.first_row;
+        c_end = c_first + (long long)c_g.ny * c_g.nz;
+        c_par = (int)((it.t0 + step) & 1);
+        c_live = it.t0 + step < it.t_end;
+        const long long local = r - c_first;
+        c_yi = (int)(local % c_g.ny);
+        c_zi = (int)(local / c_g.ny);
+        c_dy = (int)(gridDim.x % (unsigned)c_g.ny);
+        c_dz = (int)(gridDim.x / (unsigned)c_g.ny);
+      }
+      ld.r += gridDim.x;
+      // a lattice that has done its steps sits this step out: its row is
+      // neither loaded nor stored, the update warps see item -1
+      return RowHeld<L>{c_g, &items[c_item].maps, c_par, c_yi, c_zi, c_live ? c_item : -1};
+    } else {
+      const RowHeld<L> h{RowGeo::of(a.g), &maps, a.parity, ld.yi, ld.zi, 0};
+      ld.advance(gridDim.x, dyr, dzr, a.g.ny);
+      flag = row_flag(a, ld, nrows);
+      return h;
+    }
+  }
+};
+
+// One CTA.  Row j of the CTA sits in stage j % NS; its load completes phase
+// (j / NS) & 1 of full[s].
 //
-// A lattice with cell flags: the copy warp also records in the stage's slot
-// of `meta` whether the row has a non-fluid node (the per-row summary
-// row_flags), and the update warps load the flags of those rows only.
+// CW (copy warp): warps 0 .. nch-1 update chunk k of each of the CTA's
+// rows, warp nch (lane 0) moves them.  The update warps' arrivals on
+// empty[s] (one per warp) complete the row's phase there, after which the
+// copy warp stores the row, waits until the stores have read the stage, and
+// loads row j + NS into it.
+//
+// Without a copy warp: the nch warps update the rows, and the warp that
+// finishes a row last (a per-stage count in shared memory) stores it, waits
+// until the stores have read the stage and loads row j + NS into it; every
+// other warp goes on to the next row at once.  No warp waits for another
+// except through the full barriers, so fewer warps per CTA buy more
+// resident CTAs.  The last warps of consecutive rows take turns: the last
+// warp of row j + 1 can only finish it after leaving row j's copies, so the
+// copies are issued in row order, one thread at a time.  Lane 0 of every
+// warp runs its own RowLoader one row after another, so whichever warp
+// turns out last holds the cursor of the row to load.
+//
+// A lattice with cell flags: whoever loads a row also records in the
+// stage's slot of `meta` whether the row has a non-fluid node (the per-row
+// summary row_flags), and the update warps load the flags of those rows
+// only.
 //
 // BATCH: the rows of many lattices of one operator and one row width (the
 // serving loop): global row r belongs to the item whose range holds it
 // (items sorted by first_row), each item carrying its own step arguments,
-// tensor maps and time.  The copy warp finds the item of each row it moves
-// and records it in the stage's slot of `meta`; the update warps read it
-// there and take the lattice's x extent and rates when it changes.  Batched
+// tensor maps and time.  Whoever loads a row records its item in the
+// stage's slot of `meta` and its RowHeld beside it; the update warps read
+// the item there and take the lattice's x extent and rates when it changes,
+// and the row's RowHeld tells whoever stores it where it goes.  Batched
 // lattices are periodic boxes with no cell flags, buoyancy or macroscopic
 // output.
-template <class L, int ST, int OP, int EQ, bool SH, bool FORCE, int LW, bool BATCH>
+template <class L, int ST, int OP, int EQ, bool SH, bool FORCE, int LW, bool CW, bool BATCH>
 __device__ __forceinline__ void rows_body(const StepArgs& a, const RowMaps<L>& maps,
                                           const RowItem<L>* __restrict__ items, int n_items,
                                           long long batch_rows, int step) {
@@ -363,12 +481,13 @@ __device__ __forceinline__ void rows_body(const StepArgs& a, const RowMaps<L>& m
   using E = typename WO::E;
   using V = typename WO::V;
   using S = typename Lanes<V>::S;
-  using Cfg = RowsCfg<L, ST, LW>;
+  constexpr int NS = rows_stages<CW>();
+  using Cfg = RowsCfg<L, ST, LW, NS>;
   using Pl = RowPlan<L>;
   using Sl = RowSlots<L>;
   using XW = XWord<ST>;
+  using Held = RowHeld<L>;
   constexpr int Q = L::Q;
-  constexpr int NS = kRowsStages;
   const Geo& g = a.g;
 
   extern __shared__ __align__(128) unsigned char rows_smem[];
@@ -379,120 +498,97 @@ __device__ __forceinline__ void rows_body(const StepArgs& a, const RowMaps<L>& m
   uint64_t* bars = reinterpret_cast<uint64_t*>(rows_smem + NS * Cfg::STAGE_BYTES);
   int* abort_flag = reinterpret_cast<int*>(bars + 2 * NS);
   int* meta = abort_flag + 1;  // per stage: BATCH the row's item, else whether it has flags
+  Held* held = reinterpret_cast<Held*>(rows_smem + Cfg::HELD_OFF);  // per stage (no copy warp)
+  // without a copy warp, in the words of the empty barriers: per stage the
+  // update warps done with its row, and the loads issued into it
+  int* done = reinterpret_cast<int*>(bars + NS);
+  int* issued = done + NS;
   const uint32_t stage0 = smem_addr(rows_smem);
   const uint32_t full0 = smem_addr(bars), empty0 = full0 + 8 * NS;
-  const int dyr = (int)(gridDim.x % g.ny), dzr = (int)(gridDim.x / g.ny);
-
-  if (threadIdx.x == 0) {
-    for (int s = 0; s < NS; ++s) {
-      mbar_init(full0 + 8 * s, 1);
-      mbar_init(empty0 + 8 * s, nch);
+  const int dyr = BATCH ? 0 : (int)(gridDim.x % g.ny), dzr = BATCH ? 0 : (int)(gridDim.x / g.ny);
+  const int rbytes = Cfg::row_bytes(nch);
+  // Load row `ld` of the loader into stage s (a sitting-out row only
+  // completes the stage's phase), record its item or flag summary in meta[s]
+  // (published to the update warps by the barrier arrival) and, without a
+  // copy warp, its RowHeld in held[s]; returns the RowHeld.
+  auto load_row = [&](RowLoader<L, BATCH>& lo, int s) -> Held {
+    const int flag = lo.flag;
+    const Held h = lo.next(a, maps, items, n_items, step, dyr, dzr, nrows);
+    meta[s] = BATCH ? h.item : flag;
+    if constexpr (!CW) held[s] = h;
+    if (h.item >= 0) {
+      mbar_expect_tx(full0 + 8 * s, rbytes);
+      rows_copy<L, ST, LW, true>(h.g, h.maps, h.parity, h.yi, h.zi,
+                                 stage0 + s * Cfg::STAGE_BYTES, full0 + 8 * s);
+    } else {
+      mbar_arrive(full0 + 8 * s);
     }
-    *abort_flag = 0;
-    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
-  }
-  __syncthreads();
+    return h;
+  };
 
   RowCursor cur;
   if constexpr (BATCH) cur.r = blockIdx.x;
   else cur.start(blockIdx.x, g.ny);
 
+  // without a copy warp: lane 0 of every warp runs the loader, NS rows
+  // ahead of the warp's own row
+  RowLoader<L, BATCH> ahead;
+  if (!CW && lane == 0) ahead.init(cur, a, nrows);
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < NS; ++s) {
+      mbar_init(full0 + 8 * s, 1);
+      if constexpr (CW) {
+        mbar_init(empty0 + 8 * s, nch);
+      } else {
+        done[s] = 0;
+        issued[s] = 0;
+      }
+    }
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    if constexpr (!CW) {
+      // prologue: the CTA's first NS rows in flight
+      for (int s = 0; s < NS && ahead.ld.r < nrows; ++s) {
+        load_row(ahead, s);
+        issued[s] = 1;
+      }
+    }
+  }
+  if (!CW && lane == 0 && threadIdx.x != 0) {
+    // the other warps' loaders skip the prologue's rows (no copies)
+    for (int s = 0; s < NS && ahead.ld.r < nrows; ++s)
+      ahead.next(a, maps, items, n_items, step, dyr, dzr, nrows);
+  }
+  __syncthreads();
+
   // ------------------------------------------------------------ copy warp
-  if (k == nch) {
+  if (CW && k == nch) {
     if (lane != 0) return;
-    const int rbytes = Cfg::row_bytes(nch);
-    // A row in a stage: its lattice's copy geometry, maps and parity, its
-    // (y, z) there, and (BATCH) its item, -1 for a lattice sitting out.
-    struct Held {
-      RowGeo g;
-      const RowMaps<L>* maps;
-      int parity, yi, zi, item;
-    };
-    Held held[NS];
-    // BATCH: the lattice the load cursor is in, cached while consecutive rows
-    // of this CTA (gridDim.x apart) stay in it: its rows [c_first, c_end),
-    // copy geometry, parity, whether it steps, and the cursor's (y, z) with
-    // the grid stride's (y, z) parts for an incremental advance
-    int c_item = -1, c_yi = 0, c_zi = 0, c_dy = 0, c_dz = 0, c_par = 0;
-    long long c_first = 0, c_end = 0;
-    bool c_live = true;
-    RowGeo c_g = RowGeo::of(g);
-    RowCursor ld = cur;  // next row to load
+    Held hs[NS];
+    RowLoader<L, BATCH> lo;
+    lo.init(cur, a, nrows);
     int nl = 0, nst = 0;  // rows loaded, rows stored
-    // with cell flags: the flag summary of row `ld`, read one row ahead so
-    // the global load's latency passes while the copy thread waits
-    auto row_flag = [&]() -> int {
-      if (BATCH || !a.flags || ld.r >= nrows) return 0;
-      return a.row_flags ? a.row_flags[(ld.zi + g.hz) * g.sy + (ld.yi + g.hy)] : 1;
-    };
-    int ld_flag = row_flag();
     bool failed = false;
-    auto load_next = [&](int s) {
-      Held& h = held[s];
-      bool live = true;
-      if constexpr (BATCH) {
-        const long long r = ld.r;
-        if (c_item >= 0 && r >= c_first && r < c_end) {
-          c_yi += c_dy;
-          if (c_yi >= c_g.ny) { c_yi -= c_g.ny; ++c_zi; }
-          c_zi += c_dz;
-        } else {
-          int lo = 0, hi = n_items - 1;  // last item with first_row <= r
-          while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (items[mid].first_row <= r) lo = mid; else hi = mid - 1;
-          }
-          const RowItem<L>& it = items[lo];
-          c_item = lo;
-          c_g = RowGeo::of(it.a.g);
-          c_first = it.first_row;
-          c_end = c_first + (long long)c_g.ny * c_g.nz;
-          c_par = (int)((it.t0 + step) & 1);
-          c_live = it.t0 + step < it.t_end;
-          const long long local = r - c_first;
-          c_yi = (int)(local % c_g.ny);
-          c_zi = (int)(local / c_g.ny);
-          c_dy = (int)(gridDim.x % (unsigned)c_g.ny);
-          c_dz = (int)(gridDim.x / (unsigned)c_g.ny);
-        }
-        // a lattice that has done its steps sits this step out: its row is
-        // neither loaded nor stored, the update warps see item -1
-        live = c_live;
-        h = Held{c_g, &items[c_item].maps, c_par, c_yi, c_zi, live ? c_item : -1};
-        meta[s] = h.item;  // published to the update warps by the arrival below
-        ld.r += gridDim.x;
-      } else {
-        h = Held{RowGeo::of(g), &maps, a.parity, ld.yi, ld.zi, 0};
-        // whether the update warps load the row's flags (published, as in a
-        // batch, by the barrier arrival below)
-        meta[s] = ld_flag;
-        ld.advance(gridDim.x, dyr, dzr, g.ny);
-        ld_flag = row_flag();
-      }
-      if (live) {
-        mbar_expect_tx(full0 + 8 * s, rbytes);
-        rows_copy<L, ST, LW, true>(h.g, h.maps, h.parity, h.yi, h.zi,
-                                   stage0 + s * Cfg::STAGE_BYTES, full0 + 8 * s);
-      } else {
-        mbar_arrive(full0 + 8 * s);
-      }
+    while (nl < NS && lo.ld.r < nrows) {
+      hs[nl] = load_row(lo, nl);
       ++nl;
-    };
-    while (nl < NS && ld.r < nrows) load_next(nl);
+    }
     while (nst < nl) {
       const int s = nst % NS;
       if (!rows_wait(empty0 + 8 * s, (nst / NS) & 1, kRowsWaitCycles, abort_flag)) {
         failed = true;
         break;
       }
-      const Held& h = held[s];
+      const Held& h = hs[s];
       if (h.item >= 0)
         rows_copy<L, ST, LW, false>(h.g, h.maps, h.parity, h.yi, h.zi,
                                     stage0 + s * Cfg::STAGE_BYTES, 0);
       ++nst;
-      if (ld.r < nrows) {
+      if (lo.ld.r < nrows) {
         bulk_wait_read<0>();  // the stores no longer read the stage
-        load_next(s);
+        hs[s] = load_row(lo, s);
+        ++nl;
       }
     }
     bulk_wait_all();  // every store has landed
@@ -507,7 +603,7 @@ __device__ __forceinline__ void rows_body(const StepArgs& a, const RowMaps<L>& m
     return;
   }
 
-  // ---------------------------------------------------------- update warps
+// ---------------------------------------------------------- update warps
   // Per-lane element offsets of an x position inside a copy's block of
   // `count` lines ([chunk][count][64]): (x >> 6) * count * 64 + (x & 63).
   // The pair's word at x0, the words at x0 + 2 and x0 - 2 and the element
@@ -536,6 +632,38 @@ __device__ __forceinline__ void rows_body(const StepArgs& a, const RowMaps<L>& m
   if constexpr (!BATCH) set_lattice(a);
   const long long consume_limit = BATCH ? kRowsWaitCycles
                                         : (a.wait_cycles > 0 ? a.wait_cycles : kRowsWaitCycles);
+  // ---- row done for this warp: its shared-memory writes become visible to
+  // the copy engine; then one arrival on the stage's empty barrier, or (no
+  // copy warp) the count of warps done, the last of which stores the row
+  // and loads row j + NS into the stage.  Lane 0 of every warp moves its
+  // loader on by one row either way.
+  auto row_done = [&](int s) {
+    fence_async_smem();
+    __syncwarp();
+    if (lane != 0) return;
+    if constexpr (CW) {
+      mbar_arrive(empty0 + 8 * s);
+    } else {
+      __threadfence_block();
+      if (atomicAdd(&done[s], 1) == nch - 1) {
+        // every update warp is done with the row: no warp touches the count
+        // again before the stage's next load lands
+        done[s] = 0;
+        __threadfence_block();
+        const Held h = held[s];
+        if (h.item >= 0)
+          rows_copy<L, ST, LW, false>(h.g, h.maps, h.parity, h.yi, h.zi,
+                                      stage0 + s * Cfg::STAGE_BYTES, 0);
+        if (ahead.ld.r < nrows) {
+          bulk_wait_read<0>();  // this thread's stores no longer read the stage
+          load_row(ahead, s);
+          issued[s] += 1;
+        }
+      } else if (ahead.ld.r < nrows) {
+        ahead.next(a, maps, items, n_items, step, dyr, dzr, nrows);
+      }
+    }
+  };
 
   bool failed = false;
   for (int j = 0; cur.r < nrows; ++j) {
@@ -548,8 +676,7 @@ __device__ __forceinline__ void rows_body(const StepArgs& a, const RowMaps<L>& m
     if constexpr (BATCH) {
       const int item = meta[s];
       if (item < 0) {  // a finished lattice's row: nothing to update
-        __syncwarp();
-        if (lane == 0) mbar_arrive(empty0 + 8 * s);
+        row_done(s);
         cur.r += gridDim.x;
         continue;
       }
@@ -665,11 +792,7 @@ __device__ __forceinline__ void rows_body(const StepArgs& a, const RowMaps<L>& m
     if (!BATCH && a.rho)
       store_macro_pair<S>(a, ((size_t)cur.zi * g.ny + cur.yi) * g.nx + x0, m, solid0, solid1);
 
-    // ---- row done for this warp: its shared-memory writes become visible
-    // to the copy engine, then one arrival on the stage's empty barrier
-    fence_async_smem();
-    __syncwarp();
-    if (lane == 0) mbar_arrive(empty0 + 8 * s);
+    row_done(s);
     if constexpr (BATCH) cur.r += gridDim.x;
     else cur.advance(gridDim.x, dyr, dzr, g.ny);
   }
@@ -677,24 +800,38 @@ __device__ __forceinline__ void rows_body(const StepArgs& a, const RowMaps<L>& m
     atomicExch(abort_flag, 1);
     if (a.err) atomicExch(a.err, 1);
   }
+  if constexpr (!CW) {
+    if (lane == 0) bulk_wait_all();  // this thread's stores have landed
+    // every warp is out of the loop (all waits are bounded); after a
+    // failure, loads issued but never consumed land (bounded again, the
+    // abort flag not consulted) before the CTA's shared memory is released
+    if (__syncthreads_or(failed || flag_set(abort_flag)) && threadIdx.x == 0) {
+      for (int s = 0; s < NS; ++s)
+        if (issued[s] > 0) mbar_wait_bounded(full0 + 8 * s, (issued[s] - 1) & 1);
+    }
+  }
 }
 
-template <class L, int ST, int OP, int EQ, bool SH, bool FORCE, int LW>
-__global__ void __launch_bounds__((LW + 1) * 32, rows_min_blocks<OP, ST, LW>())
+// The single-lattice row kernel; CW: with a copy warp (LW 8), else the
+// update warps move the rows themselves (LW 2, 4).
+template <class L, int ST, int OP, int EQ, bool SH, bool FORCE, int LW, bool CW>
+__global__ void __launch_bounds__((LW + (CW ? 1 : 0)) * 32, rows_min_blocks<OP, ST, LW, CW>())
 step_rows(StepArgs a, const __grid_constant__ RowMaps<L> maps) {
-  rows_body<L, ST, OP, EQ, SH, FORCE, LW, false>(a, maps, nullptr, 0, 0, 0);
+  rows_body<L, ST, OP, EQ, SH, FORCE, LW, CW, false>(a, maps, nullptr, 0, 0, 0);
 }
 
 // One time step of the rows of a batch (launch descriptor read from device
-// memory, so a captured launch serves any resident set of its group).
+// memory, so a captured launch serves any resident set of its group); with
+// a copy warp for rows of 3 chunks or more, as the single-lattice kernel.
 template <class L, int ST, int OP, int EQ, int LW>
-__global__ void __launch_bounds__((LW + 1) * 32, rows_min_blocks<OP, ST, LW>())
+__global__ void __launch_bounds__((LW + (LW != 2 ? 1 : 0)) * 32,
+                                  rows_min_blocks<OP, ST, LW, (LW != 2)>())
 batch_rows(const RowItem<L>* __restrict__ items, const RowBatch* __restrict__ desc, int step) {
   const RowBatch d = *desc;
   if (d.n_items <= 0 || d.n_rows <= 0) return;
   const RowItem<L>* it = items + d.first_item;
-  rows_body<L, ST, OP, EQ, true, false, LW, true>(it[0].a, it[0].maps, it, d.n_items, d.n_rows,
-                                                 step);
+  rows_body<L, ST, OP, EQ, true, false, LW, (LW != 2), true>(it[0].a, it[0].maps, it, d.n_items,
+                                                             d.n_rows, step);
 }
 
 }  // namespace m3lb

@@ -97,8 +97,14 @@ def test_auto_mapping_rule(cuda_device):
 @pytest.mark.parametrize("storage", ["f16", "f16c", "bf16"])
 def test_rows_mapping_equals_chunks(cuda_device, storage):
     """Whole-row launches (one per operator and row width, lattices finishing
-    inside a round) give the chunk mapping's bits, ragged boxes included."""
-    reqs = MIX + RAGGED
+    inside a round) give the chunk mapping's bits, ragged boxes included:
+    rows of 1-2 chunks (moved by the update warps themselves), 3 chunks (a
+    3-chunk stage and a copy warp, N = 144 with a partial last chunk, two
+    lattices in one launch) and 5 chunks (an 8-chunk stage)."""
+    reqs = MIX + RAGGED + [SV.Request(20, 0.0, 144, capi.OP_CM, 9, 0.05),
+                           SV.Request(21, 0.0, 144, capi.OP_CM, 5, 0.03),
+                           SV.Request(22, 0.0, 144, capi.OP_BGK, 6, 0.04),
+                           SV.Request(23, 0.0, 272, capi.OP_TRT, 3, 0.05)]
     ch, ch_f, _ = _serve(reqs, storage, mapping="chunks")
     ro, ro_f, st = _serve(reqs, storage, mapping="rows", round_steps=8)
     assert st.rows_launches == st.launches > 0
