@@ -290,15 +290,21 @@ __device__ __forceinline__ void fence_async_smem() {
   asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
 }
 
-// The copies of one row (interior row yi, zi) by the calling thread.  LOAD:
-// global -> stage (completion on `bar`, whose expected bytes the caller has
-// set); else stage -> global, in one bulk group of this thread.
+// The copies of one row (interior row yi, zi).  LOAD: global -> stage
+// (completion on `bar`, whose expected bytes the caller has set); else stage
+// -> global, in one bulk group of the issuing thread.  Every calling thread
+// computes the coordinates; only where `issue` holds are the copies issued.
+// A whole warp calling with the same arguments keeps the arithmetic on
+// warp-uniform values, and one branch around the copies leaves them
+// straight-line: the copy thread's latency per row is on the path that
+// recycles a stage.
 template <class L, int ST, int LW, bool LOAD>
 __device__ __forceinline__ void rows_copy(const RowGeo g, const RowMaps<L>* maps, int P, int yi,
-                                          int zi, uint32_t stage, uint32_t bar) {
+                                          int zi, uint32_t stage, uint32_t bar, bool issue) {
   using Pl = RowPlan<L>;
   using E = typename WordOps<ST>::E;
   const int py = yi + g.hy, pz = zi + g.hz;
+  int qs[Pl::NOPS], cs[Pl::NOPS];
   static_for<0, Pl::NOPS>([&](auto O) {
     constexpr int o = decltype(O)::value;
     constexpr RowOp op = Pl::ops[o];
@@ -309,11 +315,16 @@ __device__ __forceinline__ void rows_copy(const RowGeo g, const RowMaps<L>* maps
     if constexpr (op.dz != 0) {
       if (rz < 0) rz += g.nz; else if (rz >= g.sz) rz -= g.nz;
     }
-    const int q = op.q0 + op.sgn * P;
-    const int chunk = (rz * g.sy + ry) * g.nch;
+    qs[o] = op.q0 + op.sgn * P;
+    cs[o] = (rz * g.sy + ry) * g.nch;
+  });
+  if (!issue) return;
+  static_for<0, Pl::NOPS>([&](auto O) {
+    constexpr int o = decltype(O)::value;
+    constexpr RowOp op = Pl::ops[o];
     const uint32_t dst = stage + (uint32_t)(RowSlots<L>::base_of(o, LW) * (int)sizeof(E));
-    if constexpr (LOAD) tma_load_box(dst, &maps->m[op.map], q, chunk, bar);
-    else tma_store_box(&maps->m[op.map], q, chunk, dst);
+    if constexpr (LOAD) tma_load_box(dst, &maps->m[op.map], qs[o], cs[o], bar);
+    else tma_store_box(&maps->m[op.map], qs[o], cs[o], dst);
   });
   if constexpr (!LOAD) bulk_commit();
 }
@@ -511,16 +522,18 @@ __device__ __forceinline__ void rows_body(const StepArgs& a, const RowMaps<L>& m
   // completes the stage's phase), record its item or flag summary in meta[s]
   // (published to the update warps by the barrier arrival) and, without a
   // copy warp, its RowHeld in held[s]; returns the RowHeld.
-  auto load_row = [&](RowLoader<L, BATCH>& lo, int s) -> Held {
+  auto load_row = [&](RowLoader<L, BATCH>& lo, int s, bool issue) -> Held {
     const int flag = lo.flag;
     const Held h = lo.next(a, maps, items, n_items, step, dyr, dzr, nrows);
-    meta[s] = BATCH ? h.item : flag;
-    if constexpr (!CW) held[s] = h;
+    if (issue) {
+      meta[s] = BATCH ? h.item : flag;
+      if constexpr (!CW) held[s] = h;
+    }
     if (h.item >= 0) {
-      mbar_expect_tx(full0 + 8 * s, rbytes);
+      if (issue) mbar_expect_tx(full0 + 8 * s, rbytes);
       rows_copy<L, ST, LW, true>(h.g, h.maps, h.parity, h.yi, h.zi,
-                                 stage0 + s * Cfg::STAGE_BYTES, full0 + 8 * s);
-    } else {
+                                 stage0 + s * Cfg::STAGE_BYTES, full0 + 8 * s, issue);
+    } else if (issue) {
       mbar_arrive(full0 + 8 * s);
     }
     return h;
@@ -550,7 +563,7 @@ __device__ __forceinline__ void rows_body(const StepArgs& a, const RowMaps<L>& m
     if constexpr (!CW) {
       // prologue: the CTA's first NS rows in flight
       for (int s = 0; s < NS && ahead.ld.r < nrows; ++s) {
-        load_row(ahead, s);
+        load_row(ahead, s, true);
         issued[s] = 1;
       }
     }
@@ -563,47 +576,56 @@ __device__ __forceinline__ void rows_body(const StepArgs& a, const RowMaps<L>& m
   __syncthreads();
 
   // ------------------------------------------------------------ copy warp
+  // The whole warp runs the loop on warp-uniform values; lane 0 issues the
+  // copies, the barrier arrivals and the bulk-group waits.
   if (CW && k == nch) {
-    if (lane != 0) return;
+    const bool l0 = lane == 0;
     Held hs[NS];
     RowLoader<L, BATCH> lo;
     lo.init(cur, a, nrows);
     int nl = 0, nst = 0;  // rows loaded, rows stored
     bool failed = false;
     while (nl < NS && lo.ld.r < nrows) {
-      hs[nl] = load_row(lo, nl);
+      hs[nl] = load_row(lo, nl, l0);
       ++nl;
     }
     while (nst < nl) {
       const int s = nst % NS;
-      if (!rows_wait(empty0 + 8 * s, (nst / NS) & 1, kRowsWaitCycles, abort_flag)) {
+      // lane 0's view of the wait decides for the warp
+      const bool ok = __shfl_sync(0xffffffffu,
+                                  rows_wait(empty0 + 8 * s, (nst / NS) & 1, kRowsWaitCycles,
+                                            abort_flag), 0);
+      if (!ok) {
         failed = true;
         break;
       }
-      const Held& h = hs[s];
+      const Held h = hs[s];
       if (h.item >= 0)
         rows_copy<L, ST, LW, false>(h.g, h.maps, h.parity, h.yi, h.zi,
-                                    stage0 + s * Cfg::STAGE_BYTES, 0);
+                                    stage0 + s * Cfg::STAGE_BYTES, 0, l0);
       ++nst;
       if (lo.ld.r < nrows) {
-        bulk_wait_read<0>();  // the stores no longer read the stage
-        hs[s] = load_row(lo, s);
+        if (l0) bulk_wait_read<0>();  // the stores no longer read the stage
+        __syncwarp();
+        hs[s] = load_row(lo, s, l0);
         ++nl;
       }
     }
-    bulk_wait_all();  // every store has landed
-    if (failed || flag_set(abort_flag)) {
-      atomicExch(abort_flag, 1);
-      if (a.err) atomicExch(a.err, 1);
-      // loads issued for rows not stored yet land before the CTA's shared
-      // memory is released (bounded; the abort flag is not consulted here)
-      for (int r = nst; r < nl; ++r)
-        mbar_wait_bounded(full0 + 8 * (r % NS), (r / NS) & 1);
+    if (l0) {
+      bulk_wait_all();  // every store has landed
+      if (failed || flag_set(abort_flag)) {
+        atomicExch(abort_flag, 1);
+        if (a.err) atomicExch(a.err, 1);
+        // loads issued for rows not stored yet land before the CTA's shared
+        // memory is released (bounded; the abort flag is not consulted here)
+        for (int r = nst; r < nl; ++r)
+          mbar_wait_bounded(full0 + 8 * (r % NS), (r / NS) & 1);
+      }
     }
     return;
   }
 
-// ---------------------------------------------------------- update warps
+  // ---------------------------------------------------------- update warps
   // Per-lane element offsets of an x position inside a copy's block of
   // `count` lines ([chunk][count][64]): (x >> 6) * count * 64 + (x & 63).
   // The pair's word at x0, the words at x0 + 2 and x0 - 2 and the element
@@ -653,10 +675,10 @@ __device__ __forceinline__ void rows_body(const StepArgs& a, const RowMaps<L>& m
         const Held h = held[s];
         if (h.item >= 0)
           rows_copy<L, ST, LW, false>(h.g, h.maps, h.parity, h.yi, h.zi,
-                                      stage0 + s * Cfg::STAGE_BYTES, 0);
+                                      stage0 + s * Cfg::STAGE_BYTES, 0, true);
         if (ahead.ld.r < nrows) {
           bulk_wait_read<0>();  // this thread's stores no longer read the stage
-          load_row(ahead, s);
+          load_row(ahead, s, true);
           issued[s] += 1;
         }
       } else if (ahead.ld.r < nrows) {
