@@ -25,17 +25,19 @@
 //   * rows are independent: CTAs never exchange data, and a row's global
 //     lines are read and written only by its own CTA within a step.
 // A CTA is nch update warps (warp k takes chunk k of the row; nx even,
-// periodic x; lanes past nx in a partial last chunk store nothing) and one
-// copy warp that moves the rows through a ring of kRowsStages stages: it
-// loads the rows ahead, and once every update warp has marked a row done it
-// stores the row and reloads the stage.  The stage is sized for LW chunks
-// (2, 4 or 8), the smallest that holds the row, so short rows keep more
-// CTAs resident.
+// periodic x; lanes past nx in a partial last chunk store nothing) and, for
+// rows of 3 chunks or more, one copy warp that moves the rows through a
+// ring of kRowsStages stages: it loads the rows ahead, and once every update
+// warp has marked a row done it stores the row and reloads the stage.  Rows
+// of 1-2 chunks have no copy warp: the update warp that finishes a row last
+// moves it, through a ring of 3 stages, so twice as many CTAs are resident.
+// The stage is sized for LW chunks (2, 3, 4 or 8), the smallest that holds
+// the row, so short rows keep more CTAs resident.
 //
 // Waits are bounded: past the limit a warp records a status in
-// StepArgs::err and raises the CTA's abort flag, the copy warp lets its
-// copies in flight finish (bounded again) and the CTA leaves; the host
-// reports the status at the next m3lb_sync.
+// StepArgs::err and raises the CTA's abort flag, the copies in flight
+// finish (bounded again) and the CTA leaves; the host reports the status at
+// the next m3lb_sync.
 #pragma once
 #include <cuda.h>
 
