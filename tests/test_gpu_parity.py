@@ -278,17 +278,19 @@ def test_rows_beyond_one_grid_dimension(cuda_device, lat, shape):
     c.close()
 
 
-def test_row_kernel_wait_that_runs_out_is_reported(cuda_device):
+@pytest.mark.parametrize("nx", [256, 128])
+def test_row_kernel_wait_that_runs_out_is_reported(cuda_device, nx):
     """The row kernel's waits for a row's copies are bounded.  With the
     consume wait cut to one clock cycle (a test-only option; the drain of the
     copies still in flight keeps its full limit), CTAs give up on rows whose
     copies have not landed yet: the kernel records a status instead of
     hanging, and the next m3lb_sync returns it as an error, once.  The handle
     stays usable: with the default limit restored and the lattice seeded
-    again, a step is clean."""
+    again, a step is clean.  nx = 256: rows of 4 chunks moved by a copy
+    warp; nx = 128: rows of 2 chunks moved by the update warps themselves."""
     from m3lb_b200 import capi
 
-    c = Case(lat=27, op=4, storage="f16", shape=(256, 16, 16), periodic=(True, True, True))
+    c = Case(lat=27, op=4, storage="f16", shape=(nx, 16, 16), periodic=(True, True, True))
     c.gpu.set_option(capi.OPT_KERNEL, capi.KERNEL_ROWS)
     c.gpu.initialize(1.0, 0.01, 0.0, 0.0)
     c.gpu.sync()
